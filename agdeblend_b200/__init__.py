@@ -1,0 +1,290 @@
+"""AGDeblend on B200: Python host layer over the in-tree CUDA libraries.
+
+``deblend`` and ``blend`` mirror the reference's Python wrapper
+(wrappers/python/agdeblend/agdeblend.py:13-148 and :150-...) - same argument
+names, meaning, defaults and errors - but call libagdeblend.so /
+libagdeblend_double.so built from agdeblend_b200/csrc for sm_100a.
+``Problem`` exposes the extension API (include/agdeblend_gpu.h): a planned
+problem on which the operator, its adjoint and the solver can be applied
+repeatedly.
+
+There is no CPU fallback: if the CUDA library is missing the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_double, c_int, c_long, c_void_p
+
+import numpy as np
+
+from . import capi
+
+AGDLive = 0
+AGDBad = 1
+AGDMissing = 2
+AGDBlendSum = 0
+AGDBlendMean = 1
+AGDBlendOverwrite = 2
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_NAMES = {np.dtype(np.float32): "libagdeblend.so", np.dtype(np.float64): "libagdeblend_double.so"}
+_libs: dict = {}
+
+
+def library_path(dtype=np.float32) -> str:
+    return os.path.join(PKG_DIR, LIB_NAMES[np.dtype(dtype)])
+
+
+def load_library(dtype=np.float32) -> ctypes.CDLL:
+    """Loads the CUDA library for ``dtype`` (float32 or float64)."""
+    dtype = np.dtype(dtype)
+    if dtype not in _libs:
+        path = library_path(dtype)
+        if not os.path.exists(path):
+            raise RuntimeError(
+                f"{os.path.basename(path)} is not built; run `python -m agdeblend_b200.build`")
+        lib = ctypes.CDLL(path)
+        _bind_extension(lib, dtype)
+        _libs[dtype] = lib
+    return _libs[dtype]
+
+
+def _bind_extension(lib, dtype):
+    rc = capi.real_ctype(dtype)
+    rp = POINTER(rc)
+    problem_args = capi.bind_deblend(lib, dtype, "agd_deblend").argtypes[:12]
+    capi.bind_blend(lib, dtype, "agd_blend")
+    lib.agd_gpu_problem_create.argtypes = problem_args + [POINTER(c_void_p)]
+    lib.agd_gpu_problem_create.restype = c_int
+    lib.agd_gpu_problem_destroy.argtypes = [c_void_p]
+    lib.agd_gpu_problem_destroy.restype = None
+    lib.agd_gpu_problem_info.argtypes = [c_void_p, POINTER(c_long)]
+    lib.agd_gpu_stepsize.argtypes = [c_void_p, rp]
+    lib.agd_gpu_forward.argtypes = [c_void_p, rp, rp]
+    lib.agd_gpu_adjoint.argtypes = [c_void_p, rp, rp]
+    lib.agd_gpu_blend_input.argtypes = [c_void_p, POINTER(rp), rp]
+    lib.agd_gpu_set_output.argtypes = [c_void_p, rp, POINTER(rp)]
+    lib.agd_gpu_solve.argtypes = [c_void_p, rc, c_int, c_int, POINTER(rp)]
+    lib.agd_gpu_time_iterations.argtypes = [c_void_p, POINTER(rp), rc, c_int, c_int, c_int,
+                                            POINTER(c_double)]
+    lib.agd_gpu_profile_iteration.argtypes = [c_void_p, rc, POINTER(c_double)]
+    lib.agd_gpu_profile_iteration.restype = c_int
+    lib.agd_plan_export.argtypes = problem_args + [POINTER(c_long), POINTER(c_int),
+                                                   POINTER(c_long)]
+    for name in ("agd_gpu_problem_info", "agd_gpu_stepsize", "agd_gpu_forward",
+                 "agd_gpu_adjoint", "agd_gpu_blend_input", "agd_gpu_set_output",
+                 "agd_gpu_solve", "agd_gpu_time_iterations", "agd_plan_export"):
+        getattr(lib, name).restype = c_int
+
+
+def _dtype_of(data) -> np.dtype:
+    d = np.asarray(data[0]).dtype
+    if d == np.float64:
+        return np.dtype(np.float64)
+    if d == np.float32:
+        return np.dtype(np.float32)
+    raise RuntimeError("data must be float32 or float64")
+
+
+def _n_dims(volumes, data):
+    n_volumes = int(np.max(volumes)) + 1
+    n_dims = np.zeros(n_volumes, np.int32)
+    for v, d in zip(volumes, data):
+        n_dims[int(v)] = np.asarray(d).ndim
+    return n_dims
+
+
+def deblend(volumes, window_shapes, coords, shottimes, channels, trace_types, initial_factor,
+            n_its, print_freq, data, wavelet_idxs=None, wavelets=None, comm=None):
+    """Deblends seismic data; same arguments and result as the reference's
+    ``agdeblend.deblend`` (serial form: ``comm`` must be None)."""
+    if comm is not None:
+        raise RuntimeError("MPI communicators are not supported: the problem runs on one GPU")
+    dtype = _dtype_of(data)
+    lib = load_library(dtype)
+    if len(volumes) != len(data):
+        raise RuntimeError("volumes must have the same length as data")
+    for name, arr in (("coords", coords), ("shottimes", shottimes), ("channels", channels),
+                      ("trace_types", trace_types)):
+        if len(arr) != len(data):
+            raise RuntimeError(f"{name} must have the same number of patches as data")
+    n_traces = [int(np.prod(np.asarray(d).shape[:-1])) for d in data]
+    for name, arr in (("shottimes", shottimes), ("channels", channels),
+                      ("trace_types", trace_types)):
+        for n, a in zip(n_traces, arr):
+            if np.asarray(a).size != n:
+                raise RuntimeError(f"{name} must have the same number of traces as data")
+    if (wavelet_idxs is None) != (wavelets is None):
+        raise RuntimeError("If wavelet_idxs or wavelets is not None, they both must not be")
+    wavelet_lengths = None
+    if wavelets is not None:
+        wavelet_lengths = [len(w) for w in wavelets]
+    shapes = [list(np.asarray(d).shape) for d in data]
+    args = capi.DeblendArgs(volumes, _n_dims(volumes, data), window_shapes, coords, shapes,
+                            shottimes, channels, trace_types, data, wavelet_lengths,
+                            wavelet_idxs, wavelets, dtype=dtype)
+    fn = lib.agd_deblend
+    if capi.call_deblend(fn, args, initial_factor, n_its, print_freq):
+        raise RuntimeError("Error in call to agd_deblend")
+    return [d.astype(dtype) for d in args.data]
+
+
+def blend(shottimes, channels, trace_types, data, blend_mode, taper_length=0, n_times_out=None,
+          shottimes_out=None, channels_out=None, trace_types_out=None, comm=None,
+          data_out=None):
+    """Blends seismic data or modifies already blended data; same arguments
+    and result as the reference's ``agdeblend.blend`` (serial form)."""
+    if comm is not None:
+        raise RuntimeError("MPI communicators are not supported: the problem runs on one GPU")
+    if blend_mode not in (AGDBlendSum, AGDBlendMean, AGDBlendOverwrite):
+        raise RuntimeError("Invalid blend_mode")
+    dtype = _dtype_of(data)
+    lib = load_library(dtype)
+    shottimes_out = shottimes if shottimes_out is None else shottimes_out
+    channels_out = channels if channels_out is None else channels_out
+    trace_types_out = trace_types if trace_types_out is None else trace_types_out
+    n_times = [int(np.asarray(d).shape[-1]) for d in data]
+    if data_out is not None:
+        n_times_out = [int(np.asarray(d).shape[-1]) for d in data_out]
+    elif n_times_out is None:
+        n_times_out = n_times
+    outs = None
+    if data_out is not None:
+        outs = [np.ascontiguousarray(d.reshape(-1, d.shape[-1])) for d in data_out]
+        for d in outs:
+            if d.dtype != dtype:
+                raise RuntimeError("data_out does not have the right data type")
+    rc, res = capi.call_blend(lib.agd_blend, dtype, n_times, shottimes, channels, trace_types,
+                              [np.asarray(d).reshape(-1, n) for d, n in zip(data, n_times)],
+                              blend_mode, taper_length, n_times_out, shottimes_out,
+                              channels_out, trace_types_out, outs)
+    if rc:
+        raise RuntimeError("Error in call to agd_blend")
+    shapes = [list(np.asarray(s).shape) + [n] for s, n in zip(shottimes_out, n_times_out)]
+    if data_out is not None:
+        for d, r in zip(data_out, res):
+            d[...] = r.reshape(d.shape)
+        return data_out
+    return [r.reshape(s) for r, s in zip(res, shapes)]
+
+
+class Problem:
+    """A planned deblending problem on the current GPU (extension API)."""
+
+    def __init__(self, volumes, n_dims, window_shapes, coords, shapes, shottimes, channels,
+                 trace_types, wavelet_lengths=None, wavelet_idxs=None, wavelets=None,
+                 dtype=np.float32):
+        self.dtype = np.dtype(dtype)
+        self.lib = load_library(self.dtype)
+        self.args = capi.DeblendArgs(volumes, n_dims, window_shapes, coords, shapes, shottimes,
+                                     channels, trace_types, None, wavelet_lengths, wavelet_idxs,
+                                     wavelets, dtype=self.dtype)
+        self.shapes = [tuple(int(v) for v in s) for s in shapes]
+        h = c_void_p()
+        if self.lib.agd_gpu_problem_create(*self.args.problem_args(), ctypes.byref(h)):
+            raise RuntimeError("agd_gpu_problem_create failed")
+        self.h = h
+        info = np.zeros(8, np.int64)
+        self.lib.agd_gpu_problem_info(self.h, info.ctypes.data_as(POINTER(c_long)))
+        self.info = info
+        self.n_windows = int(info[0])
+        self.model_size = int(info[1])
+        self.record_size = int(info[2])
+        rc = capi.real_ctype(self.dtype)
+        s = rc()
+        self.lib.agd_gpu_stepsize(self.h, ctypes.byref(s))
+        self.stepsize = float(s.value)
+        self._rp = POINTER(rc)
+
+    @classmethod
+    def from_survey(cls, sv, dtype=np.float32):
+        return cls(sv.volumes, sv.n_dims, sv.window_shapes, sv.coords, sv.shapes, sv.shottimes,
+                   sv.channels, sv.trace_types, sv.wavelet_lengths, sv.wavelet_idxs,
+                   sv.wavelets, dtype=dtype)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.agd_gpu_problem_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _p(self, a):
+        return a.ctypes.data_as(self._rp)
+
+    def _check(self, rc, name):
+        if rc:
+            raise RuntimeError(f"{name} failed")
+
+    def forward(self, model: np.ndarray) -> np.ndarray:
+        """A x; ``model`` interleaved (re, im) of 2 * model_size reals."""
+        m = np.ascontiguousarray(model, self.dtype)
+        out = np.zeros(self.record_size, self.dtype)
+        self._check(self.lib.agd_gpu_forward(self.h, self._p(m), self._p(out)), "forward")
+        return out
+
+    def adjoint(self, record: np.ndarray) -> np.ndarray:
+        r = np.ascontiguousarray(record, self.dtype)
+        out = np.zeros(2 * self.model_size, self.dtype)
+        self._check(self.lib.agd_gpu_adjoint(self.h, self._p(r), self._p(out)), "adjoint")
+        return out
+
+    def _data_ptrs(self, data, writable=False):
+        arrs = [np.array(d, self.dtype, copy=True, order="C") if writable
+                else np.ascontiguousarray(d, self.dtype) for d in data]
+        return capi._ptrs(arrs, self.dtype, capi.real_ctype(self.dtype), writable=writable)
+
+    def blend_input(self, data) -> np.ndarray:
+        ptrs, keep = self._data_ptrs(data)
+        out = np.zeros(self.record_size, self.dtype)
+        self._check(self.lib.agd_gpu_blend_input(self.h, ptrs, self._p(out)), "blend_input")
+        return out
+
+    def set_output(self, model: np.ndarray) -> list:
+        m = np.ascontiguousarray(model, self.dtype)
+        outs = [np.zeros(s, self.dtype) for s in self.shapes]
+        ptrs, keep = capi._ptrs(outs, self.dtype, capi.real_ctype(self.dtype), writable=True)
+        self._check(self.lib.agd_gpu_set_output(self.h, self._p(m), ptrs), "set_output")
+        return outs
+
+    def solve(self, data, initial_factor: float, n_its: int, print_freq: int = 0) -> list:
+        ptrs, keep = self._data_ptrs(data, writable=True)
+        self._check(self.lib.agd_gpu_solve(self.h, initial_factor, n_its, print_freq, ptrs),
+                    "solve")
+        return [k.reshape(s) for k, s in zip(keep, self.shapes)]
+
+    def time_iterations(self, data, initial_factor: float, n_its: int, warmup: int,
+                        steps: int) -> np.ndarray:
+        ptrs, keep = self._data_ptrs(data)
+        t = np.zeros(4, np.float64)
+        self._check(self.lib.agd_gpu_time_iterations(
+            self.h, ptrs, initial_factor, n_its, warmup, steps,
+            t.ctypes.data_as(POINTER(c_double))), "time_iterations")
+        return t
+
+    def profile_iteration(self, lamb: float) -> np.ndarray:
+        ms = np.zeros(16, np.float64)
+        self._check(self.lib.agd_gpu_profile_iteration(
+            self.h, lamb, ms.ctypes.data_as(POINTER(c_double))), "profile_iteration")
+        return ms
+
+
+def plan_export(volumes, n_dims, window_shapes, coords, shapes, shottimes, channels,
+                trace_types, wavelet_lengths=None, wavelet_idxs=None, wavelets=None,
+                dtype=np.float32):
+    """Host planning only (no GPU): (info[8], windows[n, 32], blend[n_traces, 3])."""
+    lib = load_library(dtype)
+    args = capi.DeblendArgs(volumes, n_dims, window_shapes, coords, shapes, shottimes, channels,
+                            trace_types, None, wavelet_lengths, wavelet_idxs, wavelets,
+                            dtype=dtype)
+    info = np.zeros(8, np.int64)
+    if lib.agd_plan_export(*args.problem_args(), info.ctypes.data_as(POINTER(c_long)), None,
+                           None):
+        raise RuntimeError("agd_plan_export failed")
+    win = np.zeros((int(info[0]), 32), np.int32)
+    blend_c = np.zeros((int(info[3]), 3), np.int64)
+    lib.agd_plan_export(*args.problem_args(), info.ctypes.data_as(POINTER(c_long)),
+                        win.ctypes.data_as(POINTER(c_int)), blend_c.ctypes.data_as(POINTER(c_long)))
+    return info, win, blend_c

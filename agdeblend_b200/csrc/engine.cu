@@ -1,0 +1,1202 @@
+// Device engine of the deblending path: turns a Plan into device tables and
+// launch lists, runs the operator, the ISTA solver and blending, and exports
+// the C API (include/agdeblend.h) and the extension API
+// (include/agdeblend_gpu.h).  Built twice: float (libagdeblend.so) and, with
+// -DAGD_DOUBLE, double (libagdeblend_double.so).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "agdeblend_gpu.h"
+#include "kernels.cuh"
+#include "plan.hpp"
+
+namespace agd {
+
+struct DeviceError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+static void check(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) {
+    char buf[512];
+    std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+    throw DeviceError(buf);
+  }
+}
+#define CK(x) check((x), #x)
+
+template <typename T>
+class DevArray {
+ public:
+  DevArray() = default;
+  DevArray(const DevArray &) = delete;
+  DevArray &operator=(const DevArray &) = delete;
+  DevArray(DevArray &&o) noexcept : p_(o.p_), n_(o.n_) {
+    o.p_ = nullptr;
+    o.n_ = 0;
+  }
+  DevArray &operator=(DevArray &&o) noexcept {
+    if (this != &o) {
+      release();
+      p_ = o.p_;
+      n_ = o.n_;
+      o.p_ = nullptr;
+      o.n_ = 0;
+    }
+    return *this;
+  }
+  ~DevArray() { release(); }
+  void alloc(size_t n) {
+    release();
+    if (n) CK(cudaMalloc(reinterpret_cast<void **>(&p_), n * sizeof(T)));
+    n_ = n;
+  }
+  void upload(const std::vector<T> &v, cudaStream_t s) {
+    alloc(v.size());
+    if (n_) CK(cudaMemcpyAsync(p_, v.data(), n_ * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  T *get() const { return p_; }
+  size_t size() const { return n_; }
+  size_t bytes() const { return n_ * sizeof(T); }
+  void release() {
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    n_ = 0;
+  }
+
+ private:
+  T *p_ = nullptr;
+  size_t n_ = 0;
+};
+
+// Distinct FFT lengths with their radix lists and twiddle tables.
+template <typename R>
+struct FftTable {
+  std::vector<FftDesc> descs;
+  std::vector<Cx<R>> tw;
+  std::map<int, int> index;
+
+  int get(int n) {
+    auto it = index.find(n);
+    if (it != index.end()) return it->second;
+    FftDesc d{};
+    d.n = n;
+    d.nf = 0;
+    int m = n;
+    for (int r : {4, 2, 3, 5}) {
+      while (m % r == 0) {
+        d.radix[d.nf++] = r;
+        m /= r;
+      }
+    }
+    for (int p = 7; m > 1; p += 2) {
+      while (m % p == 0) {
+        if (d.nf >= kMaxFactors) throw DeviceError("FFT length has too many factors");
+        d.radix[d.nf++] = p;
+        m /= p;
+      }
+    }
+    d.tw_off = (long)tw.size();
+    for (int k = 0; k < n; ++k) {
+      const double a = -2.0 * 3.14159265358979323846 * (double)k / (double)n;
+      Cx<R> w;
+      w.x = (R)std::cos(a);
+      w.y = (R)std::sin(a);
+      tw.push_back(w);
+    }
+    const int id = (int)descs.size();
+    descs.push_back(d);
+    index[n] = id;
+    return id;
+  }
+};
+
+static int optin_smem() {
+  int dev = 0;
+  int v = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  return v;
+}
+
+template <typename R>
+class Engine {
+ public:
+  using C = Cx<R>;
+
+  struct AxisLaunch {
+    DevArray<AxisJob<R>> jobs;
+    DevArray<int> cta_job;
+    DevArray<long> cta_line0;
+    int n_cta = 0;
+    int lpc = 0;
+    size_t smem = 0;
+  };
+  struct TimeLaunch {
+    DevArray<int> cta_job;
+    DevArray<int> cta_trace0;
+    int n_cta = 0;
+    int nb = 0;
+    size_t smem = 0;
+  };
+  struct GatherLaunch {
+    DevArray<Contrib> contrib;
+    DevArray<long> chunk_ptr;
+    int n_chunk = 0;
+    int chunk = 512;
+    long n_contrib = 0;
+  };
+
+  Plan plan;
+  cudaStream_t stream = nullptr;
+  int smem_max = 0;
+  FftTable<R> fft;
+  DevArray<FftDesc> d_descs;
+  DevArray<C> d_tw;
+
+  DevArray<C> X, S0, S1, G;
+  DevArray<R> Y, rec_d, rec_r, data_dev;
+  DevArray<uint8_t> mute;
+  DevArray<R> space_scale, space_fold, time_taper;
+  DevArray<long> blend_rec;
+  DevArray<int> blend_ts, blend_n;
+  DevArray<int> wsrc;
+  DevArray<C> spectra;
+  DevArray<long> spec_off;
+  DevArray<long> wt_dst;  // trace buffer offset of each window trace
+  DevArray<int> wt_C;
+  DevArray<TimeJob<R>> time_jobs;
+  DevArray<WaveletJob<R>> wav_jobs;
+  DevArray<long> out_ptr, out_src, out_dst;
+  DevArray<int> out_nt;
+  DevArray<R> scalar;
+  DevArray<double> dscalar;
+
+  std::vector<AxisLaunch> fwd, adj_update, adj_plain;
+  TimeLaunch time_fwd, time_adj, wav;
+  GatherLaunch g_fwd, g_input;
+  std::vector<long> trace_off;   // per window, in reals
+  std::vector<long> patch_off;   // per patch, in reals
+  long n_wtraces = 0;
+  long data_size = 0;
+  long out_traces = 0;
+  bool wavelets = false;
+  R stepsize = 0;
+
+  explicit Engine(Plan &&p) : plan(std::move(p)) {
+    CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    smem_max = optin_smem();
+    set_smem_limits();
+    build();
+  }
+
+  ~Engine() {
+    if (stream) {
+      cudaStreamSynchronize(stream);
+      cudaStreamDestroy(stream);
+    }
+  }
+
+  size_t device_bytes() const {
+    return X.bytes() + S0.bytes() + S1.bytes() + G.bytes() + Y.bytes() + rec_d.bytes() +
+           rec_r.bytes() + data_dev.bytes() + mute.bytes() + g_fwd.contrib.bytes() +
+           g_input.contrib.bytes();
+  }
+
+  // Opt every dynamic-shared-memory kernel in to the device limit minus its
+  // own static shared memory; smem_max becomes the smallest such limit.
+  template <typename K>
+  int opt_in(K kernel, int limit) {
+    cudaFuncAttributes fa;
+    CK(cudaFuncGetAttributes(&fa, kernel));
+    const int dyn = limit - (int)fa.sharedSizeBytes;
+    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+    return dyn;
+  }
+
+  void set_smem_limits() {
+    const int limit = smem_max;
+    smem_max = std::min({opt_in(axis_pass<R>, limit), opt_in(time_c2r_ola<R>, limit),
+                         opt_in(time_r2c<R>, limit), opt_in(wavelet_apply<R>, limit)});
+  }
+
+  // ---------------------------------------------------------------- set-up
+
+  void make_axis_launch(AxisLaunch &L, const std::vector<AxisJob<R>> &jobs) {
+    if (jobs.empty()) return;
+    int n_max = 1;
+    for (const auto &j : jobs) n_max = std::max(n_max, fft.descs[j.fft].n);
+    const size_t per_line = 2 * (size_t)n_max * sizeof(C);
+    const size_t budget = 64 * 1024;
+    int lpc = (int)std::max<size_t>(1, budget / per_line);
+    lpc = std::min(lpc, 256);
+    if (per_line * lpc > (size_t)smem_max) throw DeviceError("space axis too long");
+    std::vector<int> cj;
+    std::vector<long> cl;
+    for (size_t i = 0; i < jobs.size(); ++i) {
+      const long lines = jobs[i].outer * jobs[i].inner;
+      for (long q = 0; q < lines; q += lpc) {
+        cj.push_back((int)i);
+        cl.push_back(q);
+      }
+    }
+    L.jobs.upload(jobs, stream);
+    L.cta_job.upload(cj, stream);
+    L.cta_line0.upload(cl, stream);
+    L.n_cta = (int)cj.size();
+    L.lpc = lpc;
+    L.smem = per_line * lpc;
+  }
+
+  void make_time_launch(TimeLaunch &L, size_t per_trace, int nb_cap) {
+    int nb = nb_cap;
+    while (nb > 1 && per_trace * nb > (size_t)std::min(smem_max, 160 * 1024)) nb /= 2;
+    if (per_trace * nb > (size_t)smem_max)
+      throw DeviceError("time window or trace too long for shared memory");
+    std::vector<int> cj, ct;
+    for (size_t w = 0; w < plan.windows.size(); ++w) {
+      for (int t = 0; t < plan.windows[w].n_traces; t += nb) {
+        cj.push_back((int)w);
+        ct.push_back(t);
+      }
+    }
+    L.cta_job.upload(cj, stream);
+    L.cta_trace0.upload(ct, stream);
+    L.n_cta = (int)cj.size();
+    L.nb = nb;
+    L.smem = per_trace * nb;
+  }
+
+  void make_gather(GatherLaunch &G, const std::vector<Contrib> &list, long record_size) {
+    G.n_chunk = (int)((record_size + G.chunk - 1) / G.chunk);
+    std::vector<long> count(G.n_chunk + 1, 0);
+    for (const Contrib &c : list) {
+      if (c.n <= 0) continue;
+      const long a = c.rec / G.chunk;
+      const long b = (c.rec + c.n - 1) / G.chunk;
+      for (long k = a; k <= b; ++k) count[k + 1]++;
+    }
+    for (int k = 0; k < G.n_chunk; ++k) count[k + 1] += count[k];
+    std::vector<Contrib> flat(count[G.n_chunk]);
+    std::vector<long> fill(count.begin(), count.end() - 1);
+    for (const Contrib &c : list) {
+      if (c.n <= 0) continue;
+      const long a = c.rec / G.chunk;
+      const long b = (c.rec + c.n - 1) / G.chunk;
+      for (long k = a; k <= b; ++k) flat[fill[k]++] = c;
+    }
+    G.contrib.upload(flat, stream);
+    G.chunk_ptr.upload(count, stream);
+    G.n_contrib = (long)list.size();
+  }
+
+  void build() {
+    const long M = plan.model_size;
+    const int nw = (int)plan.windows.size();
+    // ---- FFT tables and per-window trace tables
+    int Pt_max = 1, C_max = 1, maxD = 0;
+    trace_off.assign(nw, 0);
+    long toff = 0;
+    std::vector<R> sscale, sfold, ttaper;
+    std::vector<long> brec, wdst;
+    std::vector<int> bts, bn, ws, wC;
+    std::vector<long> ttaper_off(nw);
+    std::vector<TimeJob<R>> tj(nw);
+    std::vector<WaveletJob<R>> wj(nw);
+    std::vector<long> wt_base(nw);
+    for (int w = 0; w < nw; ++w) {
+      const WindowPlan &W = plan.windows[w];
+      trace_off[w] = toff;
+      wt_base[w] = (long)sscale.size();
+      for (int t = 0; t < W.n_traces; ++t) {
+        // scaler then space tapers from the last dim to the first, the
+        // multiplication order of src/fk.c:343-347
+        R s = W.scaler;
+        R fold = (R)1;
+        int r = t;
+        int coord[kMaxSpaceDims];
+        for (int d = W.D - 1; d >= 0; --d) {
+          coord[d] = r % W.L[d];
+          r /= W.L[d];
+        }
+        for (int d = W.D - 1; d >= 0; --d) {
+          s *= W.taper[d][coord[d]];
+          fold *= W.taper[d][coord[d]];
+        }
+        sscale.push_back(s);
+        sfold.push_back(fold);
+        brec.push_back(W.blend[t].rec);
+        bts.push_back(W.blend[t].trace_start);
+        bn.push_back(W.blend[t].n);
+        ws.push_back(W.wavelet_src.empty() ? -1 : W.wavelet_src[t]);
+        wdst.push_back(toff + (long)t * W.C);
+        wC.push_back(W.C);
+      }
+      ttaper_off[w] = (long)ttaper.size();
+      ttaper.insert(ttaper.end(), W.taper[W.D].begin(), W.taper[W.D].end());
+      toff += (long)W.n_traces * W.C;
+      Pt_max = std::max(Pt_max, W.Pt);
+      C_max = std::max(C_max, W.C);
+      maxD = std::max(maxD, W.D);
+      if (!W.wavelet_src.empty()) wavelets = true;
+    }
+    n_wtraces = (long)sscale.size();
+    space_scale.upload(sscale, stream);
+    space_fold.upload(sfold, stream);
+    time_taper.upload(ttaper, stream);
+    blend_rec.upload(brec, stream);
+    blend_ts.upload(bts, stream);
+    blend_n.upload(bn, stream);
+    wsrc.upload(ws, stream);
+    wt_dst.upload(wdst, stream);
+    wt_C.upload(wC, stream);
+
+    X.alloc(M);
+    S0.alloc(M);
+    S1.alloc(M);
+    Y.alloc(toff);
+    rec_d.alloc(plan.record_size);
+    rec_r.alloc(plan.record_size);
+    scalar.alloc(1);
+    dscalar.alloc(1);
+    {
+      std::vector<uint8_t> m(plan.record_size, 0);
+      for (const auto &mu : plan.mute)
+        for (int k = 0; k < mu.second; ++k) m[mu.first + k] = 1;
+      mute.upload(m, stream);
+    }
+    C *Sb[2] = {S0.get(), S1.get()};
+
+    // ---- time-axis jobs
+    for (int w = 0; w < nw; ++w) {
+      const WindowPlan &W = plan.windows[w];
+      TimeJob<R> &j = tj[w];
+      j.z = Sb[(W.D - 1) & 1] + W.model_off;
+      j.y = Y.get() + trace_off[w];
+      j.space_scale = space_scale.get() + wt_base[w];
+      j.time_taper = time_taper.get() + ttaper_off[w];
+      j.blend_rec = blend_rec.get() + wt_base[w];
+      j.blend_ts = blend_ts.get() + wt_base[w];
+      j.blend_n = blend_n.get() + wt_base[w];
+      j.n_traces = W.n_traces;
+      j.T = W.T;
+      j.F = W.F;
+      j.Lt = W.Lt;
+      j.Pt = W.Pt;
+      j.h = W.h;
+      j.n_fk = W.n_fk;
+      j.C = W.C;
+      j.fft = fft.get(W.Pt);
+      WaveletJob<R> &v = wj[w];
+      v.y = Y.get() + trace_off[w];
+      v.src = wsrc.get() + wt_base[w];
+      v.n_traces = W.n_traces;
+      v.C = W.C;
+      v.fft = wavelets ? fft.get(W.C) : 0;
+    }
+    time_jobs.upload(tj, stream);
+    const size_t per_trace_time = 2 * (size_t)Pt_max * sizeof(C) + (size_t)C_max * sizeof(R);
+    make_time_launch(time_fwd, per_trace_time, 16);
+    make_time_launch(time_adj, per_trace_time, 16);
+    if (wavelets) {
+      wav_jobs.upload(wj, stream);
+      make_time_launch(wav, 2 * (size_t)C_max * sizeof(C), 8);
+      // spectra table
+      std::vector<C> sp;
+      std::vector<long> so;
+      for (const auto &s : plan.spectra) {
+        so.push_back((long)sp.size());
+        for (const auto &v : s) {
+          C c;
+          c.x = (R)v.real();
+          c.y = (R)v.imag();
+          sp.push_back(c);
+        }
+      }
+      spectra.upload(sp, stream);
+      spec_off.upload(so, stream);
+    }
+
+    // ---- space-axis passes
+    fwd.resize(maxD);
+    adj_update.resize(maxD);
+    adj_plain.resize(maxD);
+    for (int k = 0; k < maxD; ++k) {
+      std::vector<AxisJob<R>> jf, ju, jp;
+      for (int w = 0; w < nw; ++w) {
+        const WindowPlan &W = plan.windows[w];
+        if (W.D <= k) continue;
+        const long TF = (long)W.T * W.F;
+        {  // forward: axis D-1-k, inverse FFT, crop P -> L
+          const int a = W.D - 1 - k;
+          AxisJob<R> j{};
+          long outer = TF;
+          for (int d = 0; d < a; ++d) outer *= W.P[d];
+          int inner = 1;
+          for (int d = a + 1; d < W.D; ++d) inner *= W.L[d];
+          j.src = (k == 0 ? X.get() : Sb[(k - 1) & 1]) + W.model_off;
+          j.dst = Sb[k & 1] + W.model_off;
+          j.outer = outer;
+          j.inner = inner;
+          j.n_in = W.P[a];
+          j.n_out = W.L[a];
+          j.fft = fft.get(W.P[a]);
+          jf.push_back(j);
+        }
+        {  // adjoint: axis k, zero-pad L -> P, forward FFT
+          const int a = k;
+          AxisJob<R> j{};
+          long outer = TF;
+          for (int d = 0; d < a; ++d) outer *= W.P[d];
+          int inner = 1;
+          for (int d = a + 1; d < W.D; ++d) inner *= W.L[d];
+          j.src = Sb[(W.D - 1 + k) & 1] + W.model_off;
+          j.outer = outer;
+          j.inner = inner;
+          j.n_in = W.L[a];
+          j.n_out = W.P[a];
+          j.fft = fft.get(W.P[a]);
+          const bool last = (k == W.D - 1);
+          j.dst = last ? X.get() + W.model_off : Sb[(W.D + k) & 1] + W.model_off;
+          ju.push_back(j);
+          j.dst = last ? nullptr : Sb[(W.D + k) & 1] + W.model_off;  // G set lazily
+          jp.push_back(j);
+        }
+      }
+      make_axis_launch(fwd[k], jf);
+      make_axis_launch(adj_update[k], ju);
+      pending_plain.push_back(jp);
+    }
+
+    // ---- forward blend: window traces into the record, window then trace
+    {
+      std::vector<Contrib> list;
+      for (int w = 0; w < nw; ++w) {
+        const WindowPlan &W = plan.windows[w];
+        for (int t = 0; t < W.n_traces; ++t) {
+          const BlendCoord &b = W.blend[t];
+          if (b.rec < 0) continue;
+          Contrib c{b.rec, trace_off[w] + (long)t * W.C + b.trace_start, b.n, 0};
+          list.push_back(c);
+        }
+      }
+      make_gather(g_fwd, list, plan.record_size);
+    }
+
+    // ---- input blend and output gather tables (patch traces)
+    patch_off.assign(plan.n_patches, 0);
+    long poff = 0;
+    for (int p = 0; p < plan.n_patches; ++p) {
+      patch_off[p] = poff;
+      poff += (long)plan.n_traces[p] * plan.n_times[p];
+    }
+    data_size = poff;
+    data_dev.alloc(data_size);
+    {
+      std::vector<std::vector<long>> cover;  // per global patch trace
+      std::vector<long> tr_base(plan.n_patches);
+      long ntr = 0;
+      for (int p = 0; p < plan.n_patches; ++p) {
+        tr_base[p] = ntr;
+        ntr += plan.n_traces[p];
+      }
+      cover.resize(ntr);
+      for (int w = 0; w < nw; ++w) {
+        const WindowPlan &W = plan.windows[w];
+        for (int t = 0; t < W.n_traces; ++t)
+          cover[tr_base[W.patch] + W.trace_index[t]].push_back(trace_off[w] + (long)t * W.C +
+                                                              W.h);
+      }
+      std::vector<long> ptr(ntr + 1, 0), src, dst(ntr);
+      std::vector<int> nt(ntr);
+      for (int p = 0; p < plan.n_patches; ++p) {
+        for (int t = 0; t < plan.n_traces[p]; ++t) {
+          const long g = tr_base[p] + t;
+          dst[g] = patch_off[p] + (long)t * plan.n_times[p];
+          nt[g] = plan.n_times[p];
+        }
+      }
+      for (long g = 0; g < ntr; ++g) {
+        ptr[g + 1] = ptr[g] + (long)cover[g].size();
+        src.insert(src.end(), cover[g].begin(), cover[g].end());
+      }
+      out_ptr.upload(ptr, stream);
+      out_src.upload(src, stream);
+      out_dst.upload(dst, stream);
+      out_nt.upload(nt, stream);
+      out_traces = ntr;
+    }
+    d_descs.upload(fft.descs, stream);
+    d_tw.upload(fft.tw, stream);
+    CK(cudaStreamSynchronize(stream));
+  }
+
+  std::vector<std::vector<AxisJob<R>>> pending_plain;
+
+  void ensure_plain_adjoint() {
+    if (G.get() != nullptr || plan.model_size == 0) return;
+    G.alloc(plan.model_size);
+    for (size_t k = 0; k < pending_plain.size(); ++k) {
+      auto jobs = pending_plain[k];
+      size_t i = 0;
+      for (int w = 0; w < (int)plan.windows.size(); ++w) {
+        const WindowPlan &W = plan.windows[w];
+        if (W.D <= (int)k) continue;
+        if ((int)k == W.D - 1) jobs[i].dst = G.get() + W.model_off;
+        ++i;
+      }
+      make_axis_launch(adj_plain[k], jobs);
+    }
+    CK(cudaStreamSynchronize(stream));
+  }
+
+  void set_input_gather(const std::vector<Contrib> &list) {
+    make_gather(g_input, list, plan.record_size);
+  }
+
+  // ---------------------------------------------------------------- launches
+
+  void launch_axis(const AxisLaunch &L, int inverse, int epilogue, R step, R lamb) {
+    if (L.n_cta == 0) return;
+    axis_pass<R><<<L.n_cta, kThreads, L.smem, stream>>>(
+        L.jobs.get(), L.cta_job.get(), L.cta_line0.get(), L.lpc, d_descs.get(), d_tw.get(),
+        inverse, epilogue, step, lamb, scalar.get());
+    CK(cudaGetLastError());
+  }
+
+  void launch_gather(const GatherLaunch &Gl, const R *src, R *out, int mode, bool use_mute,
+                     const R *d, const R *taper, int taper_len, double *sumsq) {
+    if (Gl.n_chunk == 0) return;
+    blend_gather<R><<<Gl.n_chunk, kThreads, 0, stream>>>(
+        Gl.contrib.get(), Gl.chunk_ptr.get(), Gl.chunk, plan.record_size, src, out, mode,
+        use_mute ? mute.get() : nullptr, d, taper, taper_len, sumsq);
+    CK(cudaGetLastError());
+  }
+
+  // Y = W F X  (window traces of the current model)
+  void forward_traces() {
+    for (size_t k = 0; k < fwd.size(); ++k) launch_axis(fwd[k], 1, kStore, 0, 0);
+    if (time_fwd.n_cta) {
+      time_c2r_ola<R><<<time_fwd.n_cta, kThreads, time_fwd.smem, stream>>>(
+          time_jobs.get(), time_fwd.cta_job.get(), time_fwd.cta_trace0.get(), time_fwd.nb,
+          d_descs.get(), d_tw.get());
+      CK(cudaGetLastError());
+    }
+    if (wavelets) launch_wavelet(+1);
+  }
+
+  void launch_wavelet(int direction) {
+    if (!wav.n_cta) return;
+    wavelet_apply<R><<<wav.n_cta, kThreads, wav.smem, stream>>>(
+        wav_jobs.get(), wav.cta_job.get(), wav.cta_trace0.get(), wav.nb, d_descs.get(),
+        d_tw.get(), spectra.get(), spec_off.get(), direction);
+    CK(cudaGetLastError());
+  }
+
+  // Z = F_t^H B^H W^H record, per window (before the space passes)
+  void adjoint_time(const R *record) {
+    if (wavelets) {
+      if (n_wtraces)
+        extract_traces<R><<<(unsigned)n_wtraces, kThreads, 0, stream>>>(
+            blend_rec.get(), blend_ts.get(), blend_n.get(), wt_dst.get(), wt_C.get(), record,
+            Y.get());
+      CK(cudaGetLastError());
+      launch_wavelet(-1);
+    }
+    if (time_adj.n_cta) {
+      time_r2c<R><<<time_adj.n_cta, kThreads, time_adj.smem, stream>>>(
+          time_jobs.get(), time_adj.cta_job.get(), time_adj.cta_trace0.get(), time_adj.nb,
+          d_descs.get(), d_tw.get(), record, wavelets ? 0 : 1);
+      CK(cudaGetLastError());
+    }
+  }
+
+  // X <- threshold(X - step * A^H record, lamb)
+  void adjoint_update(const R *record, R step, R lamb, bool track_max) {
+    adjoint_time(record);
+    for (size_t k = 0; k < adj_update.size(); ++k)
+      launch_axis(adj_update[k], 0, track_max ? kUpdateMax : kUpdateThreshold, step, lamb);
+  }
+
+  void residual(bool want_norm) {
+    double *ss = nullptr;
+    if (want_norm) {
+      CK(cudaMemsetAsync(dscalar.get(), 0, sizeof(double), stream));
+      ss = dscalar.get();
+    }
+    launch_gather(g_fwd, Y.get(), rec_r.get(), kGatherResidual, true, rec_d.get(), nullptr, 0,
+                  ss);
+  }
+
+  double read_dscalar() {
+    double v = 0;
+    CK(cudaMemcpyAsync(&v, dscalar.get(), sizeof(double), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    return v;
+  }
+
+  R read_scalar() {
+    R v = 0;
+    CK(cudaMemcpyAsync(&v, scalar.get(), sizeof(R), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    return v;
+  }
+
+  double record_norm(const R *rec) {
+    CK(cudaMemsetAsync(dscalar.get(), 0, sizeof(double), stream));
+    if (plan.record_size)
+      record_sumsq<R><<<grid_for(plan.record_size), kThreads, 0, stream>>>(
+          rec, plan.record_size, dscalar.get());
+    CK(cudaGetLastError());
+    return std::sqrt(read_dscalar());
+  }
+
+  static unsigned grid_for(long n) {
+    long g = (n + kThreads - 1) / kThreads;
+    return (unsigned)std::max<long>(1, std::min<long>(g, 148L * 16));
+  }
+
+  // 0.5 / max(1, max blended sum of the space tapers)   (src/model.c:1230-1312)
+  R compute_stepsize() {
+    for (size_t w = 0; w < plan.windows.size(); ++w) {
+      const WindowPlan &W = plan.windows[w];
+      const long n = (long)W.n_traces * W.C;
+      long base = 0;
+      for (size_t v = 0; v < w; ++v) base += plan.windows[v].n_traces;
+      if (n)
+        fill_traces<R><<<grid_for(n), kThreads, 0, stream>>>(Y.get() + trace_off[w],
+                                                             space_fold.get() + base,
+                                                             W.n_traces, W.C);
+      CK(cudaGetLastError());
+    }
+    launch_gather(g_fwd, Y.get(), rec_r.get(), kGatherSum, false, nullptr, nullptr, 0, nullptr);
+    R one = (R)1;
+    CK(cudaMemcpyAsync(scalar.get(), &one, sizeof(R), cudaMemcpyHostToDevice, stream));
+    if (plan.record_size)
+      record_max<R><<<grid_for(plan.record_size), kThreads, 0, stream>>>(
+          rec_r.get(), plan.record_size, scalar.get());
+    CK(cudaGetLastError());
+    const R factor = read_scalar();
+    stepsize = (R)0.5 / factor;
+    return stepsize;
+  }
+
+  void upload_data(R const *const *data) {
+    for (int p = 0; p < plan.n_patches; ++p) {
+      const long n = (long)plan.n_traces[p] * plan.n_times[p];
+      if (n)
+        CK(cudaMemcpyAsync(data_dev.get() + patch_off[p], data[p], n * sizeof(R),
+                           cudaMemcpyHostToDevice, stream));
+    }
+  }
+
+  void download_data(R *const *data) {
+    for (int p = 0; p < plan.n_patches; ++p) {
+      const long n = (long)plan.n_traces[p] * plan.n_times[p];
+      if (n)
+        CK(cudaMemcpyAsync(data[p], data_dev.get() + patch_off[p], n * sizeof(R),
+                           cudaMemcpyDeviceToHost, stream));
+    }
+    CK(cudaStreamSynchronize(stream));
+  }
+
+  // d = mute(mean blend of the patch data at the raw shot times)
+  void blend_input(const long *const *shottimes, const int *const *channels,
+                   const enum AGDTraceType *const *trace_types) {
+    if (g_input.n_chunk == 0 && plan.record_size) {
+      std::vector<Contrib> list;
+      for (int p = 0; p < plan.n_patches; ++p) {
+        const int nt = plan.n_times[p];
+        for (int t = 0; t < plan.n_traces[p]; ++t) {
+          const BlendCoord b = plan.coord_of(shottimes[p][t], nt, channels[p][t],
+                                             (int)trace_types[p][t]);
+          if (b.rec < 0) continue;
+          list.push_back(Contrib{b.rec, patch_off[p] + (long)t * nt + b.trace_start, b.n, 0});
+        }
+      }
+      set_input_gather(list);
+    }
+    launch_gather(g_input, data_dev.get(), rec_d.get(), kGatherMean, true, nullptr, nullptr, 0,
+                  nullptr);
+  }
+
+  void output() {
+    forward_traces();
+    if (out_traces)
+      output_gather<R><<<(unsigned)out_traces, kThreads, 0, stream>>>(
+          out_ptr.get(), out_src.get(), out_dst.get(), out_nt.get(), Y.get(), data_dev.get());
+    CK(cudaGetLastError());
+  }
+
+  // Initial step: x = -step * A^H d, lambda_0 = sqrt(max |x|^2)
+  R initial_step() {
+    if (plan.model_size) CK(cudaMemsetAsync(X.get(), 0, X.bytes(), stream));
+    CK(cudaMemsetAsync(scalar.get(), 0, sizeof(R), stream));
+    adjoint_update(rec_d.get(), stepsize, (R)0, true);
+    const R m = read_scalar();
+    return (R)std::sqrt(m);
+  }
+
+  void threshold_model(R lamb) {
+    if (plan.model_size)
+      model_threshold<R><<<grid_for(plan.model_size), kThreads, 0, stream>>>(
+          X.get(), plan.model_size, lamb);
+    CK(cudaGetLastError());
+  }
+
+  // the solver of agd_deblend (src/agdeblend.c:584-633)
+  void solve(R initial_factor, int n_its, int print_freq) {
+    R lamb = initial_step();
+    const Schedule sc = lambda_schedule(initial_factor, n_its);
+    const R linear_slope = sc.linear_slope * lamb;
+    lamb *= initial_factor;
+    threshold_model(lamb);
+    if (print_freq > 0) {
+      const double r = record_norm(rec_d.get());
+      std::printf("Iteration 0 Residual %f\n", r);
+    }
+    for (int it = 1; it < n_its; ++it) {
+      const bool print_residual = print_freq > 0 && it % print_freq == 0;
+      forward_traces();
+      residual(print_residual);
+      if (print_residual) std::printf("Iteration %d Residual %f\n", it, std::sqrt(read_dscalar()));
+      if (it < sc.first_linear_it)
+        lamb *= sc.decay;
+      else
+        lamb = (R)(n_its - 1 - it) * linear_slope;
+      adjoint_update(rec_r.get(), stepsize, lamb, false);
+    }
+    output();
+  }
+
+  // host <-> device model in the reference layout
+  void model_from_ref(const R *host) {
+    DevArray<C> tmp;
+    tmp.alloc(plan.model_size);
+    if (!plan.model_size) return;
+    CK(cudaMemcpyAsync(tmp.get(), host, tmp.bytes(), cudaMemcpyHostToDevice, stream));
+    for (const WindowPlan &W : plan.windows)
+      model_layout<R><<<grid_for(W.model_size), kThreads, 0, stream>>>(
+          tmp.get() + W.model_off, X.get() + W.model_off, W.T, W.F, W.plane(), 1);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream));
+  }
+
+  void model_to_ref(const C *dev, R *host) {
+    DevArray<C> tmp;
+    tmp.alloc(plan.model_size);
+    if (!plan.model_size) return;
+    for (const WindowPlan &W : plan.windows)
+      model_layout<R><<<grid_for(W.model_size), kThreads, 0, stream>>>(
+          dev + W.model_off, tmp.get() + W.model_off, W.T, W.F, W.plane(), 0);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(host, tmp.get(), tmp.bytes(), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+};
+
+using EngineR = Engine<real>;
+
+}  // namespace agd
+
+// ==================================================================== C API
+
+struct agd_gpu_problem {
+  std::unique_ptr<agd::EngineR> eng;
+  // kept for blend_input (raw shot times, channels, trace types)
+  std::vector<std::vector<long>> shottimes;
+  std::vector<std::vector<int>> channels;
+  std::vector<std::vector<AGDTraceType>> trace_types;
+  std::vector<const long *> st_p;
+  std::vector<const int *> ch_p;
+  std::vector<const AGDTraceType *> tt_p;
+
+  void input_blend() {
+    eng->blend_input(st_p.data(), ch_p.data(), tt_p.data());
+  }
+};
+
+namespace {
+
+agd::ProblemArgs make_args(int n_patches, int const *volumes, int const *n_dims,
+                           int const *const *window_shapes, int const *const *coords,
+                           int const *const *shapes, long int const *const *shottimes,
+                           int const *const *channels,
+                           enum AGDTraceType const *const *trace_types,
+                           int const *wavelet_lengths, int const *const *wavelet_idxs,
+                           AGD_TYPE const *const *wavelets) {
+  return agd::ProblemArgs{n_patches,  volumes,     n_dims,   window_shapes,
+                          coords,     shapes,      shottimes, channels,
+                          trace_types, wavelet_lengths, wavelet_idxs, wavelets};
+}
+
+int create_problem(const agd::ProblemArgs &a, agd_gpu_problem **out) {
+  *out = nullptr;
+  agd::Plan plan;
+  if (agd::build_plan(a, plan)) return 1;
+  auto *pb = new agd_gpu_problem();
+  try {
+    pb->shottimes.resize(a.n_patches);
+    pb->channels.resize(a.n_patches);
+    pb->trace_types.resize(a.n_patches);
+    for (int p = 0; p < a.n_patches; ++p) {
+      const int n = plan.n_traces[p];
+      pb->shottimes[p].assign(a.shottimes[p], a.shottimes[p] + n);
+      pb->channels[p].assign(a.channels[p], a.channels[p] + n);
+      pb->trace_types[p].assign(a.trace_types[p], a.trace_types[p] + n);
+      pb->st_p.push_back(pb->shottimes[p].data());
+      pb->ch_p.push_back(pb->channels[p].data());
+      pb->tt_p.push_back(pb->trace_types[p].data());
+    }
+    pb->eng.reset(new agd::EngineR(std::move(plan)));
+    pb->eng->compute_stepsize();
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "ERROR: %s\n", e.what());
+    delete pb;
+    return 1;
+  }
+  *out = pb;
+  return 0;
+}
+
+template <typename F>
+int guarded(const char *name, F &&f) {
+  try {
+    return f();
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "ERROR: %s\nERROR in %s\n", e.what(), name);
+    return 1;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int agd_gpu_problem_create(int n_patches, int const *volumes, int const *n_dims,
+                           int const *const *window_shapes, int const *const *coords,
+                           int const *const *shapes, long int const *const *shottimes,
+                           int const *const *channels,
+                           enum AGDTraceType const *const *trace_types,
+                           int const *wavelet_lengths, int const *const *wavelet_idxs,
+                           AGD_TYPE const *const *wavelets, agd_gpu_problem **problem) {
+  if (problem == nullptr) return 1;
+  const agd::ProblemArgs a =
+      make_args(n_patches, volumes, n_dims, window_shapes, coords, shapes, shottimes,
+                channels, trace_types, wavelet_lengths, wavelet_idxs, wavelets);
+  // Validation with a dummy non-null data array (data is checked per call).
+  std::vector<AGD_TYPE *> dummy(n_patches > 0 ? n_patches : 1, (AGD_TYPE *)1);
+  if (agd::check_deblend_inputs(a, (AGD_TYPE)1, 1, dummy.data())) return 1;
+  return create_problem(a, problem);
+}
+
+void agd_gpu_problem_destroy(agd_gpu_problem *problem) { delete problem; }
+
+int agd_gpu_problem_info(agd_gpu_problem const *pb, long int *info) {
+  if (pb == nullptr || info == nullptr) return 1;
+  const agd::EngineR &e = *pb->eng;
+  info[0] = (long)e.plan.windows.size();
+  info[1] = e.plan.model_size;
+  info[2] = e.plan.record_size;
+  info[3] = e.n_wtraces;
+  long segs = 0;
+  for (const auto &c : e.plan.intervals) segs += (long)c.size();
+  info[4] = segs;
+  info[5] = (long)e.plan.mute.size();
+  info[6] = (long)e.device_bytes();
+  info[7] = e.g_fwd.n_contrib;
+  return 0;
+}
+
+int agd_gpu_stepsize(agd_gpu_problem *pb, AGD_TYPE *stepsize) {
+  if (pb == nullptr || stepsize == nullptr) return 1;
+  *stepsize = pb->eng->stepsize;
+  return 0;
+}
+
+int agd_gpu_forward(agd_gpu_problem *pb, AGD_TYPE const *model, AGD_TYPE *record) {
+  if (pb == nullptr || model == nullptr || record == nullptr) return 1;
+  return guarded("agd_gpu_forward", [&] {
+    agd::EngineR &e = *pb->eng;
+    e.model_from_ref(model);
+    e.forward_traces();
+    e.launch_gather(e.g_fwd, e.Y.get(), e.rec_r.get(), agd::kGatherSum, true, nullptr, nullptr,
+                    0, nullptr);
+    if (e.plan.record_size)
+      agd::CK(cudaMemcpyAsync(record, e.rec_r.get(), e.rec_r.bytes(), cudaMemcpyDeviceToHost,
+                              e.stream));
+    agd::CK(cudaStreamSynchronize(e.stream));
+    return 0;
+  });
+}
+
+int agd_gpu_adjoint(agd_gpu_problem *pb, AGD_TYPE const *record, AGD_TYPE *model) {
+  if (pb == nullptr || model == nullptr || record == nullptr) return 1;
+  return guarded("agd_gpu_adjoint", [&] {
+    agd::EngineR &e = *pb->eng;
+    e.ensure_plain_adjoint();
+    if (e.plan.record_size)
+      agd::CK(cudaMemcpyAsync(e.rec_r.get(), record, e.rec_r.bytes(), cudaMemcpyHostToDevice,
+                              e.stream));
+    e.adjoint_time(e.rec_r.get());
+    for (size_t k = 0; k < e.adj_plain.size(); ++k)
+      e.launch_axis(e.adj_plain[k], 0, agd::kStore, 0, 0);
+    e.model_to_ref(e.G.get(), model);
+    return 0;
+  });
+}
+
+int agd_gpu_blend_input(agd_gpu_problem *pb, AGD_TYPE const *const *data, AGD_TYPE *record) {
+  if (pb == nullptr || data == nullptr || record == nullptr) return 1;
+  return guarded("agd_gpu_blend_input", [&] {
+    agd::EngineR &e = *pb->eng;
+    e.upload_data(data);
+    pb->input_blend();
+    if (e.plan.record_size)
+      agd::CK(cudaMemcpyAsync(record, e.rec_d.get(), e.rec_d.bytes(), cudaMemcpyDeviceToHost,
+                              e.stream));
+    agd::CK(cudaStreamSynchronize(e.stream));
+    return 0;
+  });
+}
+
+int agd_gpu_set_output(agd_gpu_problem *pb, AGD_TYPE const *model, AGD_TYPE *const *data) {
+  if (pb == nullptr || model == nullptr || data == nullptr) return 1;
+  return guarded("agd_gpu_set_output", [&] {
+    agd::EngineR &e = *pb->eng;
+    e.model_from_ref(model);
+    e.output();
+    e.download_data(data);
+    return 0;
+  });
+}
+
+int agd_gpu_solve(agd_gpu_problem *pb, AGD_TYPE initial_factor, int n_its, int print_freq,
+                  AGD_TYPE *const *data) {
+  if (pb == nullptr || data == nullptr) return 1;
+  if (n_its <= 0) {
+    std::fprintf(stderr, "ERROR: n_its must be > 0\n");
+    return 1;
+  }
+  return guarded("agd_deblend", [&] {
+    agd::EngineR &e = *pb->eng;
+    e.upload_data(data);
+    pb->input_blend();
+    e.solve(initial_factor, n_its, print_freq);
+    e.download_data(data);
+    return 0;
+  });
+}
+
+int agd_gpu_time_iterations(agd_gpu_problem *pb, AGD_TYPE const *const *data,
+                            AGD_TYPE initial_factor, int n_its, int warmup, int steps,
+                            double *timing) {
+  if (pb == nullptr || data == nullptr || timing == nullptr || steps <= 0 || n_its < 2)
+    return 1;
+  return guarded("agd_gpu_time_iterations", [&] {
+    agd::EngineR &e = *pb->eng;
+    e.upload_data(data);
+    pb->input_blend();
+    AGD_TYPE lamb = e.initial_step();
+    const agd::Schedule sc = agd::lambda_schedule(initial_factor, n_its);
+    const AGD_TYPE slope = sc.linear_slope * lamb;
+    lamb *= initial_factor;
+    e.threshold_model(lamb);
+    auto lamb_at = [&](int it) {
+      AGD_TYPE l = lamb;
+      for (int k = 1; k <= it; ++k) l = k < sc.first_linear_it ? l * sc.decay : (AGD_TYPE)(n_its - 1 - k) * slope;
+      return l;
+    };
+    int it = 1;
+    auto iterate = [&] {
+      e.forward_traces();
+      e.residual(false);
+      e.adjoint_update(e.rec_r.get(), e.stepsize, lamb_at(it), false);
+      it = it + 1 < n_its ? it + 1 : 1;
+    };
+    for (int i = 0; i < warmup; ++i) iterate();
+    cudaEvent_t ev[4];
+    for (auto &v : ev) agd::CK(cudaEventCreate(&v));
+    agd::CK(cudaEventRecord(ev[0], e.stream));
+    for (int i = 0; i < steps; ++i) iterate();
+    agd::CK(cudaEventRecord(ev[1], e.stream));
+    // one more iteration split into its forward and adjoint halves
+    agd::CK(cudaEventRecord(ev[2], e.stream));
+    e.forward_traces();
+    e.residual(false);
+    agd::CK(cudaEventRecord(ev[3], e.stream));
+    agd::CK(cudaEventSynchronize(ev[3]));
+    float ms_total = 0, ms_fwd = 0;
+    agd::CK(cudaEventElapsedTime(&ms_total, ev[0], ev[1]));
+    agd::CK(cudaEventElapsedTime(&ms_fwd, ev[2], ev[3]));
+    agd::CK(cudaEventRecord(ev[2], e.stream));
+    e.adjoint_update(e.rec_r.get(), e.stepsize, lamb_at(it), false);
+    agd::CK(cudaEventRecord(ev[3], e.stream));
+    agd::CK(cudaEventSynchronize(ev[3]));
+    float ms_adj = 0;
+    agd::CK(cudaEventElapsedTime(&ms_adj, ev[2], ev[3]));
+    for (auto &v : ev) cudaEventDestroy(v);
+    timing[0] = ms_total;
+    timing[1] = ms_fwd;
+    timing[2] = ms_adj;
+    timing[3] = steps;
+    return 0;
+  });
+}
+
+int agd_gpu_profile_iteration(agd_gpu_problem *pb, AGD_TYPE lamb, double *ms) {
+  if (pb == nullptr || ms == nullptr) return 1;
+  return guarded("agd_gpu_profile_iteration", [&] {
+    agd::EngineR &e = *pb->eng;
+    for (int i = 0; i < 16; ++i) ms[i] = 0.0;
+    std::vector<cudaEvent_t> ev;
+    auto mark = [&] {
+      cudaEvent_t v;
+      agd::CK(cudaEventCreate(&v));
+      agd::CK(cudaEventRecord(v, e.stream));
+      ev.push_back(v);
+    };
+    const int nf = (int)e.fwd.size();
+    mark();
+    for (int k = 0; k < nf; ++k) {
+      e.launch_axis(e.fwd[k], 1, agd::kStore, 0, 0);
+      mark();
+    }
+    if (e.time_fwd.n_cta)
+      agd::time_c2r_ola<AGD_TYPE><<<e.time_fwd.n_cta, agd::kThreads, e.time_fwd.smem,
+                                    e.stream>>>(e.time_jobs.get(), e.time_fwd.cta_job.get(),
+                                                e.time_fwd.cta_trace0.get(), e.time_fwd.nb,
+                                                e.d_descs.get(), e.d_tw.get());
+    mark();
+    if (e.wavelets) e.launch_wavelet(+1);
+    mark();
+    e.residual(false);
+    mark();
+    e.adjoint_time(e.rec_r.get());
+    mark();
+    for (int k = 0; k < nf; ++k) {
+      e.launch_axis(e.adj_update[k], 0, agd::kUpdateThreshold, e.stepsize, lamb);
+      mark();
+    }
+    agd::CK(cudaEventSynchronize(ev.back()));
+    auto dt = [&](int a, int b) {
+      float v = 0;
+      agd::CK(cudaEventElapsedTime(&v, ev[a], ev[b]));
+      return (double)v;
+    };
+    // [0] forward space passes, [1] time c2r + overlap-add, [2] wavelet
+    // forward, [3] blend gather + residual, [4] adjoint time (incl. gather
+    // and wavelet), [5] adjoint space passes incl. update, [6..9] forward
+    // passes by index, [10..13] adjoint passes by index, [14] passes count
+    for (int k = 0; k < nf && k < 4; ++k) ms[6 + k] = dt(k, k + 1);
+    ms[0] = dt(0, nf);
+    ms[1] = dt(nf, nf + 1);
+    ms[2] = dt(nf + 1, nf + 2);
+    ms[3] = dt(nf + 2, nf + 3);
+    ms[4] = dt(nf + 3, nf + 4);
+    for (int k = 0; k < nf && k < 4; ++k) ms[10 + k] = dt(nf + 4 + k, nf + 5 + k);
+    ms[5] = dt(nf + 4, nf + 4 + nf);
+    ms[14] = nf;
+    for (auto v : ev) cudaEventDestroy(v);
+    return 0;
+  });
+}
+
+int agd_plan_export(int n_patches, int const *volumes, int const *n_dims,
+                    int const *const *window_shapes, int const *const *coords,
+                    int const *const *shapes, long int const *const *shottimes,
+                    int const *const *channels, enum AGDTraceType const *const *trace_types,
+                    int const *wavelet_lengths, int const *const *wavelet_idxs,
+                    AGD_TYPE const *const *wavelets, long int *info, int *win,
+                    long int *blend) {
+  if (info == nullptr) return 1;
+  const agd::ProblemArgs a =
+      make_args(n_patches, volumes, n_dims, window_shapes, coords, shapes, shottimes,
+                channels, trace_types, wavelet_lengths, wavelet_idxs, wavelets);
+  std::vector<AGD_TYPE *> dummy(n_patches > 0 ? n_patches : 1, (AGD_TYPE *)1);
+  if (agd::check_deblend_inputs(a, (AGD_TYPE)1, 1, dummy.data())) return 1;
+  agd::Plan plan;
+  if (agd::build_plan(a, plan)) return 1;
+  long ntr = 0;
+  for (const auto &w : plan.windows) ntr += w.n_traces;
+  long segs = 0;
+  for (const auto &c : plan.intervals) segs += (long)c.size();
+  info[0] = (long)plan.windows.size();
+  info[1] = plan.model_size;
+  info[2] = plan.record_size;
+  info[3] = ntr;
+  info[4] = segs;
+  info[5] = (long)plan.mute.size();
+  info[6] = 0;
+  info[7] = 0;
+  if (win != nullptr) {
+    for (size_t i = 0; i < plan.windows.size(); ++i) {
+      const agd::WindowPlan &w = plan.windows[i];
+      int *o = win + 32 * i;
+      std::memset(o, 0, 32 * sizeof(int));
+      o[0] = w.patch;
+      o[1] = w.D;
+      o[2] = w.T;
+      o[3] = w.F;
+      o[4] = w.Lt;
+      o[5] = w.Pt;
+      o[6] = w.h;
+      o[7] = w.n_fk;
+      o[8] = w.C;
+      o[9] = w.n_traces;
+      for (int d = 0; d < w.D; ++d) {
+        o[10 + d] = w.L[d];
+        o[14 + d] = w.P[d];
+      }
+      for (int k = 0; k < 2 * w.D + 2; ++k) o[18 + k] = w.use_taper[k];
+    }
+  }
+  if (blend != nullptr) {
+    long k = 0;
+    for (const auto &w : plan.windows)
+      for (const auto &b : w.blend) {
+        blend[3 * k] = b.rec;
+        blend[3 * k + 1] = b.trace_start;
+        blend[3 * k + 2] = b.n;
+        ++k;
+      }
+  }
+  return 0;
+}
+
+int agd_deblend(int n_patches, int const *volumes, int const *n_dims,
+                int const *const *window_shapes, int const *const *coords,
+                int const *const *shapes, long int const *const *shottimes,
+                int const *const *channels, enum AGDTraceType const *const *trace_types,
+                int const *wavelet_lengths, int const *const *wavelet_idxs,
+                AGD_TYPE const *const *wavelets, AGD_TYPE const initial_factor, int n_its,
+                int print_freq, AGD_TYPE *const *data) {
+  const agd::ProblemArgs a =
+      make_args(n_patches, volumes, n_dims, window_shapes, coords, shapes, shottimes,
+                channels, trace_types, wavelet_lengths, wavelet_idxs, wavelets);
+  if (agd::check_deblend_inputs(a, initial_factor, n_its, data)) {
+    std::fprintf(stderr, "ERROR in agd_deblend\n");
+    return 1;
+  }
+  agd_gpu_problem *pb = nullptr;
+  if (create_problem(a, &pb)) {
+    std::fprintf(stderr, "ERROR in agd_deblend\n");
+    return 1;
+  }
+  if (pb->eng->stepsize > (AGD_TYPE)0.3)
+    std::printf("WARNING: There does not appear to be any overlap between shots\n");
+  const int rc = agd_gpu_solve(pb, initial_factor, n_its, print_freq, data);
+  delete pb;
+  return rc;
+}
+
+}  // extern "C"

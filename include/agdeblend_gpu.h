@@ -1,0 +1,107 @@
+/*
+ * Extension API of the B200 implementation (not in the reference).
+ *
+ * The reference keeps all state inside one agd_deblend call.  These entry
+ * points expose the same planning and operators on a persistent problem
+ * handle so that callers (tests, benchmarks, batch drivers) can apply the
+ * operator A = mute . blend . wavelet . FK and its adjoint, or run the solver,
+ * without re-planning.  Every function returns 0 on success and 1 on failure
+ * with a message on stderr, like the reference.
+ *
+ * Layouts at this boundary are the reference's:
+ *   model   every window's [n_time_windows][padded space...][padded_time/2+1]
+ *           complex (interleaved re, im), windows in the reference's order
+ *           (allocate_model_fk, reference src/model.c:1160-1185);
+ *   record  every (channel, interval) segment of the blend configuration,
+ *           channel-major (allocate_blended, reference src/blend.c:796-829).
+ */
+#ifndef AGD_GPU_H
+#define AGD_GPU_H
+
+#include "agdeblend.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct agd_gpu_problem agd_gpu_problem;
+
+/* Validates and plans a problem (the arguments of agd_deblend up to the
+ * wavelets) and uploads its tables to the current device.  Replaces the
+ * set-up half of agd_deblend: check_deblend_inputs + set_model +
+ * get_stepsize (reference src/agdeblend.c:548-576). */
+int agd_gpu_problem_create(int n_patches, int const *volumes, int const *n_dims,
+                           int const *const *window_shapes, int const *const *coords,
+                           int const *const *shapes, long int const *const *shottimes,
+                           int const *const *channels,
+                           enum AGDTraceType const *const *trace_types,
+                           int const *wavelet_lengths, int const *const *wavelet_idxs,
+                           AGD_TYPE const *const *wavelets, agd_gpu_problem **problem);
+
+void agd_gpu_problem_destroy(agd_gpu_problem *problem);
+
+/* info[0] windows, [1] model complex elements, [2] record samples,
+ * [3] window traces (all windows), [4] record segments, [5] mute spans,
+ * [6] device bytes held, [7] blend contributions per forward. */
+int agd_gpu_problem_info(agd_gpu_problem const *problem, long int *info);
+
+/* Step size 0.5 / max blend fold (reference get_stepsize, src/model.c:1230-1312). */
+int agd_gpu_stepsize(agd_gpu_problem *problem, AGD_TYPE *stepsize);
+
+/* record = A model (reference model_forward, src/model.c:1067-1114). */
+int agd_gpu_forward(agd_gpu_problem *problem, AGD_TYPE const *model, AGD_TYPE *record);
+
+/* model = A^H record (reference model_adjoint_update with step -1 on a zero
+ * model, src/model.c:1116-1157). */
+int agd_gpu_adjoint(agd_gpu_problem *problem, AGD_TYPE const *record, AGD_TYPE *model);
+
+/* record = mute(mean-blend(data)) (reference blend_input, src/blend.c:1294-1335). */
+int agd_gpu_blend_input(agd_gpu_problem *problem, AGD_TYPE const *const *data,
+                        AGD_TYPE *record);
+
+/* data = sum over windows of W F model (reference set_output,
+ * src/model.c:1425-1515). */
+int agd_gpu_set_output(agd_gpu_problem *problem, AGD_TYPE const *model,
+                       AGD_TYPE *const *data);
+
+/* The solver of agd_deblend on a planned problem: data is the blended input
+ * and receives the deblended output (reference src/agdeblend.c:578-633). */
+int agd_gpu_solve(agd_gpu_problem *problem, AGD_TYPE initial_factor, int n_its,
+                  int print_freq, AGD_TYPE *const *data);
+
+/* Benchmark hook: loads `data`, runs the set-up step, then `warmup` untimed
+ * and `steps` timed ISTA iterations with every input resident on the device.
+ * Timing uses CUDA events on the library's stream.  timing[0] = total ms of
+ * the timed iterations, timing[1] = ms of the forward half, timing[2] = ms of
+ * the adjoint half (separately timed pass), timing[3] = iterations timed. */
+int agd_gpu_time_iterations(agd_gpu_problem *problem, AGD_TYPE const *const *data,
+                            AGD_TYPE initial_factor, int n_its, int warmup, int steps,
+                            double *timing);
+
+/* Benchmark hook: one ISTA iteration on the current device state with CUDA
+ * events between its launch groups (call after agd_gpu_time_iterations).
+ * ms[0] forward space passes, [1] time c2r + overlap-add, [2] wavelet
+ * forward, [3] blend gather + residual, [4] adjoint time axis (with its
+ * record gather and wavelet), [5] adjoint space passes with the update,
+ * [6..9] forward passes by index, [10..13] adjoint passes by index,
+ * [14] number of space passes. */
+int agd_gpu_profile_iteration(agd_gpu_problem *problem, AGD_TYPE lamb, double *ms);
+
+/* Host planning only (no device use): writes the plan's size summary
+ * (info layout as agd_gpu_problem_info, [6] and [7] zero) and, when the
+ * arrays are non-NULL, per window `win` (32 ints each: patch, D, T, F, Lt,
+ * Pt, h, n_fk, C, n_traces, L[4], P[4], use_taper[10]), per window trace
+ * `blend` (3 longs each: record start or -1, trace start, samples). */
+int agd_plan_export(int n_patches, int const *volumes, int const *n_dims,
+                    int const *const *window_shapes, int const *const *coords,
+                    int const *const *shapes, long int const *const *shottimes,
+                    int const *const *channels, enum AGDTraceType const *const *trace_types,
+                    int const *wavelet_lengths, int const *const *wavelet_idxs,
+                    AGD_TYPE const *const *wavelets, long int *info, int *win,
+                    long int *blend);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,121 @@
+"""End-to-end GPU parity of agd_deblend / agd_blend through the public C API.
+
+Gates: the deblended output after the same n_its is within 1e-3 relative L2
+of the float64 oracle (and of the reference's own float output where it was
+recorded), and its SNR against the unblended truth matches to 0.05 dB.  The
+reference-style quality test repeats src/test.cpp:432-561 (five random
+problems, 800 iterations, error energy below a tenth of the signal energy).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import agd_oracle as O
+import agdeblend_b200 as A
+from agdeblend_b200 import synthetic as S
+from conftest import ROOT, rel_l2
+from problems import random_problem
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def _plan(sv):
+    return O.make_plan(sv.volumes, sv.n_dims, sv.window_shapes, sv.coords, sv.shapes,
+                       sv.shottimes, sv.channels, sv.trace_types, sv.wavelet_lengths,
+                       sv.wavelet_idxs, sv.wavelets)
+
+
+def _deblend(sv, n_its=None):
+    return A.deblend(sv.volumes, sv.window_shapes, sv.coords, sv.shottimes, sv.channels,
+                     sv.trace_types, sv.initial_factor, n_its or sv.n_its, 0, sv.data,
+                     wavelet_idxs=sv.wavelet_idxs, wavelets=sv.wavelets)
+
+
+def test_gather_2d_full_vs_oracle():
+    """The 128-shot x 512-sample gather, window (32, 256), 100 iterations."""
+    sv = S.gather_2d()
+    out = _deblend(sv)
+    ref = O.deblend(_plan(sv), sv.data, sv.initial_factor, sv.n_its)
+    assert rel_l2(out[0], ref[0]) <= 1e-3
+    snr_gpu = S.snr_db(out, sv.truth, sv.trace_types)
+    snr_ref = S.snr_db(ref, sv.truth, sv.trace_types)
+    assert abs(snr_gpu - snr_ref) <= 0.05
+    path = os.path.join(GOLDEN, "gather_2d_deblend.npz")
+    if os.path.exists(path):
+        g = np.load(path)
+        assert rel_l2(out[0], g["reference_out"]) <= 1e-3
+        assert abs(snr_gpu - float(g["reference_snr_db"])) <= 0.05
+
+
+@pytest.mark.parametrize("name", ["two_volume_3d", "vibroseis_4d"])
+def test_small_surveys_vs_oracle(small_surveys, name):
+    sv = small_surveys[name]
+    out = _deblend(sv)
+    ref = O.deblend(_plan(sv), sv.data, sv.initial_factor, sv.n_its)
+    for o, r in zip(out, ref):
+        assert rel_l2(o, r) <= 1e-3
+    assert abs(S.snr_db(out, sv.truth, sv.trace_types) -
+               S.snr_db(ref, sv.truth, sv.trace_types)) <= 0.05
+
+
+def test_double_library_vs_oracle(small_surveys):
+    sv = small_surveys["two_volume_3d"]
+    data64 = [d.astype(np.float64) for d in sv.data]
+    out = A.deblend(sv.volumes, sv.window_shapes, sv.coords, sv.shottimes, sv.channels,
+                    sv.trace_types, sv.initial_factor, sv.n_its, 0, data64)
+    ref = O.deblend(_plan(sv), sv.data, sv.initial_factor, sv.n_its)
+    for o, r in zip(out, ref):
+        assert o.dtype == np.float64
+        assert rel_l2(o, r) <= 1e-9
+
+
+def test_reference_quality_random_problems():
+    """src/test.cpp:432-561: blend random problems, deblend 800 iterations."""
+    for k in range(5):
+        sv = random_problem(500 + k, bad_missing=False, max_dims=4)
+        rng = np.random.default_rng(600 + k)
+        truth = []
+        for d in sv.data:
+            nt = d.shape[-1]
+            tv = (rng.uniform(size=nt) - 0.5).astype(np.float32)
+            truth.append(np.broadcast_to(tv, d.shape).copy())
+        nts = [d.shape[-1] for d in truth]
+        blended = A.blend(sv.shottimes, sv.channels, sv.trace_types,
+                          [t.reshape(-1, n) for t, n in zip(truth, nts)], A.AGDBlendSum)
+        data = [b.reshape(t.shape) for b, t in zip(blended, truth)]
+        out = A.deblend(sv.volumes, sv.window_shapes, sv.coords, sv.shottimes, sv.channels,
+                        sv.trace_types, 1.0, 800, 0, data)
+        err = sum(float(np.sum((o - t) ** 2)) for o, t in zip(out, truth))
+        tru = sum(float(np.sum(t ** 2)) for t in truth)
+        assert err < tru / 10
+
+
+@pytest.mark.parametrize("mode", [A.AGDBlendSum, A.AGDBlendMean, A.AGDBlendOverwrite])
+@pytest.mark.parametrize("taper", [0, 5])
+def test_blend_vs_oracle(mode, taper):
+    sv = random_problem(700 + mode, bad_missing=True)
+    nts = [d.shape[-1] for d in sv.data]
+    flat = [d.reshape(-1, n) for d, n in zip(sv.data, nts)]
+    rng = np.random.default_rng(mode)
+    st_out = [s + rng.integers(-3, 4, s.shape) for s in sv.shottimes]
+    tt_out = [np.where(t == 1, 0, t).astype(np.int32) for t in sv.trace_types]
+    nt_out = [n + 2 for n in nts]
+    out = A.blend(sv.shottimes, sv.channels, sv.trace_types, flat, mode, taper_length=taper,
+                  n_times_out=nt_out, shottimes_out=st_out, channels_out=sv.channels,
+                  trace_types_out=tt_out)
+    ref = O.blend(nts, sv.shottimes, sv.channels, sv.trace_types, flat, mode, taper, nt_out,
+                  st_out, sv.channels, tt_out)
+    for o, r in zip(out, ref):
+        assert rel_l2(o.reshape(r.shape), r) <= 1e-6
+
+
+def test_print_freq_lines(capfd):
+    sv = S.gather_2d(seed=5, n_shots=32, nt=256, window=(16, 128))
+    A.deblend(sv.volumes, sv.window_shapes, sv.coords, sv.shottimes, sv.channels,
+              sv.trace_types, 1.0, 6, 2, sv.data)
+    out = capfd.readouterr().out
+    lines = [ln for ln in out.splitlines() if ln.startswith("Iteration")]
+    assert [ln.split()[1] for ln in lines] == ["0", "2", "4"]
