@@ -466,6 +466,7 @@ class Engine {
           j.n_out = W.P[a];
           j.fft = fft.get(W.P[a]);
           const bool last = (k == W.D - 1);
+          j.last = last ? 1 : 0;
           j.dst = last ? X.get() + W.model_off : Sb[(W.D + k) & 1] + W.model_off;
           ju.push_back(j);
           j.dst = last ? nullptr : Sb[(W.D + k) & 1] + W.model_off;  // G set lazily
@@ -667,15 +668,9 @@ class Engine {
 
   // 0.5 / max(1, max blended sum of the space tapers)   (src/model.c:1230-1312)
   R compute_stepsize() {
-    for (size_t w = 0; w < plan.windows.size(); ++w) {
-      const WindowPlan &W = plan.windows[w];
-      const long n = (long)W.n_traces * W.C;
-      long base = 0;
-      for (size_t v = 0; v < w; ++v) base += plan.windows[v].n_traces;
-      if (n)
-        fill_traces<R><<<grid_for(n), kThreads, 0, stream>>>(Y.get() + trace_off[w],
-                                                             space_fold.get() + base,
-                                                             W.n_traces, W.C);
+    if (n_wtraces) {
+      fill_traces<R><<<(unsigned)std::min<long>(n_wtraces, 148L * 64), kThreads, 0, stream>>>(
+          Y.get(), space_fold.get(), wt_dst.get(), wt_C.get(), n_wtraces);
       CK(cudaGetLastError());
     }
     launch_gather(g_fwd, Y.get(), rec_r.get(), kGatherSum, false, nullptr, nullptr, 0, nullptr);

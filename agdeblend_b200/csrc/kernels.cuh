@@ -36,6 +36,7 @@ struct AxisJob {
   int n_in;   // elements per line read (zero-padded up to the FFT length)
   int n_out;  // elements per line written (first n_out of the FFT output)
   int fft;    // FftDesc index
+  int last;   // 1: the window's final pass, which takes the launch's epilogue
 };
 
 enum AxisEpilogue : int {
@@ -189,6 +190,7 @@ __global__ void __launch_bounds__(kThreads)
   const FftDesc &d = descs[job.fft];
   const int n = d.n;
   const long lines = job.outer * job.inner;
+  const int epi = job.last ? epilogue : (int)kStore;  // block-uniform
   const long q0 = cta_line0[blockIdx.x];
   const int nl = (int)((lines - q0) < lines_per_cta ? (lines - q0) : lines_per_cta);
   C *a = reinterpret_cast<C *>(smem_raw);
@@ -235,14 +237,14 @@ __global__ void __launch_bounds__(kThreads)
     const long r = q - o * inner;
     const long di = (o * job.n_out + e) * inner + r;
     const C g = res[(long)i * n + e];
-    if (epilogue == kStore) {
+    if (epi == kStore) {
       job.dst[di] = g;
     } else {
       // x <- x - step * g   (src/model.c:1149-1154), then threshold
       const C x = job.dst[di];
       C xn = cmake<C>(sub_rn<R>(x.x, mul_rn<R>(step, g.x)),
                       sub_rn<R>(x.y, mul_rn<R>(step, g.y)));
-      if (epilogue == kUpdateThreshold) {
+      if (epi == kUpdateThreshold) {
         xn = soft_threshold<R>(xn, lamb, lamb_sq);
       } else {
         const R a2 = abs_sq<R>(xn);
@@ -251,7 +253,7 @@ __global__ void __launch_bounds__(kThreads)
       job.dst[di] = xn;
     }
   }
-  if (epilogue == kUpdateMax) {
+  if (epi == kUpdateMax) {
     __shared__ R red[32];
     const R m = block_max<R>(local_max, red);
     if (threadIdx.x == 0) atomic_max_nonneg(max_out, m);
@@ -518,13 +520,16 @@ __global__ void __launch_bounds__(kThreads)
     dst[t] = (r >= 0 && t >= s && t < s + m) ? record[r + (t - s)] : (R)0;
 }
 
-// Traces of per-trace constants (the stepsize probe, src/model.c:1239-1276).
+// Traces of per-trace constants (the stepsize probe, src/model.c:1239-1276):
+// trace k (of every window) gets value[k] at y[dst[k] .. dst[k] + len[k]).
 template <typename R>
-__global__ void fill_traces(R *y, const R *__restrict__ value, long n_traces, int C) {
-  const long n = n_traces * C;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (long)gridDim.x * blockDim.x)
-    y[i] = value[i / C];
+__global__ void fill_traces(R *y, const R *__restrict__ value, const long *__restrict__ dst,
+                            const int *__restrict__ len, long n_traces) {
+  for (long k = blockIdx.x; k < n_traces; k += gridDim.x) {
+    const R v = value[k];
+    R *row = y + dst[k];
+    for (int t = threadIdx.x; t < len[k]; t += blockDim.x) row[t] = v;
+  }
 }
 
 template <typename R>

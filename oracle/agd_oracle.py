@@ -582,10 +582,17 @@ def set_output(plan: Plan, x: list) -> list:
     return [d.reshape(plan.shapes[p]) for p, d in enumerate(data)]
 
 
-def lambda_schedule(initial_factor: float, n_its: int):
-    """(decay, first_linear_it, linear_slope / lambda_0) evaluated in single
-    precision with the C library's expf/logf/powf, as the float build of the
-    reference does (src/agdeblend.c:526-533)."""
+def lambda_schedule(initial_factor: float, n_its: int, double: bool = False):
+    """(decay, first_linear_it, linear_slope / lambda_0) evaluated as the
+    reference does (src/agdeblend.c:526-533): in single precision with the C
+    library's expf/logf/powf for the float build, in double precision for the
+    double build."""
+    if double:
+        decay = math.exp(math.log(TARGET_LAMB / initial_factor) / n_its)
+        ld = math.log(decay)
+        fli = int((ld * (n_its - 1.0) + 1.0) / ld)
+        slope = initial_factor * decay ** fli / (n_its - 1 - fli)
+        return decay, fli, slope
     f32 = np.float32
     f = f32(initial_factor)
     decay = _libm.expf(f32(_libm.logf(f32(f32(TARGET_LAMB) / f)) / f32(n_its)))
@@ -596,9 +603,9 @@ def lambda_schedule(initial_factor: float, n_its: int):
     return float(decay), fli, float(slope)
 
 
-def lambdas(lamb0: float, initial_factor: float, n_its: int) -> list:
+def lambdas(lamb0: float, initial_factor: float, n_its: int, double: bool = False) -> list:
     """Threshold used after the initial step and after each iteration."""
-    decay, fli, slope = lambda_schedule(initial_factor, n_its)
+    decay, fli, slope = lambda_schedule(initial_factor, n_its, double)
     slope *= lamb0
     lamb = lamb0 * initial_factor
     out = [lamb]
@@ -612,14 +619,15 @@ def lambdas(lamb0: float, initial_factor: float, n_its: int) -> list:
 
 
 def deblend(plan: Plan, data: list, initial_factor: float, n_its: int,
-            callback=None) -> list:
-    """agd_deblend's solver (src/agdeblend.c:584-633) in float64."""
+            callback=None, double_schedule: bool = False) -> list:
+    """agd_deblend's solver (src/agdeblend.c:584-633) in float64; the
+    threshold schedule follows the float (default) or the double build."""
     d = blend_input(plan, data)
     step = plan.step
     x = [-step * g for g in adjoint(plan, d)]
     lamb0 = math.sqrt(max(float(np.max(xw.real ** 2 + xw.imag ** 2)) if xw.size else 0.0
                           for xw in x))
-    lams = lambdas(lamb0, initial_factor, n_its)
+    lams = lambdas(lamb0, initial_factor, n_its, double_schedule)
     x = threshold(x, lams[0])
     for it in range(1, n_its):
         r = forward(plan, x) - d

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <string>
@@ -98,9 +99,22 @@ inline void expect_near(double a, double b, double tol, const char *sa,
   }
 }
 
+// MINI_GTEST_SKIP: comma-separated Suite.Name entries to skip.
+inline bool skipped(const Case &c) {
+  const char *env = std::getenv("MINI_GTEST_SKIP");
+  if (env == nullptr) return false;
+  const std::string full = std::string(c.suite) + "." + c.name;
+  const std::string list = std::string(",") + env + ",";
+  return list.find("," + full + ",") != std::string::npos;
+}
+
 inline int run_all() {
   int failed_cases = 0;
   for (const Case &c : registry()) {
+    if (skipped(c)) {
+      std::printf("[ SKIPPED] %s.%s\n", c.suite, c.name);
+      continue;
+    }
     long const before = failures();
     c.fn();
     bool const ok = failures() == before;
