@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -16,6 +17,7 @@
 #include <vector>
 
 #include "agdeblend_gpu.h"
+#include "fast.cuh"
 #include "kernels.cuh"
 #include "plan.hpp"
 
@@ -183,6 +185,33 @@ class Engine {
 
   std::vector<AxisLaunch> fwd, adj_update, adj_plain;
   TimeLaunch time_fwd, time_adj, wav;
+
+  // shape-specialised path (fast.cuh), used when every window has the same
+  // space and time FFT lengths and an instantiation exists
+  using SpaceFwdFn = void (*)(const PlaneJob<R> *, const int *, const long *, const long *, int);
+  using SpaceAdjFn = void (*)(const PlaneJob<R> *, const int *, const long *, const long *, int,
+                              int, R, R, R *);
+  using TimeFwdFn = void (*)(const TimeJob<R> *, const int *, const int *, int);
+  using TimeAdjFn = void (*)(const TimeJob<R> *, const int *, const int *, int, const R *, int);
+  struct PlaneLaunch {
+    DevArray<PlaneJob<R>> jobs;
+    DevArray<int> cta_job;
+    DevArray<long> cta_plane0;
+    DevArray<long> job_planes;
+    int n_cta = 0;
+    int np = 0;
+    size_t smem = 0;
+  };
+  bool fast = false;
+  SpaceFwdFn sp_fwd = nullptr;
+  SpaceAdjFn sp_adj = nullptr;
+  TimeFwdFn tm_fwd = nullptr;
+  TimeAdjFn tm_adj = nullptr;
+  int plane_smem = 0;   // complex per plane in shared memory
+  int first_lines = 1;  // lines per plane of the first space pass
+  PlaneLaunch pl_fwd, pl_adj, pl_adj_plain;
+  TimeLaunch tf_fast, ta_fast;
+  DevArray<TimeJob<R>> time_jobs_fast;
   GatherLaunch g_fwd, g_input;
   std::vector<long> trace_off;   // per window, in reals
   std::vector<long> patch_off;   // per patch, in reals
@@ -276,6 +305,119 @@ class Engine {
     L.smem = per_trace * nb;
   }
 
+  template <int D, int P0, int P1, int P2>
+  bool space_case(const WindowPlan &W) {
+    const int P[3] = {P0, P1, P2};
+    if (W.D != D) return false;
+    for (int d = 0; d < D; ++d)
+      if (W.P[d] != P[d]) return false;
+    sp_fwd = space_fwd_fast<R, D, P0, P1, P2>;
+    sp_adj = space_adj_fast<R, D, P0, P1, P2>;
+    plane_smem = PlaneShape<D, P0, P1, P2>::size;
+    first_lines = D == 1 ? 1 : (D == 2 ? P0 : P0 * P1);
+    return true;
+  }
+
+  bool pick_fast() {
+    if (plan.windows.empty()) return false;
+    const char *env = std::getenv("AGD_GPU_GENERIC");
+    if (env != nullptr && env[0] == '1') return false;
+    const WindowPlan &W0 = plan.windows[0];
+    for (const WindowPlan &W : plan.windows) {
+      if (W.D != W0.D || W.Pt != W0.Pt || W.Lt != W0.Lt || W.Lt % 2 != 0) return false;
+      for (int d = 0; d < W.D; ++d)
+        if (W.P[d] != W0.P[d]) return false;
+    }
+    const bool space = space_case<1, 40, 1, 1>(W0) || space_case<1, 20, 1, 1>(W0) ||
+                       space_case<2, 20, 40, 1>(W0) || space_case<2, 20, 20, 1>(W0) ||
+                       space_case<2, 40, 40, 1>(W0) || space_case<3, 20, 20, 20>(W0);
+    if (!space) return false;
+    if (W0.Pt == 320) {
+      tm_fwd = time_fwd_fast<R, 16, 10>;
+      tm_adj = time_adj_fast<R, 16, 10>;
+    } else if (W0.Pt == 160) {
+      tm_fwd = time_fwd_fast<R, 8, 10>;
+      tm_adj = time_adj_fast<R, 8, 10>;
+    } else {
+      return false;
+    }
+    return true;
+  }
+
+  void make_plane_launch(PlaneLaunch &L, const std::vector<PlaneJob<R>> &jobs,
+                         const std::vector<long> &planes) {
+    const size_t plane_bytes = (size_t)plane_smem * sizeof(C);
+    const size_t budget = 100 * 1024;
+    int np = std::max(1, kThreads / first_lines);
+    np = std::min<int>(np, (int)std::max<size_t>(1, budget / plane_bytes));
+    if (plane_bytes * np > (size_t)smem_max) throw DeviceError("space planes too large");
+    std::vector<int> cj;
+    std::vector<long> cp;
+    for (size_t i = 0; i < jobs.size(); ++i)
+      for (long q = 0; q < planes[i]; q += np) {
+        cj.push_back((int)i);
+        cp.push_back(q);
+      }
+    L.jobs.upload(jobs, stream);
+    L.cta_job.upload(cj, stream);
+    L.cta_plane0.upload(cp, stream);
+    L.job_planes.upload(planes, stream);
+    L.n_cta = (int)cj.size();
+    L.np = np;
+    L.smem = plane_bytes * np;
+  }
+
+  void build_fast(const std::vector<TimeJob<R>> &tj_generic) {
+    CK(cudaFuncSetAttribute(sp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
+    CK(cudaFuncSetAttribute(sp_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
+    CK(cudaFuncSetAttribute(tm_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
+    CK(cudaFuncSetAttribute(tm_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
+    // twiddle tables in constant memory of the current device
+    std::vector<C> tw(kTwTotal);
+    for (int i = 0, off = 0; i < kNumTw; off += kTwSizes[i], ++i)
+      for (int k = 0; k < kTwSizes[i]; ++k) {
+        const double a = -2.0 * 3.14159265358979323846 * (double)k / (double)kTwSizes[i];
+        tw[off + k].x = (R)std::cos(a);
+        tw[off + k].y = (R)std::sin(a);
+      }
+    if (sizeof(R) == sizeof(float))
+      CK(cudaMemcpyToSymbol(c_tw_f, tw.data(), tw.size() * sizeof(C)));
+    else
+      CK(cudaMemcpyToSymbol(c_tw_d, tw.data(), tw.size() * sizeof(C)));
+    const int nw = (int)plan.windows.size();
+    std::vector<PlaneJob<R>> jf(nw), ja(nw);
+    std::vector<long> planes(nw);
+    std::vector<TimeJob<R>> tj = tj_generic;
+    for (int w = 0; w < nw; ++w) {
+      const WindowPlan &W = plan.windows[w];
+      planes[w] = (long)W.T * W.F;
+      PlaneJob<R> j{};
+      for (int d = 0; d < 3; ++d) j.L[d] = d < W.D ? W.L[d] : 1;
+      j.src = X.get() + W.model_off;
+      j.dst = S0.get() + W.model_off;
+      jf[w] = j;
+      j.src = S0.get() + W.model_off;
+      j.dst = X.get() + W.model_off;
+      ja[w] = j;
+      tj[w].z = S0.get() + W.model_off;
+    }
+    make_plane_launch(pl_fwd, jf, planes);
+    make_plane_launch(pl_adj, ja, planes);
+    pending_plane_plain = ja;
+    pending_planes = planes;
+    time_jobs_fast.upload(tj, stream);
+    int h_max = 1;
+    for (const WindowPlan &W : plan.windows) h_max = std::max(h_max, W.h);
+    const int LS = plan.windows[0].Pt / 2 + 1;
+    const size_t per_fwd = (size_t)LS * sizeof(C) + (size_t)h_max * sizeof(R);
+    const size_t per_adj = (size_t)LS * sizeof(C);
+    make_time_launch(tf_fast, per_fwd, 32);
+    make_time_launch(ta_fast, per_adj, 32);
+  }
+
+  std::vector<PlaneJob<R>> pending_plane_plain;
+  std::vector<long> pending_planes;
+
   void make_gather(GatherLaunch &G, const std::vector<Contrib> &list, long record_size) {
     G.n_chunk = (int)((record_size + G.chunk - 1) / G.chunk);
     std::vector<long> count(G.n_chunk + 1, 0);
@@ -360,9 +502,10 @@ class Engine {
     wt_dst.upload(wdst, stream);
     wt_C.upload(wC, stream);
 
+    fast = pick_fast();
     X.alloc(M);
     S0.alloc(M);
-    S1.alloc(M);
+    if (!fast) S1.alloc(M);
     Y.alloc(toff);
     rec_d.alloc(plan.record_size);
     rec_r.alloc(plan.record_size);
@@ -404,6 +547,7 @@ class Engine {
       v.fft = wavelets ? fft.get(W.C) : 0;
     }
     time_jobs.upload(tj, stream);
+    if (fast) build_fast(tj);
     const size_t per_trace_time = 2 * (size_t)Pt_max * sizeof(C) + (size_t)C_max * sizeof(R);
     make_time_launch(time_fwd, per_trace_time, 16);
     make_time_launch(time_adj, per_trace_time, 16);
@@ -426,7 +570,8 @@ class Engine {
       spec_off.upload(so, stream);
     }
 
-    // ---- space-axis passes
+    // ---- space-axis passes (generic path)
+    if (fast) maxD = 0;
     fwd.resize(maxD);
     adj_update.resize(maxD);
     adj_plain.resize(maxD);
@@ -546,6 +691,13 @@ class Engine {
   void ensure_plain_adjoint() {
     if (G.get() != nullptr || plan.model_size == 0) return;
     G.alloc(plan.model_size);
+    if (fast) {
+      std::vector<PlaneJob<R>> jobs = pending_plane_plain;
+      for (size_t w = 0; w < jobs.size(); ++w) jobs[w].dst = G.get() + plan.windows[w].model_off;
+      make_plane_launch(pl_adj_plain, jobs, pending_planes);
+      CK(cudaStreamSynchronize(stream));
+      return;
+    }
     for (size_t k = 0; k < pending_plain.size(); ++k) {
       auto jobs = pending_plain[k];
       size_t i = 0;
@@ -583,8 +735,43 @@ class Engine {
     CK(cudaGetLastError());
   }
 
+  void launch_space_fwd() {
+    if (pl_fwd.n_cta == 0) return;
+    sp_fwd<<<pl_fwd.n_cta, kThreads, pl_fwd.smem, stream>>>(
+        pl_fwd.jobs.get(), pl_fwd.cta_job.get(), pl_fwd.cta_plane0.get(),
+        pl_fwd.job_planes.get(), pl_fwd.np);
+    CK(cudaGetLastError());
+  }
+
+  void launch_space_adj(const PlaneLaunch &L, int epilogue, R step, R lamb) {
+    if (L.n_cta == 0) return;
+    sp_adj<<<L.n_cta, kThreads, L.smem, stream>>>(L.jobs.get(), L.cta_job.get(),
+                                                  L.cta_plane0.get(), L.job_planes.get(), L.np,
+                                                  epilogue, step, lamb, scalar.get());
+    CK(cudaGetLastError());
+  }
+
+  void launch_time_fwd() {
+    if (fast) {
+      if (tf_fast.n_cta)
+        tm_fwd<<<tf_fast.n_cta, kThreads, tf_fast.smem, stream>>>(
+            time_jobs_fast.get(), tf_fast.cta_job.get(), tf_fast.cta_trace0.get(), tf_fast.nb);
+    } else if (time_fwd.n_cta) {
+      time_c2r_ola<R><<<time_fwd.n_cta, kThreads, time_fwd.smem, stream>>>(
+          time_jobs.get(), time_fwd.cta_job.get(), time_fwd.cta_trace0.get(), time_fwd.nb,
+          d_descs.get(), d_tw.get());
+    }
+    CK(cudaGetLastError());
+  }
+
   // Y = W F X  (window traces of the current model)
   void forward_traces() {
+    if (fast) {
+      launch_space_fwd();
+      launch_time_fwd();
+      if (wavelets) launch_wavelet(+1);
+      return;
+    }
     for (size_t k = 0; k < fwd.size(); ++k) launch_axis(fwd[k], 1, kStore, 0, 0);
     if (time_fwd.n_cta) {
       time_c2r_ola<R><<<time_fwd.n_cta, kThreads, time_fwd.smem, stream>>>(
@@ -613,7 +800,13 @@ class Engine {
       CK(cudaGetLastError());
       launch_wavelet(-1);
     }
-    if (time_adj.n_cta) {
+    if (fast) {
+      if (ta_fast.n_cta)
+        tm_adj<<<ta_fast.n_cta, kThreads, ta_fast.smem, stream>>>(
+            time_jobs_fast.get(), ta_fast.cta_job.get(), ta_fast.cta_trace0.get(), ta_fast.nb,
+            record, wavelets ? 0 : 1);
+      CK(cudaGetLastError());
+    } else if (time_adj.n_cta) {
       time_r2c<R><<<time_adj.n_cta, kThreads, time_adj.smem, stream>>>(
           time_jobs.get(), time_adj.cta_job.get(), time_adj.cta_trace0.get(), time_adj.nb,
           d_descs.get(), d_tw.get(), record, wavelets ? 0 : 1);
@@ -624,6 +817,10 @@ class Engine {
   // X <- threshold(X - step * A^H record, lamb)
   void adjoint_update(const R *record, R step, R lamb, bool track_max) {
     adjoint_time(record);
+    if (fast) {
+      launch_space_adj(pl_adj, track_max ? kUpdateMax : kUpdateThreshold, step, lamb);
+      return;
+    }
     for (size_t k = 0; k < adj_update.size(); ++k)
       launch_axis(adj_update[k], 0, track_max ? kUpdateMax : kUpdateThreshold, step, lamb);
   }
@@ -909,6 +1106,7 @@ int agd_gpu_problem_info(agd_gpu_problem const *pb, long int *info) {
   info[5] = (long)e.plan.mute.size();
   info[6] = (long)e.device_bytes();
   info[7] = e.g_fwd.n_contrib;
+  info[8] = e.fast ? 1 : 0;
   return 0;
 }
 
@@ -943,6 +1141,7 @@ int agd_gpu_adjoint(agd_gpu_problem *pb, AGD_TYPE const *record, AGD_TYPE *model
       agd::CK(cudaMemcpyAsync(e.rec_r.get(), record, e.rec_r.bytes(), cudaMemcpyHostToDevice,
                               e.stream));
     e.adjoint_time(e.rec_r.get());
+    if (e.fast) e.launch_space_adj(e.pl_adj_plain, agd::kStore, 0, 0);
     for (size_t k = 0; k < e.adj_plain.size(); ++k)
       e.launch_axis(e.adj_plain[k], 0, agd::kStore, 0, 0);
     e.model_to_ref(e.G.get(), model);
@@ -1060,17 +1259,16 @@ int agd_gpu_profile_iteration(agd_gpu_problem *pb, AGD_TYPE lamb, double *ms) {
       agd::CK(cudaEventRecord(v, e.stream));
       ev.push_back(v);
     };
-    const int nf = (int)e.fwd.size();
+    const int nf = e.fast ? 1 : (int)e.fwd.size();
     mark();
     for (int k = 0; k < nf; ++k) {
-      e.launch_axis(e.fwd[k], 1, agd::kStore, 0, 0);
+      if (e.fast)
+        e.launch_space_fwd();
+      else
+        e.launch_axis(e.fwd[k], 1, agd::kStore, 0, 0);
       mark();
     }
-    if (e.time_fwd.n_cta)
-      agd::time_c2r_ola<AGD_TYPE><<<e.time_fwd.n_cta, agd::kThreads, e.time_fwd.smem,
-                                    e.stream>>>(e.time_jobs.get(), e.time_fwd.cta_job.get(),
-                                                e.time_fwd.cta_trace0.get(), e.time_fwd.nb,
-                                                e.d_descs.get(), e.d_tw.get());
+    e.launch_time_fwd();
     mark();
     if (e.wavelets) e.launch_wavelet(+1);
     mark();
@@ -1079,7 +1277,10 @@ int agd_gpu_profile_iteration(agd_gpu_problem *pb, AGD_TYPE lamb, double *ms) {
     e.adjoint_time(e.rec_r.get());
     mark();
     for (int k = 0; k < nf; ++k) {
-      e.launch_axis(e.adj_update[k], 0, agd::kUpdateThreshold, e.stepsize, lamb);
+      if (e.fast)
+        e.launch_space_adj(e.pl_adj, agd::kUpdateThreshold, e.stepsize, lamb);
+      else
+        e.launch_axis(e.adj_update[k], 0, agd::kUpdateThreshold, e.stepsize, lamb);
       mark();
     }
     agd::CK(cudaEventSynchronize(ev.back()));

@@ -1,0 +1,612 @@
+// Shape-specialised kernels of the deblending operator for sm_100a.
+//
+// Every FFT here runs in registers with a compile-time size: a thread owns a
+// whole line (space axes) or one factor of a four-step transform (time axis),
+// so the radix schedule, the index arithmetic and the twiddle offsets are
+// constants.  Twiddles live in __constant__ memory (filled once per device
+// from double-precision values), so they are read as constant-bank operands.
+//
+//   space_fwd_fast  all space axes of a batch of (t, f) planes: load the
+//                   planes into shared memory, inverse FFT along every axis
+//                   (cropping P -> L), store the [L..] planes;
+//   space_adj_fast  the adjoint: zero-pad L -> P, forward FFT along every
+//                   axis, then x <- soft_threshold(x - step * g, lambda);
+//   time_fwd_fast   per block of traces, every time window: Hermitian
+//                   combine, half-length inverse FFT (four-step in shared
+//                   memory), taper, overlap-add with a one-hop carry;
+//   time_adj_fast   per block of traces, every time window: gather from the
+//                   record, taper, half-length forward FFT, split, double.
+//
+// Kernels for other sizes are the generic ones in kernels.cuh.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kernels.cuh"
+
+namespace agd {
+
+// ------------------------------------------------------------ twiddle tables
+
+// Transform lengths with a constant twiddle table W_N^k = exp(-2 pi i k / N).
+constexpr int kTwSizes[] = {6, 10, 12, 15, 16, 20, 24, 25, 32, 40, 48, 64, 80, 160, 320};
+constexpr int kNumTw = (int)(sizeof(kTwSizes) / sizeof(int));
+
+__host__ __device__ constexpr int tw_offset(int n) {
+  int off = 0;
+  for (int i = 0; i < kNumTw; ++i) {
+    if (kTwSizes[i] == n) return off;
+    off += kTwSizes[i];
+  }
+  return -1;
+}
+
+__host__ __device__ constexpr int tw_total() {
+  int off = 0;
+  for (int i = 0; i < kNumTw; ++i) off += kTwSizes[i];
+  return off;
+}
+
+constexpr int kTwTotal = tw_total();
+
+static __constant__ float2 c_tw_f[kTwTotal];
+static __constant__ double2 c_tw_d[kTwTotal];
+
+template <typename R>
+__device__ __forceinline__ Cx<R> ctw(int idx);
+template <>
+__device__ __forceinline__ float2 ctw<float>(int idx) {
+  return c_tw_f[idx];
+}
+template <>
+__device__ __forceinline__ double2 ctw<double>(int idx) {
+  return c_tw_d[idx];
+}
+
+// W_N^k (forward) or its conjugate (inverse); N must be in kTwSizes
+template <typename R, int N, bool INV>
+__device__ __forceinline__ Cx<R> wN(int k) {
+  static_assert(tw_offset(N) >= 0, "no twiddle table for this length");
+  Cx<R> w = ctw<R>(tw_offset(N) + k % N);
+  if (INV) w.y = -w.y;
+  return w;
+}
+
+// ------------------------------------------------------------ register DFTs
+
+template <bool INV, typename C>
+__device__ __forceinline__ C mul_i(C a) {  // -i a (forward) or +i a (inverse)
+  return INV ? cmake<C>(-a.y, a.x) : cmake<C>(a.y, -a.x);
+}
+
+__host__ __device__ constexpr int small_split(int n) {
+  // largest explicit radix that divides n with a nontrivial cofactor
+  return (n % 8 == 0 && n > 8) ? 8
+         : (n % 5 == 0 && n > 5) ? 5
+         : (n % 4 == 0 && n > 4) ? 4
+         : (n % 3 == 0 && n > 3) ? 3
+         : (n % 2 == 0 && n > 2) ? 2
+                                 : 0;
+}
+
+template <typename R, int N, bool INV>
+__device__ __forceinline__ void dft(Cx<R> (&v)[N]);
+
+// Four-step in registers: N = N1 * N2, natural order in and out.
+template <typename R, int N1, int N2, bool INV>
+__device__ __forceinline__ void dft_fourstep(Cx<R> (&v)[N1 * N2]) {
+  using C = Cx<R>;
+  constexpr int N = N1 * N2;
+  C a[N];
+#pragma unroll
+  for (int n2 = 0; n2 < N2; ++n2) {
+    C t[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) t[n1] = v[N2 * n1 + n2];
+    dft<R, N1, INV>(t);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1)
+      a[N2 * k1 + n2] = (n2 * k1 == 0) ? t[k1] : cmul(t[k1], wN<R, N, INV>(n2 * k1));
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < N1; ++k1) {
+    C t[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) t[n2] = a[N2 * k1 + n2];
+    dft<R, N2, INV>(t);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) v[k1 + N1 * k2] = t[k2];
+  }
+}
+
+template <typename R, int N, bool INV>
+__device__ __forceinline__ void dft(Cx<R> (&v)[N]) {
+  using C = Cx<R>;
+  if constexpr (N == 1) {
+  } else if constexpr (N == 2) {
+    const C a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if constexpr (N == 3) {
+    const R c = (R)0.86602540378443864676;
+    const C t1 = cadd(v[1], v[2]);
+    const C t2 = cmake<C>(v[0].x - (R)0.5 * t1.x, v[0].y - (R)0.5 * t1.y);
+    const C t3 = mul_i<INV>(cscale(csub(v[1], v[2]), c));
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(t2, t3);
+    v[2] = csub(t2, t3);
+  } else if constexpr (N == 4) {
+    const C s02 = cadd(v[0], v[2]);
+    const C d02 = csub(v[0], v[2]);
+    const C s13 = cadd(v[1], v[3]);
+    const C r13 = mul_i<INV>(csub(v[1], v[3]));
+    v[0] = cadd(s02, s13);
+    v[1] = cadd(d02, r13);
+    v[2] = csub(s02, s13);
+    v[3] = csub(d02, r13);
+  } else if constexpr (N == 5) {
+    const R c1 = (R)0.30901699437494742410;
+    const R c2 = (R)-0.80901699437494742410;
+    const R s1 = (R)0.95105651629515357212;
+    const R s2 = (R)0.58778525229247312917;
+    const C t1 = cadd(v[1], v[4]);
+    const C t2 = cadd(v[2], v[3]);
+    const C t3 = csub(v[1], v[4]);
+    const C t4 = csub(v[2], v[3]);
+    const C a1 = cmake<C>(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+    const C a2 = cmake<C>(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+    const C b1 = mul_i<INV>(cmake<C>(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y));
+    const C b2 = mul_i<INV>(cmake<C>(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y));
+    v[0] = cadd(v[0], cadd(t1, t2));
+    v[1] = cadd(a1, b1);
+    v[4] = csub(a1, b1);
+    v[2] = cadd(a2, b2);
+    v[3] = csub(a2, b2);
+  } else if constexpr (N == 8) {
+    // even/odd split into two 4-point DFTs, W_8 = (1 -/+ i) / sqrt(2)
+    C e[4] = {v[0], v[2], v[4], v[6]};
+    C o[4] = {v[1], v[3], v[5], v[7]};
+    dft<R, 4, INV>(e);
+    dft<R, 4, INV>(o);
+    const R h = (R)0.70710678118654752440;
+    const C o1 = INV ? cmake<C>(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
+                     : cmake<C>(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+    const C o2 = mul_i<INV>(o[2]);
+    const C o3 = INV ? cmake<C>(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
+                     : cmake<C>(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], o1);
+    v[5] = csub(e[1], o1);
+    v[2] = cadd(e[2], o2);
+    v[6] = csub(e[2], o2);
+    v[3] = cadd(e[3], o3);
+    v[7] = csub(e[3], o3);
+  } else if constexpr (small_split(N) != 0) {
+    constexpr int N1 = small_split(N);
+    dft_fourstep<R, N1, N / N1, INV>(v);
+  } else {
+    // prime length without a table: direct DFT (only small primes reach here)
+    static_assert(N <= 13, "unsupported register DFT length");
+    C out[N];
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      C acc = v[0];
+#pragma unroll
+      for (int r = 1; r < N; ++r) {
+        R s, c;
+        sincospi((R)(2 * ((r * q) % N)) / (R)N, &s, &c);
+        const C w = cmake<C>(c, INV ? s : -s);
+        acc = cadd(acc, cmul(v[r], w));
+      }
+      out[q] = acc;
+    }
+#pragma unroll
+    for (int q = 0; q < N; ++q) v[q] = out[q];
+  }
+}
+
+// ------------------------------------------------------------ space axes
+
+// One window's planes for the fast space kernels.
+template <typename R>
+struct PlaneJob {
+  const Cx<R> *src;  // forward: model planes [P..]; adjoint: Z planes [L..]
+  Cx<R> *dst;        // forward: Z planes [L..]; adjoint: model planes (update)
+  int L[3];
+};
+
+// Shared-memory plane layout [P0][P1][P2 + pad] (dims beyond D are 1): the
+// last axis is padded to an odd length so threads walking different rows hit
+// different banks.
+template <int D, int P0, int P1, int P2>
+struct PlaneShape {
+  static constexpr int PL = D == 1 ? P0 : (D == 2 ? P1 : P2);  // last axis
+  static constexpr int PLS = PL % 2 ? PL : PL + 1;            // padded
+  static constexpr int E0 = D == 1 ? PLS : P0;
+  static constexpr int E1 = D == 1 ? 1 : (D == 2 ? PLS : P1);
+  static constexpr int E2 = D == 3 ? PLS : 1;
+  static constexpr int size = E0 * E1 * E2;  // complex per plane in smem
+  static constexpr int dense = P0 * (D >= 2 ? P1 : 1) * (D == 3 ? P2 : 1);
+};
+
+// FFT of lines along `axis` of every plane in smem.  Lines run over the
+// current extents of the other axes; n_in elements are read (zero beyond),
+// n_out written.
+template <typename R, int N, bool INV>
+__device__ __forceinline__ void lines_fft(Cx<R> *buf, int n_planes, int plane_size, int e_outer,
+                                          int e_inner, int stride_outer, int stride_line,
+                                          int stride_inner, int n_in, int n_out) {
+  using C = Cx<R>;
+  const int per_plane = e_outer * e_inner;
+  const int total = n_planes * per_plane;
+  for (int l = threadIdx.x; l < total; l += blockDim.x) {
+    const int p = l / per_plane;
+    const int r = l - p * per_plane;
+    const int o = r / e_inner;
+    const int i = r - o * e_inner;
+    C *line = buf + p * plane_size + o * stride_outer + i * stride_inner;
+    C v[N];
+#pragma unroll
+    for (int e = 0; e < N; ++e) v[e] = e < n_in ? line[e * stride_line] : cmake<C>((R)0, (R)0);
+    dft<R, N, INV>(v);
+#pragma unroll
+    for (int e = 0; e < N; ++e)
+      if (e < n_out) line[e * stride_line] = v[e];
+  }
+}
+
+// All space axes of one window, forward operator direction (inverse FFT,
+// crop) or adjoint direction (zero-pad, forward FFT).  Axis a of the smem
+// plane has stride S_a and extent P_a (full) or L_a (cropped / not yet
+// padded).
+template <typename R, int D, int P0, int P1, int P2, bool FWD>
+__device__ __forceinline__ void space_axes(Cx<R> *buf, int np, const int (&L)[3]) {
+  using S = PlaneShape<D, P0, P1, P2>;
+  constexpr int S0 = S::E1 * S::E2;
+  constexpr int S1 = S::E2;
+  constexpr int P[3] = {P0, P1, P2};
+  if constexpr (FWD) {
+    // last axis first; axes after the current one are already cropped
+    if constexpr (D == 1) {
+      lines_fft<R, P0, true>(buf, np, S::size, 1, 1, 0, 1, 0, P0, L[0]);
+    } else if constexpr (D == 2) {
+      lines_fft<R, P1, true>(buf, np, S::size, P0, 1, S0, 1, 0, P1, L[1]);
+      __syncthreads();
+      lines_fft<R, P0, true>(buf, np, S::size, 1, L[1], 0, S0, 1, P0, L[0]);
+    } else {
+      lines_fft<R, P2, true>(buf, np, S::size, P0 * P1, 1, S1, 1, 0, P2, L[2]);
+      __syncthreads();
+      // axis 1: lines over (i0 < P0, i2 < L2)
+      lines_fft<R, P1, true>(buf, np, S::size, P0, L[2], S0, S1, 1, P1, L[1]);
+      __syncthreads();
+      // axis 0: lines over (i1 < L1, i2 < L2), i2 fastest
+      lines_fft<R, P0, true>(buf, np, S::size, L[1], L[2], S1, S0, 1, P0, L[0]);
+    }
+  } else {
+    if constexpr (D == 1) {
+      lines_fft<R, P0, false>(buf, np, S::size, 1, 1, 0, 1, 0, L[0], P0);
+    } else if constexpr (D == 2) {
+      // axis 0 first over the L1 filled columns, then axis 1 over all P0 rows
+      lines_fft<R, P0, false>(buf, np, S::size, 1, L[1], 0, S0, 1, L[0], P0);
+      __syncthreads();
+      lines_fft<R, P1, false>(buf, np, S::size, P0, 1, S0, 1, 0, L[1], P1);
+    } else {
+      lines_fft<R, P0, false>(buf, np, S::size, L[1], L[2], S1, S0, 1, L[0], P0);
+      __syncthreads();
+      lines_fft<R, P1, false>(buf, np, S::size, P0, L[2], S0, S1, 1, L[1], P1);
+      __syncthreads();
+      lines_fft<R, P2, false>(buf, np, S::size, P0 * P1, 1, S1, 1, 0, L[2], P2);
+    }
+  }
+  (void)P;
+}
+
+// smem position of dense element e of a plane with per-axis extents X0..X2
+// (row-major, last axis fastest) in the padded layout
+template <int D, int P0, int P1, int P2>
+__device__ __forceinline__ int plane_pos(int e, int X1, int X2) {
+  using S = PlaneShape<D, P0, P1, P2>;
+  if constexpr (D == 1) {
+    return e;
+  } else if constexpr (D == 2) {
+    const int i0 = e / X1;
+    return i0 * S::E1 + (e - i0 * X1);
+  } else {
+    const int i0 = e / (X1 * X2);
+    const int r = e - i0 * X1 * X2;
+    const int i1 = r / X2;
+    return i0 * S::E1 * S::E2 + i1 * S::E2 + (r - i1 * X2);
+  }
+}
+
+// Forward operator, all space axes: Z[L..] = crop(IFFT_space(X[P..])) for
+// planes [plane0, plane0 + np) of one window.
+template <typename R, int D, int P0, int P1, int P2>
+__global__ void __launch_bounds__(kThreads)
+    space_fwd_fast(const PlaneJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
+                   const long *__restrict__ cta_plane0, const long *__restrict__ job_planes,
+                   int np_max) {
+  using C = Cx<R>;
+  using S = PlaneShape<D, P0, P1, P2>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *buf = reinterpret_cast<C *>(smem_raw);
+  const int jb = cta_job[blockIdx.x];
+  const PlaneJob<R> job = jobs[jb];
+  const long p0 = cta_plane0[blockIdx.x];
+  const int np = (int)min((long)np_max, job_planes[jb] - p0);
+  const int L[3] = {job.L[0], job.L[1], job.L[2]};
+  // load dense [P..] planes
+  const C *src = job.src + p0 * S::dense;
+  const int n_load = np * S::dense;
+  for (int e = threadIdx.x; e < n_load; e += blockDim.x) {
+    const int p = e / S::dense;
+    const int r = e - p * S::dense;
+    buf[p * S::size + plane_pos<D, P0, P1, P2>(r, P1, P2)] = src[e];
+  }
+  __syncthreads();
+  space_axes<R, D, P0, P1, P2, true>(buf, np, L);
+  __syncthreads();
+  // store dense [L..] planes
+  const int dense_out = L[0] * (D >= 2 ? L[1] : 1) * (D == 3 ? L[2] : 1);
+  C *dst = job.dst + p0 * dense_out;
+  const int n_store = np * dense_out;
+  for (int e = threadIdx.x; e < n_store; e += blockDim.x) {
+    const int p = e / dense_out;
+    const int r = e - p * dense_out;
+    dst[e] = buf[p * S::size + plane_pos<D, P0, P1, P2>(r, L[1], L[2])];
+  }
+}
+
+// Adjoint, all space axes, with the ISTA update fused:
+// X <- soft_threshold(X - step * FFT_space(pad(G[L..])), lamb)   (epilogue
+// kUpdateThreshold), X <- X - step * ..., tracking max |X|^2 (kUpdateMax), or
+// X <- FFT_space(pad(G)) (kStore).
+template <typename R, int D, int P0, int P1, int P2>
+__global__ void __launch_bounds__(kThreads)
+    space_adj_fast(const PlaneJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
+                   const long *__restrict__ cta_plane0, const long *__restrict__ job_planes,
+                   int np_max, int epilogue, R step, R lamb, R *max_out) {
+  using C = Cx<R>;
+  using S = PlaneShape<D, P0, P1, P2>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *buf = reinterpret_cast<C *>(smem_raw);
+  const int jb = cta_job[blockIdx.x];
+  const PlaneJob<R> job = jobs[jb];
+  const long p0 = cta_plane0[blockIdx.x];
+  const int np = (int)min((long)np_max, job_planes[jb] - p0);
+  const int L[3] = {job.L[0], job.L[1], job.L[2]};
+  const int dense_in = L[0] * (D >= 2 ? L[1] : 1) * (D == 3 ? L[2] : 1);
+  const C *src = job.src + p0 * dense_in;
+  const int n_load = np * dense_in;
+  for (int e = threadIdx.x; e < n_load; e += blockDim.x) {
+    const int p = e / dense_in;
+    const int r = e - p * dense_in;
+    buf[p * S::size + plane_pos<D, P0, P1, P2>(r, L[1], L[2])] = src[e];
+  }
+  __syncthreads();
+  space_axes<R, D, P0, P1, P2, false>(buf, np, L);
+  __syncthreads();
+  C *dst = job.dst + p0 * S::dense;
+  const int n_store = np * S::dense;
+  const R lamb_sq = lamb * lamb;
+  R local_max = (R)0;
+  for (int e = threadIdx.x; e < n_store; e += blockDim.x) {
+    const int p = e / S::dense;
+    const int r = e - p * S::dense;
+    const C g = buf[p * S::size + plane_pos<D, P0, P1, P2>(r, P1, P2)];
+    if (epilogue == kStore) {
+      dst[e] = g;
+    } else {
+      const C x = dst[e];
+      C xn = cmake<C>(sub_rn<R>(x.x, mul_rn<R>(step, g.x)), sub_rn<R>(x.y, mul_rn<R>(step, g.y)));
+      if (epilogue == kUpdateThreshold) {
+        xn = soft_threshold<R>(xn, lamb, lamb_sq);
+      } else {
+        const R a2 = abs_sq<R>(xn);
+        local_max = a2 > local_max ? a2 : local_max;
+      }
+      dst[e] = xn;
+    }
+  }
+  if (epilogue == kUpdateMax) {
+    __shared__ R red[32];
+    const R m = block_max<R>(local_max, red);
+    if (threadIdx.x == 0) atomic_max_nonneg(max_out, m);
+  }
+}
+
+// ------------------------------------------------------------ time axis
+
+// Four-step FFT of length M = M1 * M2 on nl lines of shared memory (line
+// stride LS).  Output X[k1 + M1 k2] is left at position M2 k1 + k2.
+template <typename R, int M1, int M2, bool INV>
+__device__ __forceinline__ void lines_fourstep(Cx<R> *buf, int nl, int LS) {
+  using C = Cx<R>;
+  constexpr int M = M1 * M2;
+  for (int w = threadIdx.x; w < nl * M2; w += blockDim.x) {
+    const int line = w / M2;
+    const int n2 = w - line * M2;
+    C *b = buf + line * LS;
+    C v[M1];
+#pragma unroll
+    for (int n1 = 0; n1 < M1; ++n1) v[n1] = b[M2 * n1 + n2];
+    dft<R, M1, INV>(v);
+#pragma unroll
+    for (int k1 = 0; k1 < M1; ++k1)
+      b[M2 * k1 + n2] = (k1 == 0) ? v[0] : cmul(v[k1], wN<R, M, INV>(n2 * k1));
+  }
+  __syncthreads();
+  for (int w = threadIdx.x; w < nl * M1; w += blockDim.x) {
+    const int line = w / M1;
+    const int k1 = w - line * M1;
+    C *b = buf + line * LS + M2 * k1;
+    C v[M2];
+#pragma unroll
+    for (int n2 = 0; n2 < M2; ++n2) v[n2] = b[n2];
+    dft<R, M2, INV>(v);
+#pragma unroll
+    for (int k2 = 0; k2 < M2; ++k2) b[k2] = v[k2];
+  }
+  __syncthreads();
+}
+
+template <int M1, int M2>
+__device__ __forceinline__ int fourstep_pos(int k) {
+  return M2 * (k % M1) + k / M1;
+}
+
+// Forward time axis for even Pt = 2 M and Lt = 2 h: per trace and time
+// window, c2r of the F = M + 1 bins through a length-M complex FFT, then
+// taper and overlap-add; segment [t h, (t+1) h) of a trace is final once
+// window t is added, so only a one-hop carry stays in shared memory.
+template <typename R, int M1, int M2>
+__global__ void __launch_bounds__(kThreads)
+    time_fwd_fast(const TimeJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
+                  const int *__restrict__ cta_trace0, int nb_max) {
+  using C = Cx<R>;
+  constexpr int M = M1 * M2;
+  constexpr int LS = M + 1;  // F bins per line
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const TimeJob<R> job = jobs[cta_job[blockIdx.x]];
+  const int t0 = cta_trace0[blockIdx.x];
+  const int nb = min(nb_max, job.n_traces - t0);
+  const int h = job.h;
+  C *buf = reinterpret_cast<C *>(smem_raw);
+  R *carry = reinterpret_cast<R *>(buf + nb_max * LS);  // [nb][h]
+  for (int i = threadIdx.x; i < nb * h; i += blockDim.x) carry[i] = (R)0;
+  for (int t = 0; t < job.T; ++t) {
+    const C *zt = job.z + (long)t * job.F * job.n_traces + t0;
+    for (int idx = threadIdx.x; idx < nb * LS; idx += blockDim.x) {
+      const int f = idx / nb;
+      const int i = idx - f * nb;
+      buf[i * LS + f] = zt[(long)f * job.n_traces + i];
+    }
+    __syncthreads();
+    // Hermitian combine into M complex values (pairs k, M - k per thread):
+    // Z_k = (X_k + conj X_{M-k}) + i e^{+2 pi i k / Pt} (X_k - conj X_{M-k})
+    for (int w = threadIdx.x; w < nb * (M / 2 + 1); w += blockDim.x) {
+      const int i = w / (M / 2 + 1);
+      const int k = w - i * (M / 2 + 1);
+      C *b = buf + i * LS;
+      const int kk = M - k;
+      C xa = b[k];
+      C xb = b[kk];
+      if (k == 0) {
+        xa.y = (R)0;
+        xb.y = (R)0;
+      }
+      auto comb = [&](C a, C bc_src, int kidx) {
+        const C bc = cmake<C>(bc_src.x, -bc_src.y);
+        const C e = cadd(a, bc);
+        const C d = csub(a, bc);
+        const C w2 = wN<R, 2 * M, true>(kidx);
+        const C o = cmul(d, w2);
+        return cmake<C>(e.x - o.y, e.y + o.x);
+      };
+      const C za = comb(xa, xb, k);
+      if (k != 0 && k != kk) {
+        const C zb = comb(xb, xa, kk);
+        b[kk] = zb;
+      }
+      b[k] = za;  // k == 0 pairs with the Nyquist bin, which is then unused
+    }
+    __syncthreads();
+    lines_fourstep<R, M1, M2, true>(buf, nb, LS);
+    // taper, overlap-add, write the completed segment of each trace; one
+    // thread owns samples j and j + h, so the carry is read then rewritten
+    // by the same thread
+    for (int idx = threadIdx.x; idx < nb * h; idx += blockDim.x) {
+      const int i = idx / h;
+      const int j = idx - i * h;
+      const R sc = job.space_scale[t0 + i];
+      const C z_lo = buf[i * LS + fourstep_pos<M1, M2>(j >> 1)];
+      const C z_hi = buf[i * LS + fourstep_pos<M1, M2>((j + h) >> 1)];
+      const R u_lo = (j & 1) ? z_lo.y : z_lo.x;
+      const R u_hi = ((j + h) & 1) ? z_hi.y : z_hi.x;
+      job.y[(long)(t0 + i) * job.C + t * h + j] =
+          carry[idx] + (u_lo * sc) * job.time_taper[j];
+      carry[idx] = (u_hi * sc) * job.time_taper[j + h];
+    }
+    __syncthreads();
+  }
+  // last half window and the zero tail up to C
+  for (int idx = threadIdx.x; idx < nb * h; idx += blockDim.x) {
+    const int i = idx / h;
+    const int j = idx - i * h;
+    job.y[(long)(t0 + i) * job.C + job.T * h + j] = carry[i * h + j];
+  }
+  const int tail = job.C - (job.T + 1) * h;
+  for (int idx = threadIdx.x; idx < nb * tail; idx += blockDim.x) {
+    const int i = idx / tail;
+    const int j = idx - i * tail;
+    job.y[(long)(t0 + i) * job.C + (job.T + 1) * h + j] = (R)0;
+  }
+}
+
+// Adjoint time axis for even Pt = 2 M and Lt = 2 h: per trace and window,
+// gather Lt samples (record through the blend coordinates, or the trace
+// buffer), taper, pack pairs into M complex values, forward FFT, split into
+// the M + 1 bins and double bins 1..M-1.
+template <typename R, int M1, int M2>
+__global__ void __launch_bounds__(kThreads)
+    time_adj_fast(const TimeJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
+                  const int *__restrict__ cta_trace0, int nb_max, const R *__restrict__ record,
+                  int from_record) {
+  using C = Cx<R>;
+  constexpr int M = M1 * M2;
+  constexpr int LS = M + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const TimeJob<R> job = jobs[cta_job[blockIdx.x]];
+  const int t0 = cta_trace0[blockIdx.x];
+  const int nb = min(nb_max, job.n_traces - t0);
+  const int h = job.h;
+  const int Lt = job.Lt;
+  C *buf = reinterpret_cast<C *>(smem_raw);
+  for (int t = 0; t < job.T; ++t) {
+    for (int idx = threadIdx.x; idx < nb * M; idx += blockDim.x) {
+      const int i = idx / M;
+      const int m = idx - i * M;
+      const int tr = t0 + i;
+      R v[2] = {(R)0, (R)0};
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int j = 2 * m + q;
+        if (j < Lt) {
+          const int s = t * h + j;
+          R x = (R)0;
+          if (from_record) {
+            const long rec = job.blend_rec[tr];
+            const int ts = job.blend_ts[tr];
+            if (rec >= 0 && s >= ts && s < ts + job.blend_n[tr]) x = record[rec + (s - ts)];
+          } else if (s < job.C) {
+            x = job.y[(long)tr * job.C + s];
+          }
+          v[q] = (x * job.space_scale[tr]) * job.time_taper[j];
+        }
+      }
+      buf[i * LS + m] = cmake<C>(v[0], v[1]);
+    }
+    __syncthreads();
+    lines_fourstep<R, M1, M2, false>(buf, nb, LS);
+    // split: X_k = (Z_k + conj Z_{M-k}) / 2 - i e^{-2 pi i k / Pt} (Z_k - conj Z_{M-k}) / 2
+    C *zt = job.z + (long)t * job.F * job.n_traces + t0;
+    for (int idx = threadIdx.x; idx < nb * LS; idx += blockDim.x) {
+      const int f = idx / nb;
+      const int i = idx - f * nb;
+      const C *b = buf + i * LS;
+      const C zk = b[fourstep_pos<M1, M2>(f % M)];
+      const C zm = b[fourstep_pos<M1, M2>((M - f) % M)];
+      const C zc = cmake<C>(zm.x, -zm.y);
+      const C e = cmake<C>((R)0.5 * (zk.x + zc.x), (R)0.5 * (zk.y + zc.y));
+      const C o = cmake<C>((R)0.5 * (zk.y - zc.y), (R)-0.5 * (zk.x - zc.x));
+      C x = cadd(e, cmul(wN<R, 2 * M, false>(f), o));
+      if (f >= 1 && f <= M - 1) x = cmake<C>(x.x * (R)2, x.y * (R)2);
+      zt[(long)f * job.n_traces + i] = x;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace agd
