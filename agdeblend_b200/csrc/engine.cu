@@ -188,19 +188,23 @@ class Engine {
 
   // shape-specialised path (fast.cuh), used when every window has the same
   // space and time FFT lengths and an instantiation exists
-  using SpaceFwdFn = void (*)(const PlaneJob<R> *, const int *, const long *, const long *, int);
-  using SpaceAdjFn = void (*)(const PlaneJob<R> *, const int *, const long *, const long *, int,
-                              int, R, R, R *);
+  using SpaceFwdFn = void (*)(const PlaneJob<R> *, PlaneBatches, int);
+  using SpaceAdjFn = void (*)(const PlaneJob<R> *, PlaneBatches, int, int, int, R, R, R *);
   using TimeFwdFn = void (*)(const TimeJob<R> *, const int *, const int *, int);
   using TimeAdjFn = void (*)(const TimeJob<R> *, const int *, const int *, int, const R *, int);
   struct PlaneLaunch {
     DevArray<PlaneJob<R>> jobs;
-    DevArray<int> cta_job;
-    DevArray<long> cta_plane0;
+    DevArray<int> batch_job;
+    DevArray<long> batch_plane0;
     DevArray<long> job_planes;
-    int n_cta = 0;
+    int n_batch = 0;
+    int grid = 0;
     int np = 0;
+    int stage_x = 0;
     size_t smem = 0;
+    PlaneBatches batches() const {
+      return PlaneBatches{batch_job.get(), batch_plane0.get(), job_planes.get(), n_batch};
+    }
   };
   bool fast = false;
   SpaceFwdFn sp_fwd = nullptr;
@@ -208,7 +212,9 @@ class Engine {
   TimeFwdFn tm_fwd = nullptr;
   TimeAdjFn tm_adj = nullptr;
   int plane_smem = 0;   // complex per plane in shared memory
+  int plane_dense = 0;  // complex per plane in global memory
   int first_lines = 1;  // lines per plane of the first space pass
+  int n_sm = 148;
   PlaneLaunch pl_fwd, pl_adj, pl_adj_plain;
   TimeLaunch tf_fast, ta_fast;
   DevArray<TimeJob<R>> time_jobs_fast;
@@ -224,6 +230,11 @@ class Engine {
   explicit Engine(Plan &&p) : plan(std::move(p)) {
     CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     smem_max = optin_smem();
+    {
+      int dev = 0;
+      CK(cudaGetDevice(&dev));
+      CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    }
     set_smem_limits();
     build();
   }
@@ -314,6 +325,7 @@ class Engine {
     sp_fwd = space_fwd_fast<R, D, P0, P1, P2>;
     sp_adj = space_adj_fast<R, D, P0, P1, P2>;
     plane_smem = PlaneShape<D, P0, P1, P2>::size;
+    plane_dense = PlaneShape<D, P0, P1, P2>::dense;
     first_lines = D == 1 ? 1 : (D == 2 ? P0 : P0 * P1);
     return true;
   }
@@ -332,6 +344,7 @@ class Engine {
                        space_case<2, 20, 40, 1>(W0) || space_case<2, 20, 20, 1>(W0) ||
                        space_case<2, 40, 40, 1>(W0) || space_case<3, 20, 20, 20>(W0);
     if (!space) return false;
+    if (2 * (size_t)plane_smem * sizeof(C) > (size_t)smem_max) return false;
     if (W0.Pt == 320) {
       tm_fwd = time_fwd_fast<R, 16, 10>;
       tm_adj = time_adj_fast<R, 16, 10>;
@@ -344,34 +357,42 @@ class Engine {
     return true;
   }
 
+  // Persistent, double-buffered plane batches: a stage holds np planes (and,
+  // for the adjoint, their model values); grid = resident blocks.
+  template <typename K>
   void make_plane_launch(PlaneLaunch &L, const std::vector<PlaneJob<R>> &jobs,
-                         const std::vector<long> &planes) {
-    const size_t plane_bytes = (size_t)plane_smem * sizeof(C);
-    const size_t budget = 100 * 1024;
-    int np = std::max(1, kThreads / first_lines);
-    np = std::min<int>(np, (int)std::max<size_t>(1, budget / plane_bytes));
-    if (plane_bytes * np > (size_t)smem_max) throw DeviceError("space planes too large");
-    std::vector<int> cj;
-    std::vector<long> cp;
+                         const std::vector<long> &planes, bool adjoint, K kernel) {
+    // the adjoint stages the model values too when two such stages fit
+    L.stage_x = adjoint && 2 * (size_t)(plane_smem + plane_dense) * sizeof(C) <= (size_t)smem_max;
+    const size_t plane_bytes = (size_t)(plane_smem + (L.stage_x ? plane_dense : 0)) * sizeof(C);
+    const size_t stage_budget = 96 * 1024;
+    int np = std::max(1, 2 * kThreads / first_lines);
+    np = std::min<int>(np, (int)std::max<size_t>(1, stage_budget / plane_bytes));
+    if (2 * plane_bytes * np > (size_t)smem_max) throw DeviceError("space planes too large");
+    std::vector<int> bj;
+    std::vector<long> bp;
     for (size_t i = 0; i < jobs.size(); ++i)
       for (long q = 0; q < planes[i]; q += np) {
-        cj.push_back((int)i);
-        cp.push_back(q);
+        bj.push_back((int)i);
+        bp.push_back(q);
       }
     L.jobs.upload(jobs, stream);
-    L.cta_job.upload(cj, stream);
-    L.cta_plane0.upload(cp, stream);
+    L.batch_job.upload(bj, stream);
+    L.batch_plane0.upload(bp, stream);
     L.job_planes.upload(planes, stream);
-    L.n_cta = (int)cj.size();
+    L.n_batch = (int)bj.size();
     L.np = np;
-    L.smem = plane_bytes * np;
+    L.smem = 2 * plane_bytes * np;
+    int per_sm = 1;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, L.smem));
+    L.grid = std::max(1, std::min(L.n_batch, std::max(per_sm, 1) * n_sm));
   }
 
   void build_fast(const std::vector<TimeJob<R>> &tj_generic) {
-    CK(cudaFuncSetAttribute(sp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
-    CK(cudaFuncSetAttribute(sp_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
-    CK(cudaFuncSetAttribute(tm_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
-    CK(cudaFuncSetAttribute(tm_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
+    const int limit = optin_smem();
+    const int dyn = std::min({opt_in(sp_fwd, limit), opt_in(sp_adj, limit), opt_in(tm_fwd, limit),
+                              opt_in(tm_adj, limit)});
+    smem_max = std::min(smem_max, dyn);
     // twiddle tables in constant memory of the current device
     std::vector<C> tw(kTwTotal);
     for (int i = 0, off = 0; i < kNumTw; off += kTwSizes[i], ++i)
@@ -401,16 +422,16 @@ class Engine {
       ja[w] = j;
       tj[w].z = S0.get() + W.model_off;
     }
-    make_plane_launch(pl_fwd, jf, planes);
-    make_plane_launch(pl_adj, ja, planes);
+    make_plane_launch(pl_fwd, jf, planes, false, sp_fwd);
+    make_plane_launch(pl_adj, ja, planes, true, sp_adj);
     pending_plane_plain = ja;
     pending_planes = planes;
     time_jobs_fast.upload(tj, stream);
     int h_max = 1;
     for (const WindowPlan &W : plan.windows) h_max = std::max(h_max, W.h);
     const int LS = plan.windows[0].Pt / 2 + 1;
-    const size_t per_fwd = (size_t)LS * sizeof(C) + (size_t)h_max * sizeof(R);
-    const size_t per_adj = (size_t)LS * sizeof(C);
+    const size_t per_fwd = 2 * (size_t)LS * sizeof(C) + (size_t)h_max * sizeof(R);
+    const size_t per_adj = (size_t)LS * sizeof(C) + 2 * (size_t)(2 * h_max) * sizeof(R);
     make_time_launch(tf_fast, per_fwd, 32);
     make_time_launch(ta_fast, per_adj, 32);
   }
@@ -694,7 +715,7 @@ class Engine {
     if (fast) {
       std::vector<PlaneJob<R>> jobs = pending_plane_plain;
       for (size_t w = 0; w < jobs.size(); ++w) jobs[w].dst = G.get() + plan.windows[w].model_off;
-      make_plane_launch(pl_adj_plain, jobs, pending_planes);
+      make_plane_launch(pl_adj_plain, jobs, pending_planes, true, sp_adj);
       CK(cudaStreamSynchronize(stream));
       return;
     }
@@ -736,18 +757,16 @@ class Engine {
   }
 
   void launch_space_fwd() {
-    if (pl_fwd.n_cta == 0) return;
-    sp_fwd<<<pl_fwd.n_cta, kThreads, pl_fwd.smem, stream>>>(
-        pl_fwd.jobs.get(), pl_fwd.cta_job.get(), pl_fwd.cta_plane0.get(),
-        pl_fwd.job_planes.get(), pl_fwd.np);
+    if (pl_fwd.n_batch == 0) return;
+    sp_fwd<<<pl_fwd.grid, kThreads, pl_fwd.smem, stream>>>(pl_fwd.jobs.get(), pl_fwd.batches(),
+                                                           pl_fwd.np);
     CK(cudaGetLastError());
   }
 
   void launch_space_adj(const PlaneLaunch &L, int epilogue, R step, R lamb) {
-    if (L.n_cta == 0) return;
-    sp_adj<<<L.n_cta, kThreads, L.smem, stream>>>(L.jobs.get(), L.cta_job.get(),
-                                                  L.cta_plane0.get(), L.job_planes.get(), L.np,
-                                                  epilogue, step, lamb, scalar.get());
+    if (L.n_batch == 0) return;
+    sp_adj<<<L.grid, kThreads, L.smem, stream>>>(L.jobs.get(), L.batches(), L.np, L.stage_x,
+                                                 epilogue, step, lamb, scalar.get());
     CK(cudaGetLastError());
   }
 

@@ -73,6 +73,29 @@ __device__ __forceinline__ Cx<R> wN(int k) {
   return w;
 }
 
+// ------------------------------------------------------------ async copies
+
+// global -> shared copies that complete asynchronously (cp.async, grouped
+// with commit/wait); `valid == false` fills the destination with zeros
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem, bool valid = true) {
+  static_assert(BYTES == 4 || BYTES == 8 || BYTES == 16, "cp.async size");
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? BYTES : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(s), "l"(gmem),
+               "n"(BYTES), "r"(n)
+               : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // ------------------------------------------------------------ register DFTs
 
 template <bool INV, typename C>
@@ -321,94 +344,145 @@ __device__ __forceinline__ int plane_pos(int e, int X1, int X2) {
   }
 }
 
-// Forward operator, all space axes: Z[L..] = crop(IFFT_space(X[P..])) for
-// planes [plane0, plane0 + np) of one window.
+// Batches of planes for the persistent space kernels: batch b covers planes
+// [plane0[b], plane0[b] + np) of job job[b].
+struct PlaneBatches {
+  const int *job;
+  const long *plane0;
+  const long *job_planes;
+  int n;
+};
+
+// Forward operator, all space axes: Z[L..] = crop(IFFT_space(X[P..])).
+// Persistent blocks walk the batches; the planes of the next batch are
+// copied into the second shared buffer (cp.async) while the current one is
+// transformed.
 template <typename R, int D, int P0, int P1, int P2>
 __global__ void __launch_bounds__(kThreads)
-    space_fwd_fast(const PlaneJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
-                   const long *__restrict__ cta_plane0, const long *__restrict__ job_planes,
-                   int np_max) {
+    space_fwd_fast(const PlaneJob<R> *__restrict__ jobs, PlaneBatches batches, int np_max) {
   using C = Cx<R>;
   using S = PlaneShape<D, P0, P1, P2>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *buf = reinterpret_cast<C *>(smem_raw);
-  const int jb = cta_job[blockIdx.x];
-  const PlaneJob<R> job = jobs[jb];
-  const long p0 = cta_plane0[blockIdx.x];
-  const int np = (int)min((long)np_max, job_planes[jb] - p0);
-  const int L[3] = {job.L[0], job.L[1], job.L[2]};
-  // load dense [P..] planes
-  const C *src = job.src + p0 * S::dense;
-  const int n_load = np * S::dense;
-  for (int e = threadIdx.x; e < n_load; e += blockDim.x) {
-    const int p = e / S::dense;
-    const int r = e - p * S::dense;
-    buf[p * S::size + plane_pos<D, P0, P1, P2>(r, P1, P2)] = src[e];
-  }
-  __syncthreads();
-  space_axes<R, D, P0, P1, P2, true>(buf, np, L);
-  __syncthreads();
-  // store dense [L..] planes
-  const int dense_out = L[0] * (D >= 2 ? L[1] : 1) * (D == 3 ? L[2] : 1);
-  C *dst = job.dst + p0 * dense_out;
-  const int n_store = np * dense_out;
-  for (int e = threadIdx.x; e < n_store; e += blockDim.x) {
-    const int p = e / dense_out;
-    const int r = e - p * dense_out;
-    dst[e] = buf[p * S::size + plane_pos<D, P0, P1, P2>(r, L[1], L[2])];
+  C *stage[2] = {reinterpret_cast<C *>(smem_raw),
+                 reinterpret_cast<C *>(smem_raw) + np_max * S::size};
+  auto count = [&](int b) {
+    const long p0 = batches.plane0[b];
+    return (int)min((long)np_max, batches.job_planes[batches.job[b]] - p0);
+  };
+  auto issue = [&](int b, C *buf) {
+    const PlaneJob<R> &job = jobs[batches.job[b]];
+    const C *src = job.src + batches.plane0[b] * S::dense;
+    const int n = count(b) * S::dense;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      const int p = e / S::dense;
+      cp_async<sizeof(C)>(buf + p * S::size + plane_pos<D, P0, P1, P2>(e - p * S::dense, P1, P2),
+                          src + e);
+    }
+  };
+  int b = blockIdx.x;
+  if (b < batches.n) issue(b, stage[0]);
+  cp_async_commit();
+  for (int k = 0; b < batches.n; ++k, b += gridDim.x) {
+    const int bn = b + gridDim.x;
+    if (bn < batches.n) issue(bn, stage[(k + 1) & 1]);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    C *buf = stage[k & 1];
+    const PlaneJob<R> &job = jobs[batches.job[b]];
+    const int np = count(b);
+    const int L[3] = {job.L[0], job.L[1], job.L[2]};
+    space_axes<R, D, P0, P1, P2, true>(buf, np, L);
+    __syncthreads();
+    const int dense_out = L[0] * (D >= 2 ? L[1] : 1) * (D == 3 ? L[2] : 1);
+    C *dst = job.dst + batches.plane0[b] * dense_out;
+    const int n_store = np * dense_out;
+    for (int e = threadIdx.x; e < n_store; e += blockDim.x) {
+      const int p = e / dense_out;
+      dst[e] = buf[p * S::size + plane_pos<D, P0, P1, P2>(e - p * dense_out, L[1], L[2])];
+    }
+    __syncthreads();
   }
 }
 
 // Adjoint, all space axes, with the ISTA update fused:
 // X <- soft_threshold(X - step * FFT_space(pad(G[L..])), lamb)   (epilogue
 // kUpdateThreshold), X <- X - step * ..., tracking max |X|^2 (kUpdateMax), or
-// X <- FFT_space(pad(G)) (kStore).
+// X <- FFT_space(pad(G)) (kStore).  Persistent and double buffered like the
+// forward kernel; each stage also prefetches the batch's model planes.
 template <typename R, int D, int P0, int P1, int P2>
 __global__ void __launch_bounds__(kThreads)
-    space_adj_fast(const PlaneJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
-                   const long *__restrict__ cta_plane0, const long *__restrict__ job_planes,
-                   int np_max, int epilogue, R step, R lamb, R *max_out) {
+    space_adj_fast(const PlaneJob<R> *__restrict__ jobs, PlaneBatches batches, int np_max,
+                   int stage_x, int epilogue, R step, R lamb, R *max_out) {
   using C = Cx<R>;
   using S = PlaneShape<D, P0, P1, P2>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *buf = reinterpret_cast<C *>(smem_raw);
-  const int jb = cta_job[blockIdx.x];
-  const PlaneJob<R> job = jobs[jb];
-  const long p0 = cta_plane0[blockIdx.x];
-  const int np = (int)min((long)np_max, job_planes[jb] - p0);
-  const int L[3] = {job.L[0], job.L[1], job.L[2]};
-  const int dense_in = L[0] * (D >= 2 ? L[1] : 1) * (D == 3 ? L[2] : 1);
-  const C *src = job.src + p0 * dense_in;
-  const int n_load = np * dense_in;
-  for (int e = threadIdx.x; e < n_load; e += blockDim.x) {
-    const int p = e / dense_in;
-    const int r = e - p * dense_in;
-    buf[p * S::size + plane_pos<D, P0, P1, P2>(r, L[1], L[2])] = src[e];
-  }
-  __syncthreads();
-  space_axes<R, D, P0, P1, P2, false>(buf, np, L);
-  __syncthreads();
-  C *dst = job.dst + p0 * S::dense;
-  const int n_store = np * S::dense;
+  const int stage_size = np_max * (S::size + (stage_x ? S::dense : 0));
+  C *base = reinterpret_cast<C *>(smem_raw);
+  C *stage[2] = {base, base + stage_size};
+  const bool need_x = epilogue != kStore && stage_x;
+  auto count = [&](int b) {
+    const long p0 = batches.plane0[b];
+    return (int)min((long)np_max, batches.job_planes[batches.job[b]] - p0);
+  };
+  auto issue = [&](int b, C *buf) {
+    const PlaneJob<R> &job = jobs[batches.job[b]];
+    const int np = count(b);
+    const int dense_in = job.L[0] * (D >= 2 ? job.L[1] : 1) * (D == 3 ? job.L[2] : 1);
+    const C *src = job.src + batches.plane0[b] * dense_in;
+    const int n = np * dense_in;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      const int p = e / dense_in;
+      cp_async<sizeof(C)>(
+          buf + p * S::size + plane_pos<D, P0, P1, P2>(e - p * dense_in, job.L[1], job.L[2]),
+          src + e);
+    }
+    if (need_x) {
+      C *xb = buf + np_max * S::size;
+      const C *x = job.dst + batches.plane0[b] * S::dense;
+      for (int e = threadIdx.x; e < np * S::dense; e += blockDim.x)
+        cp_async<sizeof(C)>(xb + e, x + e);
+    }
+  };
   const R lamb_sq = lamb * lamb;
   R local_max = (R)0;
-  for (int e = threadIdx.x; e < n_store; e += blockDim.x) {
-    const int p = e / S::dense;
-    const int r = e - p * S::dense;
-    const C g = buf[p * S::size + plane_pos<D, P0, P1, P2>(r, P1, P2)];
-    if (epilogue == kStore) {
-      dst[e] = g;
-    } else {
-      const C x = dst[e];
-      C xn = cmake<C>(sub_rn<R>(x.x, mul_rn<R>(step, g.x)), sub_rn<R>(x.y, mul_rn<R>(step, g.y)));
-      if (epilogue == kUpdateThreshold) {
-        xn = soft_threshold<R>(xn, lamb, lamb_sq);
+  int b = blockIdx.x;
+  if (b < batches.n) issue(b, stage[0]);
+  cp_async_commit();
+  for (int k = 0; b < batches.n; ++k, b += gridDim.x) {
+    const int bn = b + gridDim.x;
+    if (bn < batches.n) issue(bn, stage[(k + 1) & 1]);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    C *buf = stage[k & 1];
+    const C *xb = buf + np_max * S::size;
+    const PlaneJob<R> &job = jobs[batches.job[b]];
+    const int np = count(b);
+    const int L[3] = {job.L[0], job.L[1], job.L[2]};
+    space_axes<R, D, P0, P1, P2, false>(buf, np, L);
+    __syncthreads();
+    C *dst = job.dst + batches.plane0[b] * S::dense;
+    const int n_store = np * S::dense;
+    for (int e = threadIdx.x; e < n_store; e += blockDim.x) {
+      const int p = e / S::dense;
+      const C g = buf[p * S::size + plane_pos<D, P0, P1, P2>(e - p * S::dense, P1, P2)];
+      if (epilogue == kStore) {
+        dst[e] = g;
       } else {
-        const R a2 = abs_sq<R>(xn);
-        local_max = a2 > local_max ? a2 : local_max;
+        const C x = stage_x ? xb[e] : dst[e];
+        C xn = cmake<C>(sub_rn<R>(x.x, mul_rn<R>(step, g.x)),
+                        sub_rn<R>(x.y, mul_rn<R>(step, g.y)));
+        if (epilogue == kUpdateThreshold) {
+          xn = soft_threshold<R>(xn, lamb, lamb_sq);
+        } else {
+          const R a2 = abs_sq<R>(xn);
+          local_max = a2 > local_max ? a2 : local_max;
+        }
+        dst[e] = xn;
       }
-      dst[e] = xn;
     }
+    __syncthreads();
   }
   if (epilogue == kUpdateMax) {
     __shared__ R red[32];
@@ -419,10 +493,25 @@ __global__ void __launch_bounds__(kThreads)
 
 // ------------------------------------------------------------ time axis
 
+// Twiddles W_N^k, k < N, copied to shared memory for lookups whose index
+// differs between threads (constant memory serialises such accesses).
+template <typename R, int N>
+__device__ __forceinline__ void load_twiddles(Cx<R> *tw) {
+  for (int k = threadIdx.x; k < N; k += blockDim.x) tw[k] = ctw<R>(tw_offset(N) + k);
+}
+
+template <bool INV, typename C>
+__device__ __forceinline__ C tw_at(const C *tw, int k) {
+  C w = tw[k];
+  if (INV) w.y = -w.y;
+  return w;
+}
+
 // Four-step FFT of length M = M1 * M2 on nl lines of shared memory (line
-// stride LS).  Output X[k1 + M1 k2] is left at position M2 k1 + k2.
+// stride LS), twiddles W_M from shared memory.  Output X[k1 + M1 k2] is left
+// at position M2 k1 + k2.
 template <typename R, int M1, int M2, bool INV>
-__device__ __forceinline__ void lines_fourstep(Cx<R> *buf, int nl, int LS) {
+__device__ __forceinline__ void lines_fourstep(Cx<R> *buf, int nl, int LS, const Cx<R> *twM) {
   using C = Cx<R>;
   constexpr int M = M1 * M2;
   for (int w = threadIdx.x; w < nl * M2; w += blockDim.x) {
@@ -435,7 +524,7 @@ __device__ __forceinline__ void lines_fourstep(Cx<R> *buf, int nl, int LS) {
     dft<R, M1, INV>(v);
 #pragma unroll
     for (int k1 = 0; k1 < M1; ++k1)
-      b[M2 * k1 + n2] = (k1 == 0) ? v[0] : cmul(v[k1], wN<R, M, INV>(n2 * k1));
+      b[M2 * k1 + n2] = (k1 == 0) ? v[0] : cmul(v[k1], tw_at<INV>(twM, (n2 * k1) % M));
   }
   __syncthreads();
   for (int w = threadIdx.x; w < nl * M1; w += blockDim.x) {
@@ -460,7 +549,8 @@ __device__ __forceinline__ int fourstep_pos(int k) {
 // Forward time axis for even Pt = 2 M and Lt = 2 h: per trace and time
 // window, c2r of the F = M + 1 bins through a length-M complex FFT, then
 // taper and overlap-add; segment [t h, (t+1) h) of a trace is final once
-// window t is added, so only a one-hop carry stays in shared memory.
+// window t is added, so only a one-hop carry stays in shared memory.  The
+// bins of window t + 1 are copied in (cp.async) while window t is processed.
 template <typename R, int M1, int M2>
 __global__ void __launch_bounds__(kThreads)
     time_fwd_fast(const TimeJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
@@ -473,17 +563,29 @@ __global__ void __launch_bounds__(kThreads)
   const int t0 = cta_trace0[blockIdx.x];
   const int nb = min(nb_max, job.n_traces - t0);
   const int h = job.h;
-  C *buf = reinterpret_cast<C *>(smem_raw);
-  R *carry = reinterpret_cast<R *>(buf + nb_max * LS);  // [nb][h]
-  for (int i = threadIdx.x; i < nb * h; i += blockDim.x) carry[i] = (R)0;
-  for (int t = 0; t < job.T; ++t) {
+  __shared__ C twM[M];
+  __shared__ C tw2M[2 * M];
+  load_twiddles<R, M>(twM);
+  load_twiddles<R, 2 * M>(tw2M);
+  C *stage[2] = {reinterpret_cast<C *>(smem_raw), reinterpret_cast<C *>(smem_raw) + nb_max * LS};
+  R *carry = reinterpret_cast<R *>(stage[1] + nb_max * LS);  // [nb][h]
+  auto issue = [&](int t, C *buf) {
     const C *zt = job.z + (long)t * job.F * job.n_traces + t0;
     for (int idx = threadIdx.x; idx < nb * LS; idx += blockDim.x) {
       const int f = idx / nb;
       const int i = idx - f * nb;
-      buf[i * LS + f] = zt[(long)f * job.n_traces + i];
+      cp_async<sizeof(C)>(buf + i * LS + f, zt + (long)f * job.n_traces + i);
     }
+  };
+  for (int i = threadIdx.x; i < nb * h; i += blockDim.x) carry[i] = (R)0;
+  issue(0, stage[0]);
+  cp_async_commit();
+  for (int t = 0; t < job.T; ++t) {
+    if (t + 1 < job.T) issue(t + 1, stage[(t + 1) & 1]);
+    cp_async_commit();
+    cp_async_wait<1>();
     __syncthreads();
+    C *buf = stage[t & 1];
     // Hermitian combine into M complex values (pairs k, M - k per thread):
     // Z_k = (X_k + conj X_{M-k}) + i e^{+2 pi i k / Pt} (X_k - conj X_{M-k})
     for (int w = threadIdx.x; w < nb * (M / 2 + 1); w += blockDim.x) {
@@ -501,19 +603,15 @@ __global__ void __launch_bounds__(kThreads)
         const C bc = cmake<C>(bc_src.x, -bc_src.y);
         const C e = cadd(a, bc);
         const C d = csub(a, bc);
-        const C w2 = wN<R, 2 * M, true>(kidx);
-        const C o = cmul(d, w2);
+        const C o = cmul(d, tw_at<true>(tw2M, kidx));
         return cmake<C>(e.x - o.y, e.y + o.x);
       };
       const C za = comb(xa, xb, k);
-      if (k != 0 && k != kk) {
-        const C zb = comb(xb, xa, kk);
-        b[kk] = zb;
-      }
+      if (k != 0 && k != kk) b[kk] = comb(xb, xa, kk);
       b[k] = za;  // k == 0 pairs with the Nyquist bin, which is then unused
     }
     __syncthreads();
-    lines_fourstep<R, M1, M2, true>(buf, nb, LS);
+    lines_fourstep<R, M1, M2, true>(buf, nb, LS, twM);
     // taper, overlap-add, write the completed segment of each trace; one
     // thread owns samples j and j + h, so the carry is read then rewritten
     // by the same thread
@@ -525,8 +623,7 @@ __global__ void __launch_bounds__(kThreads)
       const C z_hi = buf[i * LS + fourstep_pos<M1, M2>((j + h) >> 1)];
       const R u_lo = (j & 1) ? z_lo.y : z_lo.x;
       const R u_hi = ((j + h) & 1) ? z_hi.y : z_hi.x;
-      job.y[(long)(t0 + i) * job.C + t * h + j] =
-          carry[idx] + (u_lo * sc) * job.time_taper[j];
+      job.y[(long)(t0 + i) * job.C + t * h + j] = carry[idx] + (u_lo * sc) * job.time_taper[j];
       carry[idx] = (u_hi * sc) * job.time_taper[j + h];
     }
     __syncthreads();
@@ -535,7 +632,7 @@ __global__ void __launch_bounds__(kThreads)
   for (int idx = threadIdx.x; idx < nb * h; idx += blockDim.x) {
     const int i = idx / h;
     const int j = idx - i * h;
-    job.y[(long)(t0 + i) * job.C + job.T * h + j] = carry[i * h + j];
+    job.y[(long)(t0 + i) * job.C + job.T * h + j] = carry[idx];
   }
   const int tail = job.C - (job.T + 1) * h;
   for (int idx = threadIdx.x; idx < nb * tail; idx += blockDim.x) {
@@ -548,7 +645,9 @@ __global__ void __launch_bounds__(kThreads)
 // Adjoint time axis for even Pt = 2 M and Lt = 2 h: per trace and window,
 // gather Lt samples (record through the blend coordinates, or the trace
 // buffer), taper, pack pairs into M complex values, forward FFT, split into
-// the M + 1 bins and double bins 1..M-1.
+// the M + 1 bins and double bins 1..M-1.  The raw samples of window t + 1
+// are copied in (cp.async, zero-filled outside the blended span) while
+// window t is transformed.
 template <typename R, int M1, int M2>
 __global__ void __launch_bounds__(kThreads)
     time_adj_fast(const TimeJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
@@ -563,45 +662,70 @@ __global__ void __launch_bounds__(kThreads)
   const int nb = min(nb_max, job.n_traces - t0);
   const int h = job.h;
   const int Lt = job.Lt;
-  C *buf = reinterpret_cast<C *>(smem_raw);
+  __shared__ C twM[M];
+  __shared__ C tw2M[2 * M];
+  __shared__ long span_base[64];  // source index of trace sample 0
+  __shared__ int span_lo[64], span_hi[64];  // readable trace samples [lo, hi)
+  load_twiddles<R, M>(twM);
+  load_twiddles<R, 2 * M>(tw2M);
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    const int tr = t0 + i;
+    if (from_record) {
+      const long rec = job.blend_rec[tr];
+      const int ts = job.blend_ts[tr];
+      span_base[i] = rec - ts;
+      span_lo[i] = rec >= 0 ? ts : 0;
+      span_hi[i] = rec >= 0 ? ts + job.blend_n[tr] : 0;
+    } else {
+      span_base[i] = (long)tr * job.C;
+      span_lo[i] = 0;
+      span_hi[i] = job.C;
+    }
+  }
+  __syncthreads();
+  const R *src_base = from_record ? record : job.y;
+  C *line = reinterpret_cast<C *>(smem_raw);
+  R *raw[2] = {reinterpret_cast<R *>(line + nb_max * LS),
+               reinterpret_cast<R *>(line + nb_max * LS) + nb_max * Lt};
+  auto issue = [&](int t, R *rb) {
+    for (int idx = threadIdx.x; idx < nb * Lt; idx += blockDim.x) {
+      const int i = idx / Lt;
+      const int s = t * h + (idx - i * Lt);
+      const bool valid = s >= span_lo[i] && s < span_hi[i];
+      cp_async<sizeof(R)>(rb + idx, src_base + (valid ? span_base[i] + s : 0), valid);
+    }
+  };
+  issue(0, raw[0]);
+  cp_async_commit();
   for (int t = 0; t < job.T; ++t) {
+    if (t + 1 < job.T) issue(t + 1, raw[(t + 1) & 1]);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const R *rb = raw[t & 1];
     for (int idx = threadIdx.x; idx < nb * M; idx += blockDim.x) {
       const int i = idx / M;
       const int m = idx - i * M;
-      const int tr = t0 + i;
-      R v[2] = {(R)0, (R)0};
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int j = 2 * m + q;
-        if (j < Lt) {
-          const int s = t * h + j;
-          R x = (R)0;
-          if (from_record) {
-            const long rec = job.blend_rec[tr];
-            const int ts = job.blend_ts[tr];
-            if (rec >= 0 && s >= ts && s < ts + job.blend_n[tr]) x = record[rec + (s - ts)];
-          } else if (s < job.C) {
-            x = job.y[(long)tr * job.C + s];
-          }
-          v[q] = (x * job.space_scale[tr]) * job.time_taper[j];
-        }
-      }
-      buf[i * LS + m] = cmake<C>(v[0], v[1]);
+      const R sc = job.space_scale[t0 + i];
+      const int j = 2 * m;
+      const R v0 = j < Lt ? (rb[i * Lt + j] * sc) * job.time_taper[j] : (R)0;
+      const R v1 = j + 1 < Lt ? (rb[i * Lt + j + 1] * sc) * job.time_taper[j + 1] : (R)0;
+      line[i * LS + m] = cmake<C>(v0, v1);
     }
     __syncthreads();
-    lines_fourstep<R, M1, M2, false>(buf, nb, LS);
+    lines_fourstep<R, M1, M2, false>(line, nb, LS, twM);
     // split: X_k = (Z_k + conj Z_{M-k}) / 2 - i e^{-2 pi i k / Pt} (Z_k - conj Z_{M-k}) / 2
     C *zt = job.z + (long)t * job.F * job.n_traces + t0;
     for (int idx = threadIdx.x; idx < nb * LS; idx += blockDim.x) {
       const int f = idx / nb;
       const int i = idx - f * nb;
-      const C *b = buf + i * LS;
+      const C *b = line + i * LS;
       const C zk = b[fourstep_pos<M1, M2>(f % M)];
       const C zm = b[fourstep_pos<M1, M2>((M - f) % M)];
       const C zc = cmake<C>(zm.x, -zm.y);
       const C e = cmake<C>((R)0.5 * (zk.x + zc.x), (R)0.5 * (zk.y + zc.y));
       const C o = cmake<C>((R)0.5 * (zk.y - zc.y), (R)-0.5 * (zk.x - zc.x));
-      C x = cadd(e, cmul(wN<R, 2 * M, false>(f), o));
+      C x = cadd(e, cmul(tw_at<false>(tw2M, f), o));
       if (f >= 1 && f <= M - 1) x = cmake<C>(x.x * (R)2, x.y * (R)2);
       zt[(long)f * job.n_traces + i] = x;
     }

@@ -56,7 +56,10 @@ def test_fast_operators_vs_oracle(name, make, dtype):
     tol = 1e-5 if dtype == np.float32 else 1e-11
     sv = make()
     prob = _problem(sv, dtype=dtype)
-    assert prob.info[8] == 1, "fast path not selected"
+    # a double-precision 20x20x20 plane does not fit two shared-memory stages;
+    # that case runs on the generic kernels
+    expect_fast = not (name == "3d_P20x20x20" and dtype == np.float64)
+    assert prob.info[8] == (1 if expect_fast else 0)
     plan = _plan(sv)
     rng = np.random.default_rng(1)
     rec = rng.standard_normal(prob.record_size)
