@@ -16,8 +16,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
-SOURCES = ["plan.cpp", "engine.cu", "blend.cu"]
-HEADERS = ["plan.hpp", "fft.cuh", "kernels.cuh"]
+SOURCES = ["plan.cpp", "engine.cu", "blend.cu", "blend_noalloc.cu"]
+HEADERS = ["plan.hpp", "fft.cuh", "kernels.cuh", "fast.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 LIBS = {

@@ -101,6 +101,29 @@ int agd_plan_export(int n_patches, int const *volumes, int const *n_dims,
                     AGD_TYPE const *const *wavelets, long int *info, int *win,
                     long int *blend);
 
+/* agd_blend for callers that cannot allocate device memory (code running
+ * inside a CUDA stream capture, hosts whose pool owns all device memory,
+ * latency-critical callers).  No counterpart in the reference: it is an
+ * addition of this library.  Same arguments and results as agd_blend, except
+ * that the data are device pointers - data_dev holds all input patches one
+ * after another ([n_traces][n_times] each), data_out_dev receives all output
+ * patches the same way - and `stream` (a cudaStream_t, NULL for the default
+ * stream) orders the work.  It allocates nothing: every intermediate lives
+ * in a fixed 16 MiB device array built into the library; larger problems are
+ * rejected with an error (use agd_blend).  The first call on a device looks
+ * up that array's device address, so make it before any stream capture.
+ * Calls overlapping on one device race on the shared array; each call
+ * returns after its work has finished. */
+int agd_blend_device_noalloc(int n_patches, int const *n_traces, int const *n_times,
+                             long int const *const *shottimes, int const *const *channels,
+                             enum AGDTraceType const *const *trace_types,
+                             AGD_TYPE const *data_dev, enum AGDBlendMode blend_mode,
+                             int taper_length, int n_patches_out, int const *n_traces_out,
+                             int const *n_times_out, long int const *const *shottimes_out,
+                             int const *const *channels_out,
+                             enum AGDTraceType const *const *trace_types_out,
+                             AGD_TYPE *data_out_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
