@@ -188,10 +188,11 @@ class Engine {
 
   // shape-specialised path (fast.cuh), used when every window has the same
   // space and time FFT lengths and an instantiation exists
-  using SpaceFwdFn = void (*)(const PlaneJob<R> *, PlaneBatches, int);
-  using SpaceAdjFn = void (*)(const PlaneJob<R> *, PlaneBatches, int, int, int, R, R, R *);
-  using TimeFwdFn = void (*)(const TimeJob<R> *, const int *, const int *, int);
-  using TimeAdjFn = void (*)(const TimeJob<R> *, const int *, const int *, int, const R *, int);
+  using SpaceFwdFn = void (*)(const PlaneJob<R> *, PlaneBatches);
+  using SpaceAdjFn = void (*)(const PlaneJob<R> *, PlaneBatches, int, R, R, R *);
+  using TimeFwdFn = void (*)(const TimeJob<R> *, const int *, const int *);
+  using TimeAdjFn = void (*)(const TimeJob<R> *, const int *, const int *, const R *, int);
+  static constexpr int kTimeNB = 32;  // traces per block of the fast time kernels
   struct PlaneLaunch {
     DevArray<PlaneJob<R>> jobs;
     DevArray<int> batch_job;
@@ -199,8 +200,7 @@ class Engine {
     DevArray<long> job_planes;
     int n_batch = 0;
     int grid = 0;
-    int np = 0;
-    int stage_x = 0;
+    int nt = 0;
     size_t smem = 0;
     PlaneBatches batches() const {
       return PlaneBatches{batch_job.get(), batch_plane0.get(), job_planes.get(), n_batch};
@@ -211,9 +211,8 @@ class Engine {
   SpaceAdjFn sp_adj = nullptr;
   TimeFwdFn tm_fwd = nullptr;
   TimeAdjFn tm_adj = nullptr;
-  int plane_smem = 0;   // complex per plane in shared memory
-  int plane_dense = 0;  // complex per plane in global memory
-  int first_lines = 1;  // lines per plane of the first space pass
+  int nt_fwd = 0, np_fwd = 0, nt_adj = 0, np_adj = 0;  // threads, planes per batch
+  size_t smem_fwd = 0, smem_adj = 0;
   int n_sm = 148;
   PlaneLaunch pl_fwd, pl_adj, pl_adj_plain;
   TimeLaunch tf_fast, ta_fast;
@@ -316,18 +315,43 @@ class Engine {
     L.smem = per_trace * nb;
   }
 
-  template <int D, int P0, int P1, int P2>
+  // One instantiation of the fast space kernels: padded lengths P0..P2 (the
+  // window lengths are then 4P/5), threads and planes per batch of the
+  // forward (NTF, NPF) and adjoint (NTA, NPA) kernels, chosen so that the
+  // double-buffered stages fill most of the shared memory.
+  template <int D, int P0, int P1, int P2, int NTF, int NPF, int NTA, int NPA>
   bool space_case(const WindowPlan &W) {
+    using Sh = PlaneShape<D, P0, P1, P2>;
     const int P[3] = {P0, P1, P2};
     if (W.D != D) return false;
     for (int d = 0; d < D; ++d)
       if (W.P[d] != P[d]) return false;
-    sp_fwd = space_fwd_fast<R, D, P0, P1, P2>;
-    sp_adj = space_adj_fast<R, D, P0, P1, P2>;
-    plane_smem = PlaneShape<D, P0, P1, P2>::size;
-    plane_dense = PlaneShape<D, P0, P1, P2>::dense;
-    first_lines = D == 1 ? 1 : (D == 2 ? P0 : P0 * P1);
+    sp_fwd = space_fwd_fast<R, D, P0, P1, P2, NTF, NPF>;
+    sp_adj = space_adj_fast<R, D, P0, P1, P2, NTA, NPA>;
+    nt_fwd = NTF;
+    np_fwd = NPF;
+    nt_adj = NTA;
+    np_adj = NPA;
+    smem_fwd = 2 * (size_t)NPF * Sh::size * sizeof(C);
+    smem_adj = (2 * (size_t)NPA * Sh::size + (size_t)NPA * Sh::dense_P) * sizeof(C);
     return true;
+  }
+
+  bool space_cases(const WindowPlan &W) {
+    if constexpr (sizeof(R) == sizeof(float)) {
+      return space_case<1, 40, 1, 1, 256, 256, 192, 192>(W) ||
+             space_case<1, 20, 1, 1, 256, 256, 256, 256>(W) ||
+             space_case<2, 20, 40, 1, 384, 16, 384, 11>(W) ||
+             space_case<2, 20, 20, 1, 384, 24, 384, 20>(W) ||
+             space_case<2, 40, 40, 1, 320, 8, 256, 5>(W) ||
+             space_case<3, 20, 20, 20, 512, 1, 512, 1>(W);
+    } else {
+      return space_case<1, 40, 1, 1, 256, 128, 192, 96>(W) ||
+             space_case<1, 20, 1, 1, 256, 256, 256, 160>(W) ||
+             space_case<2, 20, 40, 1, 384, 8, 384, 5>(W) ||
+             space_case<2, 20, 20, 1, 384, 12, 384, 10>(W) ||
+             space_case<2, 40, 40, 1, 320, 4, 256, 2>(W);
+    }
   }
 
   bool pick_fast() {
@@ -337,38 +361,30 @@ class Engine {
     const WindowPlan &W0 = plan.windows[0];
     for (const WindowPlan &W : plan.windows) {
       if (W.D != W0.D || W.Pt != W0.Pt || W.Lt != W0.Lt || W.Lt % 2 != 0) return false;
+      // the kernels assume L = 4P/5 in space and Lt = 2h = 4Pt/5 in time
+      if (W.Lt * 5 != W.Pt * 4) return false;
       for (int d = 0; d < W.D; ++d)
-        if (W.P[d] != W0.P[d]) return false;
+        if (W.P[d] != W0.P[d] || W.L[d] * 5 != W.P[d] * 4) return false;
     }
-    const bool space = space_case<1, 40, 1, 1>(W0) || space_case<1, 20, 1, 1>(W0) ||
-                       space_case<2, 20, 40, 1>(W0) || space_case<2, 20, 20, 1>(W0) ||
-                       space_case<2, 40, 40, 1>(W0) || space_case<3, 20, 20, 20>(W0);
-    if (!space) return false;
-    if (2 * (size_t)plane_smem * sizeof(C) > (size_t)smem_max) return false;
+    if (!space_cases(W0)) return false;
     if (W0.Pt == 320) {
-      tm_fwd = time_fwd_fast<R, 16, 10>;
-      tm_adj = time_adj_fast<R, 16, 10>;
+      tm_fwd = time_fwd_fast<R, 16, 10, kTimeNB>;
+      tm_adj = time_adj_fast<R, 16, 10, kTimeNB>;
     } else if (W0.Pt == 160) {
-      tm_fwd = time_fwd_fast<R, 8, 10>;
-      tm_adj = time_adj_fast<R, 8, 10>;
+      tm_fwd = time_fwd_fast<R, 8, 10, kTimeNB>;
+      tm_adj = time_adj_fast<R, 8, 10, kTimeNB>;
     } else {
       return false;
     }
     return true;
   }
 
-  // Persistent, double-buffered plane batches: a stage holds np planes (and,
-  // for the adjoint, their model values); grid = resident blocks.
+  // Persistent, double-buffered batches of np planes; grid = resident blocks.
   template <typename K>
   void make_plane_launch(PlaneLaunch &L, const std::vector<PlaneJob<R>> &jobs,
-                         const std::vector<long> &planes, bool adjoint, K kernel) {
-    // the adjoint stages the model values too when two such stages fit
-    L.stage_x = adjoint && 2 * (size_t)(plane_smem + plane_dense) * sizeof(C) <= (size_t)smem_max;
-    const size_t plane_bytes = (size_t)(plane_smem + (L.stage_x ? plane_dense : 0)) * sizeof(C);
-    const size_t stage_budget = 96 * 1024;
-    int np = std::max(1, 2 * kThreads / first_lines);
-    np = std::min<int>(np, (int)std::max<size_t>(1, stage_budget / plane_bytes));
-    if (2 * plane_bytes * np > (size_t)smem_max) throw DeviceError("space planes too large");
+                         const std::vector<long> &planes, int nt, int np, size_t smem,
+                         K kernel) {
+    if (smem > (size_t)smem_max) throw DeviceError("space planes too large");
     std::vector<int> bj;
     std::vector<long> bp;
     for (size_t i = 0; i < jobs.size(); ++i)
@@ -381,10 +397,10 @@ class Engine {
     L.batch_plane0.upload(bp, stream);
     L.job_planes.upload(planes, stream);
     L.n_batch = (int)bj.size();
-    L.np = np;
-    L.smem = 2 * plane_bytes * np;
+    L.nt = nt;
+    L.smem = smem;
     int per_sm = 1;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, L.smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, nt, L.smem));
     L.grid = std::max(1, std::min(L.n_batch, std::max(per_sm, 1) * n_sm));
   }
 
@@ -413,7 +429,6 @@ class Engine {
       const WindowPlan &W = plan.windows[w];
       planes[w] = (long)W.T * W.F;
       PlaneJob<R> j{};
-      for (int d = 0; d < 3; ++d) j.L[d] = d < W.D ? W.L[d] : 1;
       j.src = X.get() + W.model_off;
       j.dst = S0.get() + W.model_off;
       jf[w] = j;
@@ -422,22 +437,36 @@ class Engine {
       ja[w] = j;
       tj[w].z = S0.get() + W.model_off;
     }
-    make_plane_launch(pl_fwd, jf, planes, false, sp_fwd);
-    make_plane_launch(pl_adj, ja, planes, true, sp_adj);
+    make_plane_launch(pl_fwd, jf, planes, nt_fwd, np_fwd, smem_fwd, sp_fwd);
+    make_plane_launch(pl_adj, ja, planes, nt_adj, np_adj, smem_adj, sp_adj);
     pending_plane_plain = ja;
     pending_planes = planes;
     time_jobs_fast.upload(tj, stream);
-    int h_max = 1;
-    for (const WindowPlan &W : plan.windows) h_max = std::max(h_max, W.h);
+    const int h = plan.windows[0].h;
     const int LS = plan.windows[0].Pt / 2 + 1;
-    const size_t per_fwd = 2 * (size_t)LS * sizeof(C) + (size_t)h_max * sizeof(R);
-    const size_t per_adj = (size_t)LS * sizeof(C) + 2 * (size_t)(2 * h_max) * sizeof(R);
-    make_time_launch(tf_fast, per_fwd, 32);
-    make_time_launch(ta_fast, per_adj, 32);
+    const size_t per_fwd = 2 * (size_t)LS * sizeof(C) + (size_t)h * sizeof(R);
+    const size_t per_adj = (size_t)LS * sizeof(C) + 2 * (size_t)(2 * h) * sizeof(R);
+    make_fixed_time_launch(tf_fast, per_fwd * kTimeNB);
+    make_fixed_time_launch(ta_fast, per_adj * kTimeNB);
   }
 
   std::vector<PlaneJob<R>> pending_plane_plain;
   std::vector<long> pending_planes;
+
+  void make_fixed_time_launch(TimeLaunch &L, size_t smem) {
+    if (smem > (size_t)smem_max) throw DeviceError("time window too long for shared memory");
+    std::vector<int> cj, ct;
+    for (size_t w = 0; w < plan.windows.size(); ++w)
+      for (int t = 0; t < plan.windows[w].n_traces; t += kTimeNB) {
+        cj.push_back((int)w);
+        ct.push_back(t);
+      }
+    L.cta_job.upload(cj, stream);
+    L.cta_trace0.upload(ct, stream);
+    L.n_cta = (int)cj.size();
+    L.nb = kTimeNB;
+    L.smem = smem;
+  }
 
   void make_gather(GatherLaunch &G, const std::vector<Contrib> &list, long record_size) {
     G.n_chunk = (int)((record_size + G.chunk - 1) / G.chunk);
@@ -715,7 +744,7 @@ class Engine {
     if (fast) {
       std::vector<PlaneJob<R>> jobs = pending_plane_plain;
       for (size_t w = 0; w < jobs.size(); ++w) jobs[w].dst = G.get() + plan.windows[w].model_off;
-      make_plane_launch(pl_adj_plain, jobs, pending_planes, true, sp_adj);
+      make_plane_launch(pl_adj_plain, jobs, pending_planes, nt_adj, np_adj, smem_adj, sp_adj);
       CK(cudaStreamSynchronize(stream));
       return;
     }
@@ -758,15 +787,14 @@ class Engine {
 
   void launch_space_fwd() {
     if (pl_fwd.n_batch == 0) return;
-    sp_fwd<<<pl_fwd.grid, kThreads, pl_fwd.smem, stream>>>(pl_fwd.jobs.get(), pl_fwd.batches(),
-                                                           pl_fwd.np);
+    sp_fwd<<<pl_fwd.grid, pl_fwd.nt, pl_fwd.smem, stream>>>(pl_fwd.jobs.get(), pl_fwd.batches());
     CK(cudaGetLastError());
   }
 
   void launch_space_adj(const PlaneLaunch &L, int epilogue, R step, R lamb) {
     if (L.n_batch == 0) return;
-    sp_adj<<<L.grid, kThreads, L.smem, stream>>>(L.jobs.get(), L.batches(), L.np, L.stage_x,
-                                                 epilogue, step, lamb, scalar.get());
+    sp_adj<<<L.grid, L.nt, L.smem, stream>>>(L.jobs.get(), L.batches(), epilogue, step, lamb,
+                                             scalar.get());
     CK(cudaGetLastError());
   }
 
@@ -774,7 +802,7 @@ class Engine {
     if (fast) {
       if (tf_fast.n_cta)
         tm_fwd<<<tf_fast.n_cta, kThreads, tf_fast.smem, stream>>>(
-            time_jobs_fast.get(), tf_fast.cta_job.get(), tf_fast.cta_trace0.get(), tf_fast.nb);
+            time_jobs_fast.get(), tf_fast.cta_job.get(), tf_fast.cta_trace0.get());
     } else if (time_fwd.n_cta) {
       time_c2r_ola<R><<<time_fwd.n_cta, kThreads, time_fwd.smem, stream>>>(
           time_jobs.get(), time_fwd.cta_job.get(), time_fwd.cta_trace0.get(), time_fwd.nb,
@@ -822,8 +850,8 @@ class Engine {
     if (fast) {
       if (ta_fast.n_cta)
         tm_adj<<<ta_fast.n_cta, kThreads, ta_fast.smem, stream>>>(
-            time_jobs_fast.get(), ta_fast.cta_job.get(), ta_fast.cta_trace0.get(), ta_fast.nb,
-            record, wavelets ? 0 : 1);
+            time_jobs_fast.get(), ta_fast.cta_job.get(), ta_fast.cta_trace0.get(), record,
+            wavelets ? 0 : 1);
       CK(cudaGetLastError());
     } else if (time_adj.n_cta) {
       time_r2c<R><<<time_adj.n_cta, kThreads, time_adj.smem, stream>>>(

@@ -237,12 +237,22 @@ template <typename R>
 struct PlaneJob {
   const Cx<R> *src;  // forward: model planes [P..]; adjoint: Z planes [L..]
   Cx<R> *dst;        // forward: Z planes [L..]; adjoint: model planes (update)
-  int L[3];
 };
 
-// Shared-memory plane layout [P0][P1][P2 + pad] (dims beyond D are 1): the
-// last axis is padded to an odd length so threads walking different rows hit
-// different banks.
+// Batches of planes for the persistent space kernels: batch b covers planes
+// [plane0[b], plane0[b] + NP) of job job[b] (fewer at the end of a job).
+struct PlaneBatches {
+  const int *job;
+  const long *plane0;
+  const long *job_planes;
+  int n;
+};
+
+// Shape of the (t, f) planes one instantiation handles: D space axes of
+// padded length P_d; the window length is L_d = 4 P_d / 5, the only length
+// whose padded length ceil(1.25 L) is P_d for the instantiated sizes.
+// Shared-memory layout [P0][P1][P2 + pad]: the last axis is padded to an odd
+// length so threads walking different rows hit different banks.
 template <int D, int P0, int P1, int P2>
 struct PlaneShape {
   static constexpr int PL = D == 1 ? P0 : (D == 2 ? P1 : P2);  // last axis
@@ -250,86 +260,22 @@ struct PlaneShape {
   static constexpr int E0 = D == 1 ? PLS : P0;
   static constexpr int E1 = D == 1 ? 1 : (D == 2 ? PLS : P1);
   static constexpr int E2 = D == 3 ? PLS : 1;
+  static constexpr int S0 = E1 * E2;  // smem stride of axis 0 (D >= 2)
+  static constexpr int S1 = E2;       // smem stride of axis 1 (D == 3)
   static constexpr int size = E0 * E1 * E2;  // complex per plane in smem
-  static constexpr int dense = P0 * (D >= 2 ? P1 : 1) * (D == 3 ? P2 : 1);
+  static constexpr int L0 = P0 * 4 / 5;
+  static constexpr int L1 = D >= 2 ? P1 * 4 / 5 : 1;
+  static constexpr int L2 = D == 3 ? P2 * 4 / 5 : 1;
+  static constexpr int Q1 = D >= 2 ? P1 : 1;
+  static constexpr int Q2 = D == 3 ? P2 : 1;
+  static constexpr int dense_P = P0 * Q1 * Q2;  // model plane
+  static constexpr int dense_L = L0 * L1 * L2;  // cropped plane
 };
 
-// FFT of lines along `axis` of every plane in smem.  Lines run over the
-// current extents of the other axes; n_in elements are read (zero beyond),
-// n_out written.
-template <typename R, int N, bool INV>
-__device__ __forceinline__ void lines_fft(Cx<R> *buf, int n_planes, int plane_size, int e_outer,
-                                          int e_inner, int stride_outer, int stride_line,
-                                          int stride_inner, int n_in, int n_out) {
-  using C = Cx<R>;
-  const int per_plane = e_outer * e_inner;
-  const int total = n_planes * per_plane;
-  for (int l = threadIdx.x; l < total; l += blockDim.x) {
-    const int p = l / per_plane;
-    const int r = l - p * per_plane;
-    const int o = r / e_inner;
-    const int i = r - o * e_inner;
-    C *line = buf + p * plane_size + o * stride_outer + i * stride_inner;
-    C v[N];
-#pragma unroll
-    for (int e = 0; e < N; ++e) v[e] = e < n_in ? line[e * stride_line] : cmake<C>((R)0, (R)0);
-    dft<R, N, INV>(v);
-#pragma unroll
-    for (int e = 0; e < N; ++e)
-      if (e < n_out) line[e * stride_line] = v[e];
-  }
-}
-
-// All space axes of one window, forward operator direction (inverse FFT,
-// crop) or adjoint direction (zero-pad, forward FFT).  Axis a of the smem
-// plane has stride S_a and extent P_a (full) or L_a (cropped / not yet
-// padded).
-template <typename R, int D, int P0, int P1, int P2, bool FWD>
-__device__ __forceinline__ void space_axes(Cx<R> *buf, int np, const int (&L)[3]) {
-  using S = PlaneShape<D, P0, P1, P2>;
-  constexpr int S0 = S::E1 * S::E2;
-  constexpr int S1 = S::E2;
-  constexpr int P[3] = {P0, P1, P2};
-  if constexpr (FWD) {
-    // last axis first; axes after the current one are already cropped
-    if constexpr (D == 1) {
-      lines_fft<R, P0, true>(buf, np, S::size, 1, 1, 0, 1, 0, P0, L[0]);
-    } else if constexpr (D == 2) {
-      lines_fft<R, P1, true>(buf, np, S::size, P0, 1, S0, 1, 0, P1, L[1]);
-      __syncthreads();
-      lines_fft<R, P0, true>(buf, np, S::size, 1, L[1], 0, S0, 1, P0, L[0]);
-    } else {
-      lines_fft<R, P2, true>(buf, np, S::size, P0 * P1, 1, S1, 1, 0, P2, L[2]);
-      __syncthreads();
-      // axis 1: lines over (i0 < P0, i2 < L2)
-      lines_fft<R, P1, true>(buf, np, S::size, P0, L[2], S0, S1, 1, P1, L[1]);
-      __syncthreads();
-      // axis 0: lines over (i1 < L1, i2 < L2), i2 fastest
-      lines_fft<R, P0, true>(buf, np, S::size, L[1], L[2], S1, S0, 1, P0, L[0]);
-    }
-  } else {
-    if constexpr (D == 1) {
-      lines_fft<R, P0, false>(buf, np, S::size, 1, 1, 0, 1, 0, L[0], P0);
-    } else if constexpr (D == 2) {
-      // axis 0 first over the L1 filled columns, then axis 1 over all P0 rows
-      lines_fft<R, P0, false>(buf, np, S::size, 1, L[1], 0, S0, 1, L[0], P0);
-      __syncthreads();
-      lines_fft<R, P1, false>(buf, np, S::size, P0, 1, S0, 1, 0, L[1], P1);
-    } else {
-      lines_fft<R, P0, false>(buf, np, S::size, L[1], L[2], S1, S0, 1, L[0], P0);
-      __syncthreads();
-      lines_fft<R, P1, false>(buf, np, S::size, P0, L[2], S0, S1, 1, L[1], P1);
-      __syncthreads();
-      lines_fft<R, P2, false>(buf, np, S::size, P0 * P1, 1, S1, 1, 0, L[2], P2);
-    }
-  }
-  (void)P;
-}
-
-// smem position of dense element e of a plane with per-axis extents X0..X2
-// (row-major, last axis fastest) in the padded layout
-template <int D, int P0, int P1, int P2>
-__device__ __forceinline__ int plane_pos(int e, int X1, int X2) {
+// smem position of dense element e of a plane with extents (X0, X1, X2)
+// (row-major, last axis fastest)
+template <int D, int P0, int P1, int P2, int X1, int X2>
+__device__ __forceinline__ int plane_pos(int e) {
   using S = PlaneShape<D, P0, P1, P2>;
   if constexpr (D == 1) {
     return e;
@@ -344,38 +290,89 @@ __device__ __forceinline__ int plane_pos(int e, int X1, int X2) {
   }
 }
 
-// Batches of planes for the persistent space kernels: batch b covers planes
-// [plane0[b], plane0[b] + np) of job job[b].
-struct PlaneBatches {
-  const int *job;
-  const long *plane0;
-  const long *job_planes;
-  int n;
-};
+// FFT of length N of the lines along one axis of np planes in smem: lines
+// run over EO x EI positions of the other axes (smem strides SO, SI), line
+// elements have stride SL; NIN elements are read (zero beyond), NOUT written.
+template <typename R, int N, bool INV, int NT, int NP, int PLANE, int EO, int EI, int SO, int SL,
+          int SI, int NIN, int NOUT>
+__device__ __forceinline__ void lines_fft(Cx<R> *buf, int np) {
+  using C = Cx<R>;
+  constexpr int PER = EO * EI;
+  const int total = np * PER;
+  for (int l = threadIdx.x; l < total; l += NT) {
+    const int p = l / PER;
+    const int r = l - p * PER;
+    const int o = r / EI;
+    const int i = r - o * EI;
+    C *line = buf + p * PLANE + o * SO + i * SI;
+    C v[N];
+#pragma unroll
+    for (int e = 0; e < N; ++e) v[e] = e < NIN ? line[e * SL] : cmake<C>((R)0, (R)0);
+    dft<R, N, INV>(v);
+#pragma unroll
+    for (int e = 0; e < NOUT; ++e) line[e * SL] = v[e];
+  }
+}
+
+// All space axes of np planes: forward operator direction (inverse FFT with
+// cropping, last axis first) or adjoint direction (zero-padding, forward FFT,
+// first axis first).
+template <typename R, int D, int P0, int P1, int P2, int NT, int NP, bool FWD>
+__device__ __forceinline__ void space_axes(Cx<R> *buf, int np) {
+  using S = PlaneShape<D, P0, P1, P2>;
+  constexpr int Z = S::size;
+  if constexpr (FWD) {
+    if constexpr (D == 1) {
+      lines_fft<R, P0, true, NT, NP, Z, 1, 1, 0, 1, 0, P0, S::L0>(buf, np);
+    } else if constexpr (D == 2) {
+      lines_fft<R, P1, true, NT, NP, Z, P0, 1, S::S0, 1, 0, P1, S::L1>(buf, np);
+      __syncthreads();
+      lines_fft<R, P0, true, NT, NP, Z, 1, S::L1, 0, S::S0, 1, P0, S::L0>(buf, np);
+    } else {
+      lines_fft<R, P2, true, NT, NP, Z, P0 * P1, 1, S::S1, 1, 0, P2, S::L2>(buf, np);
+      __syncthreads();
+      lines_fft<R, P1, true, NT, NP, Z, P0, S::L2, S::S0, S::S1, 1, P1, S::L1>(buf, np);
+      __syncthreads();
+      lines_fft<R, P0, true, NT, NP, Z, S::L1, S::L2, S::S1, S::S0, 1, P0, S::L0>(buf, np);
+    }
+  } else {
+    if constexpr (D == 1) {
+      lines_fft<R, P0, false, NT, NP, Z, 1, 1, 0, 1, 0, S::L0, P0>(buf, np);
+    } else if constexpr (D == 2) {
+      lines_fft<R, P0, false, NT, NP, Z, 1, S::L1, 0, S::S0, 1, S::L0, P0>(buf, np);
+      __syncthreads();
+      lines_fft<R, P1, false, NT, NP, Z, P0, 1, S::S0, 1, 0, S::L1, P1>(buf, np);
+    } else {
+      lines_fft<R, P0, false, NT, NP, Z, S::L1, S::L2, S::S1, S::S0, 1, S::L0, P0>(buf, np);
+      __syncthreads();
+      lines_fft<R, P1, false, NT, NP, Z, P0, S::L2, S::S0, S::S1, 1, S::L1, P1>(buf, np);
+      __syncthreads();
+      lines_fft<R, P2, false, NT, NP, Z, P0 * P1, 1, S::S1, 1, 0, S::L2, P2>(buf, np);
+    }
+  }
+}
 
 // Forward operator, all space axes: Z[L..] = crop(IFFT_space(X[P..])).
-// Persistent blocks walk the batches; the planes of the next batch are
-// copied into the second shared buffer (cp.async) while the current one is
-// transformed.
-template <typename R, int D, int P0, int P1, int P2>
-__global__ void __launch_bounds__(kThreads)
-    space_fwd_fast(const PlaneJob<R> *__restrict__ jobs, PlaneBatches batches, int np_max) {
+// Persistent blocks of NT threads walk batches of NP planes; the planes of
+// the next batch are copied into the second shared buffer (cp.async) while
+// the current one is transformed.  Shared memory: 2 NP planes.
+template <typename R, int D, int P0, int P1, int P2, int NT, int NP>
+__global__ void __launch_bounds__(NT, 1)
+    space_fwd_fast(const PlaneJob<R> *__restrict__ jobs, PlaneBatches batches) {
   using C = Cx<R>;
   using S = PlaneShape<D, P0, P1, P2>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *stage[2] = {reinterpret_cast<C *>(smem_raw),
-                 reinterpret_cast<C *>(smem_raw) + np_max * S::size};
+  C *stage[2] = {reinterpret_cast<C *>(smem_raw), reinterpret_cast<C *>(smem_raw) + NP * S::size};
   auto count = [&](int b) {
-    const long p0 = batches.plane0[b];
-    return (int)min((long)np_max, batches.job_planes[batches.job[b]] - p0);
+    return (int)min((long)NP, batches.job_planes[batches.job[b]] - batches.plane0[b]);
   };
   auto issue = [&](int b, C *buf) {
-    const PlaneJob<R> &job = jobs[batches.job[b]];
-    const C *src = job.src + batches.plane0[b] * S::dense;
-    const int n = count(b) * S::dense;
-    for (int e = threadIdx.x; e < n; e += blockDim.x) {
-      const int p = e / S::dense;
-      cp_async<sizeof(C)>(buf + p * S::size + plane_pos<D, P0, P1, P2>(e - p * S::dense, P1, P2),
+    const C *src = jobs[batches.job[b]].src + batches.plane0[b] * S::dense_P;
+    const int n = count(b) * S::dense_P;
+    for (int e = threadIdx.x; e < n; e += NT) {
+      const int p = e / S::dense_P;
+      cp_async<sizeof(C)>(buf + p * S::size + plane_pos<D, P0, P1, P2, S::Q1, S::Q2>(
+                                                  e - p * S::dense_P),
                           src + e);
     }
   };
@@ -389,17 +386,14 @@ __global__ void __launch_bounds__(kThreads)
     cp_async_wait<1>();
     __syncthreads();
     C *buf = stage[k & 1];
-    const PlaneJob<R> &job = jobs[batches.job[b]];
     const int np = count(b);
-    const int L[3] = {job.L[0], job.L[1], job.L[2]};
-    space_axes<R, D, P0, P1, P2, true>(buf, np, L);
+    space_axes<R, D, P0, P1, P2, NT, NP, true>(buf, np);
     __syncthreads();
-    const int dense_out = L[0] * (D >= 2 ? L[1] : 1) * (D == 3 ? L[2] : 1);
-    C *dst = job.dst + batches.plane0[b] * dense_out;
-    const int n_store = np * dense_out;
-    for (int e = threadIdx.x; e < n_store; e += blockDim.x) {
-      const int p = e / dense_out;
-      dst[e] = buf[p * S::size + plane_pos<D, P0, P1, P2>(e - p * dense_out, L[1], L[2])];
+    C *dst = jobs[batches.job[b]].dst + batches.plane0[b] * S::dense_L;
+    const int n_store = np * S::dense_L;
+    for (int e = threadIdx.x; e < n_store; e += NT) {
+      const int p = e / S::dense_L;
+      dst[e] = buf[p * S::size + plane_pos<D, P0, P1, P2, S::L1, S::L2>(e - p * S::dense_L)];
     }
     __syncthreads();
   }
@@ -409,39 +403,31 @@ __global__ void __launch_bounds__(kThreads)
 // X <- soft_threshold(X - step * FFT_space(pad(G[L..])), lamb)   (epilogue
 // kUpdateThreshold), X <- X - step * ..., tracking max |X|^2 (kUpdateMax), or
 // X <- FFT_space(pad(G)) (kStore).  Persistent and double buffered like the
-// forward kernel; each stage also prefetches the batch's model planes.
-template <typename R, int D, int P0, int P1, int P2>
-__global__ void __launch_bounds__(kThreads)
-    space_adj_fast(const PlaneJob<R> *__restrict__ jobs, PlaneBatches batches, int np_max,
-                   int stage_x, int epilogue, R step, R lamb, R *max_out) {
+// forward kernel; the model planes of the current batch are copied into a
+// third buffer while its FFTs run.  Shared memory: 2 NP padded planes and NP
+// dense planes.
+template <typename R, int D, int P0, int P1, int P2, int NT, int NP>
+__global__ void __launch_bounds__(NT, 1)
+    space_adj_fast(const PlaneJob<R> *__restrict__ jobs, PlaneBatches batches, int epilogue,
+                   R step, R lamb, R *max_out) {
   using C = Cx<R>;
   using S = PlaneShape<D, P0, P1, P2>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int stage_size = np_max * (S::size + (stage_x ? S::dense : 0));
   C *base = reinterpret_cast<C *>(smem_raw);
-  C *stage[2] = {base, base + stage_size};
-  const bool need_x = epilogue != kStore && stage_x;
+  C *stage[2] = {base, base + NP * S::size};
+  C *xbuf = base + 2 * NP * S::size;
+  const bool need_x = epilogue != kStore;
   auto count = [&](int b) {
-    const long p0 = batches.plane0[b];
-    return (int)min((long)np_max, batches.job_planes[batches.job[b]] - p0);
+    return (int)min((long)NP, batches.job_planes[batches.job[b]] - batches.plane0[b]);
   };
   auto issue = [&](int b, C *buf) {
-    const PlaneJob<R> &job = jobs[batches.job[b]];
-    const int np = count(b);
-    const int dense_in = job.L[0] * (D >= 2 ? job.L[1] : 1) * (D == 3 ? job.L[2] : 1);
-    const C *src = job.src + batches.plane0[b] * dense_in;
-    const int n = np * dense_in;
-    for (int e = threadIdx.x; e < n; e += blockDim.x) {
-      const int p = e / dense_in;
-      cp_async<sizeof(C)>(
-          buf + p * S::size + plane_pos<D, P0, P1, P2>(e - p * dense_in, job.L[1], job.L[2]),
-          src + e);
-    }
-    if (need_x) {
-      C *xb = buf + np_max * S::size;
-      const C *x = job.dst + batches.plane0[b] * S::dense;
-      for (int e = threadIdx.x; e < np * S::dense; e += blockDim.x)
-        cp_async<sizeof(C)>(xb + e, x + e);
+    const C *src = jobs[batches.job[b]].src + batches.plane0[b] * S::dense_L;
+    const int n = count(b) * S::dense_L;
+    for (int e = threadIdx.x; e < n; e += NT) {
+      const int p = e / S::dense_L;
+      cp_async<sizeof(C)>(buf + p * S::size + plane_pos<D, P0, P1, P2, S::L1, S::L2>(
+                                                  e - p * S::dense_L),
+                          src + e);
     }
   };
   const R lamb_sq = lamb * lamb;
@@ -455,22 +441,24 @@ __global__ void __launch_bounds__(kThreads)
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
-    C *buf = stage[k & 1];
-    const C *xb = buf + np_max * S::size;
-    const PlaneJob<R> &job = jobs[batches.job[b]];
     const int np = count(b);
-    const int L[3] = {job.L[0], job.L[1], job.L[2]};
-    space_axes<R, D, P0, P1, P2, false>(buf, np, L);
+    C *dst = jobs[batches.job[b]].dst + batches.plane0[b] * S::dense_P;
+    const int n_store = np * S::dense_P;
+    if (need_x) {
+      for (int e = threadIdx.x; e < n_store; e += NT) cp_async<sizeof(C)>(xbuf + e, dst + e);
+    }
+    cp_async_commit();
+    C *buf = stage[k & 1];
+    space_axes<R, D, P0, P1, P2, NT, NP, false>(buf, np);
+    cp_async_wait<0>();
     __syncthreads();
-    C *dst = job.dst + batches.plane0[b] * S::dense;
-    const int n_store = np * S::dense;
-    for (int e = threadIdx.x; e < n_store; e += blockDim.x) {
-      const int p = e / S::dense;
-      const C g = buf[p * S::size + plane_pos<D, P0, P1, P2>(e - p * S::dense, P1, P2)];
+    for (int e = threadIdx.x; e < n_store; e += NT) {
+      const int p = e / S::dense_P;
+      const C g = buf[p * S::size + plane_pos<D, P0, P1, P2, S::Q1, S::Q2>(e - p * S::dense_P)];
       if (epilogue == kStore) {
         dst[e] = g;
       } else {
-        const C x = stage_x ? xb[e] : dst[e];
+        const C x = xbuf[e];
         C xn = cmake<C>(sub_rn<R>(x.x, mul_rn<R>(step, g.x)),
                         sub_rn<R>(x.y, mul_rn<R>(step, g.y)));
         if (epilogue == kUpdateThreshold) {
@@ -546,38 +534,42 @@ __device__ __forceinline__ int fourstep_pos(int k) {
   return M2 * (k % M1) + k / M1;
 }
 
-// Forward time axis for even Pt = 2 M and Lt = 2 h: per trace and time
-// window, c2r of the F = M + 1 bins through a length-M complex FFT, then
-// taper and overlap-add; segment [t h, (t+1) h) of a trace is final once
-// window t is added, so only a one-hop carry stays in shared memory.  The
-// bins of window t + 1 are copied in (cp.async) while window t is processed.
-template <typename R, int M1, int M2>
+// Forward time axis for Pt = 2 M (M = M1 M2) and Lt = 2 h with h = 4 M / 5
+// (the window length whose padded length is Pt): per trace and time window,
+// c2r of the F = M + 1 bins through a length-M complex FFT, then taper and
+// overlap-add; segment [t h, (t+1) h) of a trace is final once window t is
+// added, so only a one-hop carry stays in shared memory.  Blocks own NB
+// traces; the bins of window t + 1 are copied in (cp.async) while window t is
+// processed.
+template <typename R, int M1, int M2, int NB>
 __global__ void __launch_bounds__(kThreads)
     time_fwd_fast(const TimeJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
-                  const int *__restrict__ cta_trace0, int nb_max) {
+                  const int *__restrict__ cta_trace0) {
   using C = Cx<R>;
   constexpr int M = M1 * M2;
   constexpr int LS = M + 1;  // F bins per line
+  constexpr int H = 4 * M / 5;
+  constexpr int HALF = M / 2 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const TimeJob<R> job = jobs[cta_job[blockIdx.x]];
-  const int t0 = cta_trace0[blockIdx.x];
-  const int nb = min(nb_max, job.n_traces - t0);
-  const int h = job.h;
   __shared__ C twM[M];
   __shared__ C tw2M[2 * M];
   load_twiddles<R, M>(twM);
   load_twiddles<R, 2 * M>(tw2M);
-  C *stage[2] = {reinterpret_cast<C *>(smem_raw), reinterpret_cast<C *>(smem_raw) + nb_max * LS};
-  R *carry = reinterpret_cast<R *>(stage[1] + nb_max * LS);  // [nb][h]
+  const TimeJob<R> job = jobs[cta_job[blockIdx.x]];
+  const int t0 = cta_trace0[blockIdx.x];
+  const int nb = min(NB, job.n_traces - t0);
+  const long ntr = job.n_traces;
+  C *stage[2] = {reinterpret_cast<C *>(smem_raw), reinterpret_cast<C *>(smem_raw) + NB * LS};
+  R *carry = reinterpret_cast<R *>(stage[1] + NB * LS);  // [NB][H]
   auto issue = [&](int t, C *buf) {
-    const C *zt = job.z + (long)t * job.F * job.n_traces + t0;
-    for (int idx = threadIdx.x; idx < nb * LS; idx += blockDim.x) {
-      const int f = idx / nb;
-      const int i = idx - f * nb;
-      cp_async<sizeof(C)>(buf + i * LS + f, zt + (long)f * job.n_traces + i);
+    const C *zt = job.z + (long)t * LS * ntr + t0;
+    for (int idx = threadIdx.x; idx < NB * LS; idx += kThreads) {
+      const int f = idx / NB;
+      const int i = idx - f * NB;
+      if (i < nb) cp_async<sizeof(C)>(buf + i * LS + f, zt + f * ntr + i);
     }
   };
-  for (int i = threadIdx.x; i < nb * h; i += blockDim.x) carry[i] = (R)0;
+  for (int i = threadIdx.x; i < NB * H; i += kThreads) carry[i] = (R)0;
   issue(0, stage[0]);
   cp_async_commit();
   for (int t = 0; t < job.T; ++t) {
@@ -588,9 +580,9 @@ __global__ void __launch_bounds__(kThreads)
     C *buf = stage[t & 1];
     // Hermitian combine into M complex values (pairs k, M - k per thread):
     // Z_k = (X_k + conj X_{M-k}) + i e^{+2 pi i k / Pt} (X_k - conj X_{M-k})
-    for (int w = threadIdx.x; w < nb * (M / 2 + 1); w += blockDim.x) {
-      const int i = w / (M / 2 + 1);
-      const int k = w - i * (M / 2 + 1);
+    for (int w = threadIdx.x; w < NB * HALF; w += kThreads) {
+      const int i = w / HALF;
+      const int k = w - i * HALF;
       C *b = buf + i * LS;
       const int kk = M - k;
       C xa = b[k];
@@ -611,65 +603,74 @@ __global__ void __launch_bounds__(kThreads)
       b[k] = za;  // k == 0 pairs with the Nyquist bin, which is then unused
     }
     __syncthreads();
-    lines_fourstep<R, M1, M2, true>(buf, nb, LS, twM);
+    lines_fourstep<R, M1, M2, true>(buf, NB, LS, twM);
     // taper, overlap-add, write the completed segment of each trace; one
-    // thread owns samples j and j + h, so the carry is read then rewritten
+    // thread owns samples j and j + H, so the carry is read then rewritten
     // by the same thread
-    for (int idx = threadIdx.x; idx < nb * h; idx += blockDim.x) {
-      const int i = idx / h;
-      const int j = idx - i * h;
-      const R sc = job.space_scale[t0 + i];
-      const C z_lo = buf[i * LS + fourstep_pos<M1, M2>(j >> 1)];
-      const C z_hi = buf[i * LS + fourstep_pos<M1, M2>((j + h) >> 1)];
-      const R u_lo = (j & 1) ? z_lo.y : z_lo.x;
-      const R u_hi = ((j + h) & 1) ? z_hi.y : z_hi.x;
-      job.y[(long)(t0 + i) * job.C + t * h + j] = carry[idx] + (u_lo * sc) * job.time_taper[j];
-      carry[idx] = (u_hi * sc) * job.time_taper[j + h];
+    for (int idx = threadIdx.x; idx < NB * H; idx += kThreads) {
+      const int i = idx / H;
+      const int j = idx - i * H;
+      if (i < nb) {
+        const R sc = job.space_scale[t0 + i];
+        const C z_lo = buf[i * LS + fourstep_pos<M1, M2>(j >> 1)];
+        const C z_hi = buf[i * LS + fourstep_pos<M1, M2>((j + H) >> 1)];
+        const R u_lo = (j & 1) ? z_lo.y : z_lo.x;
+        const R u_hi = ((j + H) & 1) ? z_hi.y : z_hi.x;
+        job.y[(long)(t0 + i) * job.C + t * H + j] = carry[idx] + (u_lo * sc) * job.time_taper[j];
+        carry[idx] = (u_hi * sc) * job.time_taper[j + H];
+      }
     }
     __syncthreads();
   }
   // last half window and the zero tail up to C
-  for (int idx = threadIdx.x; idx < nb * h; idx += blockDim.x) {
-    const int i = idx / h;
-    const int j = idx - i * h;
-    job.y[(long)(t0 + i) * job.C + job.T * h + j] = carry[idx];
+  for (int idx = threadIdx.x; idx < NB * H; idx += kThreads) {
+    const int i = idx / H;
+    if (i < nb) job.y[(long)(t0 + i) * job.C + job.T * H + (idx - i * H)] = carry[idx];
   }
-  const int tail = job.C - (job.T + 1) * h;
-  for (int idx = threadIdx.x; idx < nb * tail; idx += blockDim.x) {
+  const int tail = job.C - (job.T + 1) * H;
+  for (int idx = threadIdx.x; idx < nb * tail; idx += kThreads) {
     const int i = idx / tail;
     const int j = idx - i * tail;
-    job.y[(long)(t0 + i) * job.C + (job.T + 1) * h + j] = (R)0;
+    job.y[(long)(t0 + i) * job.C + (job.T + 1) * H + j] = (R)0;
   }
 }
 
-// Adjoint time axis for even Pt = 2 M and Lt = 2 h: per trace and window,
-// gather Lt samples (record through the blend coordinates, or the trace
-// buffer), taper, pack pairs into M complex values, forward FFT, split into
-// the M + 1 bins and double bins 1..M-1.  The raw samples of window t + 1
-// are copied in (cp.async, zero-filled outside the blended span) while
+// Adjoint time axis for Pt = 2 M and Lt = 2 h, h = 4 M / 5: per trace and
+// window, gather Lt samples (record through the blend coordinates, or the
+// trace buffer), taper, pack pairs into M complex values, forward FFT, split
+// into the M + 1 bins and double bins 1..M-1.  The raw samples of window
+// t + 1 are copied in (cp.async, zero-filled outside the blended span) while
 // window t is transformed.
-template <typename R, int M1, int M2>
+template <typename R, int M1, int M2, int NB>
 __global__ void __launch_bounds__(kThreads)
     time_adj_fast(const TimeJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
-                  const int *__restrict__ cta_trace0, int nb_max, const R *__restrict__ record,
+                  const int *__restrict__ cta_trace0, const R *__restrict__ record,
                   int from_record) {
   using C = Cx<R>;
   constexpr int M = M1 * M2;
   constexpr int LS = M + 1;
+  constexpr int H = 4 * M / 5;
+  constexpr int LT = 2 * H;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const TimeJob<R> job = jobs[cta_job[blockIdx.x]];
-  const int t0 = cta_trace0[blockIdx.x];
-  const int nb = min(nb_max, job.n_traces - t0);
-  const int h = job.h;
-  const int Lt = job.Lt;
   __shared__ C twM[M];
   __shared__ C tw2M[2 * M];
-  __shared__ long span_base[64];  // source index of trace sample 0
-  __shared__ int span_lo[64], span_hi[64];  // readable trace samples [lo, hi)
+  __shared__ long span_base[NB];  // source index of trace sample 0
+  __shared__ int span_lo[NB], span_hi[NB];  // readable trace samples [lo, hi)
+  __shared__ R scale[NB];
   load_twiddles<R, M>(twM);
   load_twiddles<R, 2 * M>(tw2M);
-  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+  const TimeJob<R> job = jobs[cta_job[blockIdx.x]];
+  const int t0 = cta_trace0[blockIdx.x];
+  const int nb = min(NB, job.n_traces - t0);
+  const long ntr = job.n_traces;
+  for (int i = threadIdx.x; i < NB; i += kThreads) {
     const int tr = t0 + i;
+    span_lo[i] = 0;
+    span_hi[i] = 0;
+    span_base[i] = 0;
+    scale[i] = (R)0;
+    if (i >= nb) continue;
+    scale[i] = job.space_scale[tr];
     if (from_record) {
       const long rec = job.blend_rec[tr];
       const int ts = job.blend_ts[tr];
@@ -678,19 +679,17 @@ __global__ void __launch_bounds__(kThreads)
       span_hi[i] = rec >= 0 ? ts + job.blend_n[tr] : 0;
     } else {
       span_base[i] = (long)tr * job.C;
-      span_lo[i] = 0;
       span_hi[i] = job.C;
     }
   }
   __syncthreads();
   const R *src_base = from_record ? record : job.y;
   C *line = reinterpret_cast<C *>(smem_raw);
-  R *raw[2] = {reinterpret_cast<R *>(line + nb_max * LS),
-               reinterpret_cast<R *>(line + nb_max * LS) + nb_max * Lt};
+  R *raw[2] = {reinterpret_cast<R *>(line + NB * LS), reinterpret_cast<R *>(line + NB * LS) + NB * LT};
   auto issue = [&](int t, R *rb) {
-    for (int idx = threadIdx.x; idx < nb * Lt; idx += blockDim.x) {
-      const int i = idx / Lt;
-      const int s = t * h + (idx - i * Lt);
+    for (int idx = threadIdx.x; idx < NB * LT; idx += kThreads) {
+      const int i = idx / LT;
+      const int s = t * H + (idx - i * LT);
       const bool valid = s >= span_lo[i] && s < span_hi[i];
       cp_async<sizeof(R)>(rb + idx, src_base + (valid ? span_base[i] + s : 0), valid);
     }
@@ -703,31 +702,35 @@ __global__ void __launch_bounds__(kThreads)
     cp_async_wait<1>();
     __syncthreads();
     const R *rb = raw[t & 1];
-    for (int idx = threadIdx.x; idx < nb * M; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < NB * M; idx += kThreads) {
       const int i = idx / M;
       const int m = idx - i * M;
-      const R sc = job.space_scale[t0 + i];
       const int j = 2 * m;
-      const R v0 = j < Lt ? (rb[i * Lt + j] * sc) * job.time_taper[j] : (R)0;
-      const R v1 = j + 1 < Lt ? (rb[i * Lt + j + 1] * sc) * job.time_taper[j + 1] : (R)0;
+      R v0 = (R)0, v1 = (R)0;
+      if (j < LT) {
+        v0 = (rb[i * LT + j] * scale[i]) * job.time_taper[j];
+        v1 = (rb[i * LT + j + 1] * scale[i]) * job.time_taper[j + 1];
+      }
       line[i * LS + m] = cmake<C>(v0, v1);
     }
     __syncthreads();
-    lines_fourstep<R, M1, M2, false>(line, nb, LS, twM);
+    lines_fourstep<R, M1, M2, false>(line, NB, LS, twM);
     // split: X_k = (Z_k + conj Z_{M-k}) / 2 - i e^{-2 pi i k / Pt} (Z_k - conj Z_{M-k}) / 2
-    C *zt = job.z + (long)t * job.F * job.n_traces + t0;
-    for (int idx = threadIdx.x; idx < nb * LS; idx += blockDim.x) {
-      const int f = idx / nb;
-      const int i = idx - f * nb;
-      const C *b = line + i * LS;
-      const C zk = b[fourstep_pos<M1, M2>(f % M)];
-      const C zm = b[fourstep_pos<M1, M2>((M - f) % M)];
-      const C zc = cmake<C>(zm.x, -zm.y);
-      const C e = cmake<C>((R)0.5 * (zk.x + zc.x), (R)0.5 * (zk.y + zc.y));
-      const C o = cmake<C>((R)0.5 * (zk.y - zc.y), (R)-0.5 * (zk.x - zc.x));
-      C x = cadd(e, cmul(tw_at<false>(tw2M, f), o));
-      if (f >= 1 && f <= M - 1) x = cmake<C>(x.x * (R)2, x.y * (R)2);
-      zt[(long)f * job.n_traces + i] = x;
+    C *zt = job.z + (long)t * LS * ntr + t0;
+    for (int idx = threadIdx.x; idx < NB * LS; idx += kThreads) {
+      const int f = idx / NB;
+      const int i = idx - f * NB;
+      if (i < nb) {
+        const C *b = line + i * LS;
+        const C zk = b[fourstep_pos<M1, M2>(f % M)];
+        const C zm = b[fourstep_pos<M1, M2>((M - f) % M)];
+        const C zc = cmake<C>(zm.x, -zm.y);
+        const C e = cmake<C>((R)0.5 * (zk.x + zc.x), (R)0.5 * (zk.y + zc.y));
+        const C o = cmake<C>((R)0.5 * (zk.y - zc.y), (R)-0.5 * (zk.x - zc.x));
+        C x = cadd(e, cmul(tw_at<false>(tw2M, f), o));
+        if (f >= 1 && f <= M - 1) x = cmake<C>(x.x * (R)2, x.y * (R)2);
+        zt[f * ntr + i] = x;
+      }
     }
     __syncthreads();
   }
