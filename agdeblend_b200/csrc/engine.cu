@@ -188,23 +188,18 @@ class Engine {
 
   // shape-specialised path (fast.cuh), used when every window has the same
   // space and time FFT lengths and an instantiation exists
-  using SpaceFwdFn = void (*)(const PlaneJob<R> *, PlaneBatches);
-  using SpaceAdjFn = void (*)(const PlaneJob<R> *, PlaneBatches, int, R, R, R *);
+  using SpaceFwdFn = void (*)(PlaneBatches<R>);
+  using SpaceAdjFn = void (*)(PlaneBatches<R>, int, R, R, R *);
   using TimeFwdFn = void (*)(const TimeJob<R> *, const int *, const int *);
   using TimeAdjFn = void (*)(const TimeJob<R> *, const int *, const int *, const R *, int);
   static constexpr int kTimeNB = 32;  // traces per block of the fast time kernels
   struct PlaneLaunch {
-    DevArray<PlaneJob<R>> jobs;
-    DevArray<int> batch_job;
-    DevArray<long> batch_plane0;
-    DevArray<long> job_planes;
+    DevArray<PlaneBatch<R>> batch;
     int n_batch = 0;
     int grid = 0;
     int nt = 0;
     size_t smem = 0;
-    PlaneBatches batches() const {
-      return PlaneBatches{batch_job.get(), batch_plane0.get(), job_planes.get(), n_batch};
-    }
+    PlaneBatches<R> batches() const { return PlaneBatches<R>{batch.get(), n_batch}; }
   };
   bool fast = false;
   SpaceFwdFn sp_fwd = nullptr;
@@ -385,18 +380,17 @@ class Engine {
                          const std::vector<long> &planes, int nt, int np, size_t smem,
                          K kernel) {
     if (smem > (size_t)smem_max) throw DeviceError("space planes too large");
-    std::vector<int> bj;
-    std::vector<long> bp;
+    std::vector<PlaneBatch<R>> bt;
     for (size_t i = 0; i < jobs.size(); ++i)
       for (long q = 0; q < planes[i]; q += np) {
-        bj.push_back((int)i);
-        bp.push_back(q);
+        PlaneBatch<R> x{};
+        x.src = jobs[i].src + q * jobs[i].src_plane;
+        x.dst = jobs[i].dst + q * jobs[i].dst_plane;
+        x.count = (int)std::min<long>(np, planes[i] - q);
+        bt.push_back(x);
       }
-    L.jobs.upload(jobs, stream);
-    L.batch_job.upload(bj, stream);
-    L.batch_plane0.upload(bp, stream);
-    L.job_planes.upload(planes, stream);
-    L.n_batch = (int)bj.size();
+    L.batch.upload(bt, stream);
+    L.n_batch = (int)bt.size();
     L.nt = nt;
     L.smem = smem;
     int per_sm = 1;
@@ -423,6 +417,12 @@ class Engine {
       CK(cudaMemcpyToSymbol(c_tw_d, tw.data(), tw.size() * sizeof(C)));
     const int nw = (int)plan.windows.size();
     std::vector<PlaneJob<R>> jf(nw), ja(nw);
+    const WindowPlan &W0 = plan.windows[0];
+    long dense_P = 1, dense_L = 1;
+    for (int d = 0; d < W0.D; ++d) {
+      dense_P *= W0.P[d];
+      dense_L *= W0.L[d];
+    }
     std::vector<long> planes(nw);
     std::vector<TimeJob<R>> tj = tj_generic;
     for (int w = 0; w < nw; ++w) {
@@ -431,9 +431,13 @@ class Engine {
       PlaneJob<R> j{};
       j.src = X.get() + W.model_off;
       j.dst = S0.get() + W.model_off;
+      j.src_plane = dense_P;
+      j.dst_plane = dense_L;
       jf[w] = j;
       j.src = S0.get() + W.model_off;
       j.dst = X.get() + W.model_off;
+      j.src_plane = dense_L;
+      j.dst_plane = dense_P;
       ja[w] = j;
       tj[w].z = S0.get() + W.model_off;
     }
@@ -787,14 +791,13 @@ class Engine {
 
   void launch_space_fwd() {
     if (pl_fwd.n_batch == 0) return;
-    sp_fwd<<<pl_fwd.grid, pl_fwd.nt, pl_fwd.smem, stream>>>(pl_fwd.jobs.get(), pl_fwd.batches());
+    sp_fwd<<<pl_fwd.grid, pl_fwd.nt, pl_fwd.smem, stream>>>(pl_fwd.batches());
     CK(cudaGetLastError());
   }
 
   void launch_space_adj(const PlaneLaunch &L, int epilogue, R step, R lamb) {
     if (L.n_batch == 0) return;
-    sp_adj<<<L.grid, L.nt, L.smem, stream>>>(L.jobs.get(), L.batches(), epilogue, step, lamb,
-                                             scalar.get());
+    sp_adj<<<L.grid, L.nt, L.smem, stream>>>(L.batches(), epilogue, step, lamb, scalar.get());
     CK(cudaGetLastError());
   }
 

@@ -232,19 +232,29 @@ __device__ __forceinline__ void dft(Cx<R> (&v)[N]) {
 
 // ------------------------------------------------------------ space axes
 
-// One window's planes for the fast space kernels.
+// One window's planes for the fast space kernels (host-side description,
+// cut into PlaneBatch records).
 template <typename R>
 struct PlaneJob {
   const Cx<R> *src;  // forward: model planes [P..]; adjoint: Z planes [L..]
   Cx<R> *dst;        // forward: Z planes [L..]; adjoint: model planes (update)
+  long src_plane;    // complex per input plane
+  long dst_plane;    // complex per output plane
 };
 
-// Batches of planes for the persistent space kernels: batch b covers planes
-// [plane0[b], plane0[b] + NP) of job job[b] (fewer at the end of a job).
+// One batch of planes for the persistent space kernels: `count` planes
+// starting at src (input planes) and dst (output planes).
+template <typename R>
+struct PlaneBatch {
+  const Cx<R> *src;
+  Cx<R> *dst;
+  int count;
+  int pad;
+};
+
+template <typename R>
 struct PlaneBatches {
-  const int *job;
-  const long *plane0;
-  const long *job_planes;
+  const PlaneBatch<R> *b;
   int n;
 };
 
@@ -357,45 +367,47 @@ __device__ __forceinline__ void space_axes(Cx<R> *buf, int np) {
 // the next batch are copied into the second shared buffer (cp.async) while
 // the current one is transformed.  Shared memory: 2 NP planes.
 template <typename R, int D, int P0, int P1, int P2, int NT, int NP>
-__global__ void __launch_bounds__(NT, 1)
-    space_fwd_fast(const PlaneJob<R> *__restrict__ jobs, PlaneBatches batches) {
+__global__ void __launch_bounds__(NT, 1) space_fwd_fast(PlaneBatches<R> batches) {
   using C = Cx<R>;
   using S = PlaneShape<D, P0, P1, P2>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *stage[2] = {reinterpret_cast<C *>(smem_raw), reinterpret_cast<C *>(smem_raw) + NP * S::size};
-  auto count = [&](int b) {
-    return (int)min((long)NP, batches.job_planes[batches.job[b]] - batches.plane0[b]);
-  };
-  auto issue = [&](int b, C *buf) {
-    const C *src = jobs[batches.job[b]].src + batches.plane0[b] * S::dense_P;
-    const int n = count(b) * S::dense_P;
+  auto issue = [&](const PlaneBatch<R> &bt, C *buf) {
+    const int n = bt.count * S::dense_P;
     for (int e = threadIdx.x; e < n; e += NT) {
       const int p = e / S::dense_P;
       cp_async<sizeof(C)>(buf + p * S::size + plane_pos<D, P0, P1, P2, S::Q1, S::Q2>(
                                                   e - p * S::dense_P),
-                          src + e);
+                          bt.src + e);
     }
   };
+  const PlaneBatch<R> none{nullptr, nullptr, 0, 0};
   int b = blockIdx.x;
-  if (b < batches.n) issue(b, stage[0]);
+  PlaneBatch<R> cur = b < batches.n ? batches.b[b] : none;
+  PlaneBatch<R> nxt = b + gridDim.x < batches.n ? batches.b[b + gridDim.x] : none;
+  if (b < batches.n) issue(cur, stage[0]);
   cp_async_commit();
   for (int k = 0; b < batches.n; ++k, b += gridDim.x) {
-    const int bn = b + gridDim.x;
-    if (bn < batches.n) issue(bn, stage[(k + 1) & 1]);
+    // batch records are loaded one batch ahead of their use
+    const int b2 = b + 2 * gridDim.x;
+    const PlaneBatch<R> after = b2 < batches.n ? batches.b[b2] : none;
+    if (nxt.count > 0) issue(nxt, stage[(k + 1) & 1]);
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
     C *buf = stage[k & 1];
-    const int np = count(b);
+    const int np = cur.count;
     space_axes<R, D, P0, P1, P2, NT, NP, true>(buf, np);
     __syncthreads();
-    C *dst = jobs[batches.job[b]].dst + batches.plane0[b] * S::dense_L;
+    C *dst = cur.dst;
     const int n_store = np * S::dense_L;
     for (int e = threadIdx.x; e < n_store; e += NT) {
       const int p = e / S::dense_L;
       dst[e] = buf[p * S::size + plane_pos<D, P0, P1, P2, S::L1, S::L2>(e - p * S::dense_L)];
     }
     __syncthreads();
+    cur = nxt;
+    nxt = after;
   }
 }
 
@@ -408,8 +420,7 @@ __global__ void __launch_bounds__(NT, 1)
 // dense planes.
 template <typename R, int D, int P0, int P1, int P2, int NT, int NP>
 __global__ void __launch_bounds__(NT, 1)
-    space_adj_fast(const PlaneJob<R> *__restrict__ jobs, PlaneBatches batches, int epilogue,
-                   R step, R lamb, R *max_out) {
+    space_adj_fast(PlaneBatches<R> batches, int epilogue, R step, R lamb, R *max_out) {
   using C = Cx<R>;
   using S = PlaneShape<D, P0, P1, P2>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -417,32 +428,32 @@ __global__ void __launch_bounds__(NT, 1)
   C *stage[2] = {base, base + NP * S::size};
   C *xbuf = base + 2 * NP * S::size;
   const bool need_x = epilogue != kStore;
-  auto count = [&](int b) {
-    return (int)min((long)NP, batches.job_planes[batches.job[b]] - batches.plane0[b]);
-  };
-  auto issue = [&](int b, C *buf) {
-    const C *src = jobs[batches.job[b]].src + batches.plane0[b] * S::dense_L;
-    const int n = count(b) * S::dense_L;
+  auto issue = [&](const PlaneBatch<R> &bt, C *buf) {
+    const int n = bt.count * S::dense_L;
     for (int e = threadIdx.x; e < n; e += NT) {
       const int p = e / S::dense_L;
       cp_async<sizeof(C)>(buf + p * S::size + plane_pos<D, P0, P1, P2, S::L1, S::L2>(
                                                   e - p * S::dense_L),
-                          src + e);
+                          bt.src + e);
     }
   };
   const R lamb_sq = lamb * lamb;
   R local_max = (R)0;
+  const PlaneBatch<R> none{nullptr, nullptr, 0, 0};
   int b = blockIdx.x;
-  if (b < batches.n) issue(b, stage[0]);
+  PlaneBatch<R> cur = b < batches.n ? batches.b[b] : none;
+  PlaneBatch<R> nxt = b + gridDim.x < batches.n ? batches.b[b + gridDim.x] : none;
+  if (b < batches.n) issue(cur, stage[0]);
   cp_async_commit();
   for (int k = 0; b < batches.n; ++k, b += gridDim.x) {
-    const int bn = b + gridDim.x;
-    if (bn < batches.n) issue(bn, stage[(k + 1) & 1]);
+    const int b2 = b + 2 * gridDim.x;
+    const PlaneBatch<R> after = b2 < batches.n ? batches.b[b2] : none;
+    if (nxt.count > 0) issue(nxt, stage[(k + 1) & 1]);
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
-    const int np = count(b);
-    C *dst = jobs[batches.job[b]].dst + batches.plane0[b] * S::dense_P;
+    const int np = cur.count;
+    C *dst = cur.dst;
     const int n_store = np * S::dense_P;
     if (need_x) {
       for (int e = threadIdx.x; e < n_store; e += NT) cp_async<sizeof(C)>(xbuf + e, dst + e);
@@ -471,6 +482,8 @@ __global__ void __launch_bounds__(NT, 1)
       }
     }
     __syncthreads();
+    cur = nxt;
+    nxt = after;
   }
   if (epilogue == kUpdateMax) {
     __shared__ R red[32];
@@ -553,12 +566,16 @@ __global__ void __launch_bounds__(kThreads)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ C twM[M];
   __shared__ C tw2M[2 * M];
+  __shared__ R taper[2 * H];
+  __shared__ R scale[NB];
   load_twiddles<R, M>(twM);
   load_twiddles<R, 2 * M>(tw2M);
   const TimeJob<R> job = jobs[cta_job[blockIdx.x]];
   const int t0 = cta_trace0[blockIdx.x];
   const int nb = min(NB, job.n_traces - t0);
   const long ntr = job.n_traces;
+  for (int j = threadIdx.x; j < 2 * H; j += kThreads) taper[j] = job.time_taper[j];
+  for (int i = threadIdx.x; i < NB; i += kThreads) scale[i] = i < nb ? job.space_scale[t0 + i] : (R)0;
   C *stage[2] = {reinterpret_cast<C *>(smem_raw), reinterpret_cast<C *>(smem_raw) + NB * LS};
   R *carry = reinterpret_cast<R *>(stage[1] + NB * LS);  // [NB][H]
   auto issue = [&](int t, C *buf) {
@@ -611,13 +628,13 @@ __global__ void __launch_bounds__(kThreads)
       const int i = idx / H;
       const int j = idx - i * H;
       if (i < nb) {
-        const R sc = job.space_scale[t0 + i];
+        const R sc = scale[i];
         const C z_lo = buf[i * LS + fourstep_pos<M1, M2>(j >> 1)];
         const C z_hi = buf[i * LS + fourstep_pos<M1, M2>((j + H) >> 1)];
         const R u_lo = (j & 1) ? z_lo.y : z_lo.x;
         const R u_hi = ((j + H) & 1) ? z_hi.y : z_hi.x;
-        job.y[(long)(t0 + i) * job.C + t * H + j] = carry[idx] + (u_lo * sc) * job.time_taper[j];
-        carry[idx] = (u_hi * sc) * job.time_taper[j + H];
+        job.y[(long)(t0 + i) * job.C + t * H + j] = carry[idx] + (u_lo * sc) * taper[j];
+        carry[idx] = (u_hi * sc) * taper[j + H];
       }
     }
     __syncthreads();
@@ -657,12 +674,14 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ long span_base[NB];  // source index of trace sample 0
   __shared__ int span_lo[NB], span_hi[NB];  // readable trace samples [lo, hi)
   __shared__ R scale[NB];
+  __shared__ R taper[LT];
   load_twiddles<R, M>(twM);
   load_twiddles<R, 2 * M>(tw2M);
   const TimeJob<R> job = jobs[cta_job[blockIdx.x]];
   const int t0 = cta_trace0[blockIdx.x];
   const int nb = min(NB, job.n_traces - t0);
   const long ntr = job.n_traces;
+  for (int j = threadIdx.x; j < LT; j += kThreads) taper[j] = job.time_taper[j];
   for (int i = threadIdx.x; i < NB; i += kThreads) {
     const int tr = t0 + i;
     span_lo[i] = 0;
@@ -687,11 +706,19 @@ __global__ void __launch_bounds__(kThreads)
   C *line = reinterpret_cast<C *>(smem_raw);
   R *raw[2] = {reinterpret_cast<R *>(line + NB * LS), reinterpret_cast<R *>(line + NB * LS) + NB * LT};
   auto issue = [&](int t, R *rb) {
-    for (int idx = threadIdx.x; idx < NB * LT; idx += kThreads) {
-      const int i = idx / LT;
-      const int s = t * H + (idx - i * LT);
-      const bool valid = s >= span_lo[i] && s < span_hi[i];
-      cp_async<sizeof(R)>(rb + idx, src_base + (valid ? span_base[i] + s : 0), valid);
+    // four consecutive samples per thread and step
+    for (int g = threadIdx.x; g < NB * (LT / 4); g += kThreads) {
+      const int i = g / (LT / 4);
+      const int j0 = 4 * (g - i * (LT / 4));
+      const int s0 = t * H + j0;
+      const int lo = span_lo[i];
+      const int hi = span_hi[i];
+      const R *src = src_base + span_base[i] + s0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const bool valid = s0 + q >= lo && s0 + q < hi;
+        cp_async<sizeof(R)>(rb + i * LT + j0 + q, valid ? src + q : src_base, valid);
+      }
     }
   };
   issue(0, raw[0]);
@@ -708,8 +735,8 @@ __global__ void __launch_bounds__(kThreads)
       const int j = 2 * m;
       R v0 = (R)0, v1 = (R)0;
       if (j < LT) {
-        v0 = (rb[i * LT + j] * scale[i]) * job.time_taper[j];
-        v1 = (rb[i * LT + j + 1] * scale[i]) * job.time_taper[j + 1];
+        v0 = (rb[i * LT + j] * scale[i]) * taper[j];
+        v1 = (rb[i * LT + j + 1] * scale[i]) * taper[j + 1];
       }
       line[i * LS + m] = cmake<C>(v0, v1);
     }
