@@ -189,7 +189,7 @@ class Engine {
   // shape-specialised path (fast.cuh), used when every window has the same
   // space and time FFT lengths and an instantiation exists
   using SpaceFwdFn = void (*)(PlaneBatches<R>);
-  using SpaceAdjFn = void (*)(PlaneBatches<R>, int, R, R, R *);
+  using SpaceAdjFn = void (*)(PlaneBatches<R>, int, R, R, const R *, R *);
   using TimeFwdFn = void (*)(const TimeJob<R> *, const int *, const int *);
   using TimeAdjFn = void (*)(const TimeJob<R> *, const int *, const int *, const R *, int);
   static constexpr int kTimeNB = 32;  // traces per block of the fast time kernels
@@ -236,6 +236,7 @@ class Engine {
   ~Engine() {
     if (stream) {
       cudaStreamSynchronize(stream);
+      release_graph();
       cudaStreamDestroy(stream);
     }
   }
@@ -772,11 +773,12 @@ class Engine {
 
   // ---------------------------------------------------------------- launches
 
-  void launch_axis(const AxisLaunch &L, int inverse, int epilogue, R step, R lamb) {
+  void launch_axis(const AxisLaunch &L, int inverse, int epilogue, R step, R lamb,
+                   const R *lamb_dev = nullptr) {
     if (L.n_cta == 0) return;
     axis_pass<R><<<L.n_cta, kThreads, L.smem, stream>>>(
         L.jobs.get(), L.cta_job.get(), L.cta_line0.get(), L.lpc, d_descs.get(), d_tw.get(),
-        inverse, epilogue, step, lamb, scalar.get());
+        inverse, epilogue, step, lamb, lamb_dev, scalar.get());
     CK(cudaGetLastError());
   }
 
@@ -795,9 +797,11 @@ class Engine {
     CK(cudaGetLastError());
   }
 
-  void launch_space_adj(const PlaneLaunch &L, int epilogue, R step, R lamb) {
+  void launch_space_adj(const PlaneLaunch &L, int epilogue, R step, R lamb,
+                        const R *lamb_dev = nullptr) {
     if (L.n_batch == 0) return;
-    sp_adj<<<L.grid, L.nt, L.smem, stream>>>(L.batches(), epilogue, step, lamb, scalar.get());
+    sp_adj<<<L.grid, L.nt, L.smem, stream>>>(L.batches(), epilogue, step, lamb, lamb_dev,
+                                             scalar.get());
     CK(cudaGetLastError());
   }
 
@@ -864,16 +868,78 @@ class Engine {
     }
   }
 
-  // X <- threshold(X - step * A^H record, lamb)
-  void adjoint_update(const R *record, R step, R lamb, bool track_max) {
+  // X <- threshold(X - step * A^H record, lamb); lambda is read from
+  // lamb_dev instead when given (graph replays)
+  void adjoint_update(const R *record, R step, R lamb, bool track_max,
+                      const R *lamb_dev = nullptr) {
     adjoint_time(record);
     if (fast) {
-      launch_space_adj(pl_adj, track_max ? kUpdateMax : kUpdateThreshold, step, lamb);
+      launch_space_adj(pl_adj, track_max ? kUpdateMax : kUpdateThreshold, step, lamb, lamb_dev);
       return;
     }
     for (size_t k = 0; k < adj_update.size(); ++k)
-      launch_axis(adj_update[k], 0, track_max ? kUpdateMax : kUpdateThreshold, step, lamb);
+      launch_axis(adj_update[k], 0, track_max ? kUpdateMax : kUpdateThreshold, step, lamb,
+                  lamb_dev);
   }
+
+  // ---------------------------------------------------------------- graphs
+
+  // One ISTA iteration (forward, residual, next lambda, adjoint update)
+  // captured once and replayed; lambda comes from a device table indexed by
+  // a device counter the graph advances.
+  DevArray<R> lamb_table, lamb_cur;
+  DevArray<int> lamb_counter;
+  cudaGraphExec_t iter_graph = nullptr;
+
+  void release_graph() {
+    if (iter_graph != nullptr) {
+      cudaGraphExecDestroy(iter_graph);
+      iter_graph = nullptr;
+    }
+  }
+
+  // table[k] = lambda used after iteration k + 1.  The captured graph holds
+  // the table's address, so the table keeps its allocation while it is
+  // large enough; growing it drops the graph (re-captured on next use).
+  void load_schedule(const std::vector<R> &table) {
+    if (table.size() > lamb_table.size()) {
+      release_graph();
+      CK(cudaStreamSynchronize(stream));
+      lamb_table.alloc(table.size());
+    }
+    CK(cudaMemcpyAsync(lamb_table.get(), table.data(), table.size() * sizeof(R),
+                       cudaMemcpyHostToDevice, stream));
+    if (lamb_cur.get() == nullptr) lamb_cur.alloc(1);
+    if (lamb_counter.get() == nullptr) lamb_counter.alloc(1);
+    CK(cudaMemsetAsync(lamb_counter.get(), 0, sizeof(int), stream));
+  }
+
+  void iteration_body(bool want_norm) {
+    forward_traces();
+    residual(want_norm);
+    next_lambda<R><<<1, 32, 0, stream>>>(lamb_table.get(), lamb_counter.get(), lamb_cur.get());
+    CK(cudaGetLastError());
+    adjoint_update(rec_r.get(), stepsize, (R)0, false, lamb_cur.get());
+  }
+
+  void capture_iteration() {
+    if (iter_graph != nullptr) return;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      iteration_body(false);
+    } catch (...) {
+      cudaStreamEndCapture(stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    CK(cudaStreamEndCapture(stream, &g));
+    const cudaError_t e = cudaGraphInstantiate(&iter_graph, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+  }
+
+  void replay_iteration() { CK(cudaGraphLaunch(iter_graph, stream)); }
 
   void residual(bool want_norm) {
     double *ss = nullptr;
@@ -995,27 +1061,44 @@ class Engine {
     CK(cudaGetLastError());
   }
 
-  // the solver of agd_deblend (src/agdeblend.c:584-633)
-  void solve(R initial_factor, int n_its, int print_freq) {
-    R lamb = initial_step();
+  // Thresholds after the initial step: the schedule of src/agdeblend.c:
+  // 526-533,588-589,623-627 evaluated in AGD_TYPE on the host.
+  static std::vector<R> schedule_table(R lamb0, R initial_factor, int n_its, R *first) {
     const Schedule sc = lambda_schedule(initial_factor, n_its);
-    const R linear_slope = sc.linear_slope * lamb;
-    lamb *= initial_factor;
-    threshold_model(lamb);
-    if (print_freq > 0) {
-      const double r = record_norm(rec_d.get());
-      std::printf("Iteration 0 Residual %f\n", r);
-    }
+    const R linear_slope = sc.linear_slope * lamb0;
+    R lamb = lamb0 * initial_factor;
+    *first = lamb;
+    std::vector<R> t(n_its > 1 ? n_its - 1 : 1, (R)0);
     for (int it = 1; it < n_its; ++it) {
-      const bool print_residual = print_freq > 0 && it % print_freq == 0;
-      forward_traces();
-      residual(print_residual);
-      if (print_residual) std::printf("Iteration %d Residual %f\n", it, std::sqrt(read_dscalar()));
       if (it < sc.first_linear_it)
         lamb *= sc.decay;
       else
         lamb = (R)(n_its - 1 - it) * linear_slope;
-      adjoint_update(rec_r.get(), stepsize, lamb, false);
+      t[it - 1] = lamb;
+    }
+    return t;
+  }
+
+  // the solver of agd_deblend (src/agdeblend.c:584-633); iterations replay a
+  // captured CUDA graph unless residuals are printed
+  void solve(R initial_factor, int n_its, int print_freq) {
+    R lamb0 = initial_step();
+    R first = 0;
+    const std::vector<R> table = schedule_table(lamb0, initial_factor, n_its, &first);
+    threshold_model(first);
+    load_schedule(table);
+    if (print_freq > 0) {
+      const double r = record_norm(rec_d.get());
+      std::printf("Iteration 0 Residual %f\n", r);
+      for (int it = 1; it < n_its; ++it) {
+        const bool print_residual = it % print_freq == 0;
+        iteration_body(print_residual);
+        if (print_residual)
+          std::printf("Iteration %d Residual %f\n", it, std::sqrt(read_dscalar()));
+      }
+    } else if (n_its > 1) {
+      capture_iteration();
+      for (int it = 1; it < n_its; ++it) replay_iteration();
     }
     output();
   }
@@ -1244,34 +1327,30 @@ int agd_gpu_solve(agd_gpu_problem *pb, AGD_TYPE initial_factor, int n_its, int p
 int agd_gpu_time_iterations(agd_gpu_problem *pb, AGD_TYPE const *const *data,
                             AGD_TYPE initial_factor, int n_its, int warmup, int steps,
                             double *timing) {
-  if (pb == nullptr || data == nullptr || timing == nullptr || steps <= 0 || n_its < 2)
+  if (pb == nullptr || data == nullptr || timing == nullptr || steps <= 0 || n_its < 2 ||
+      warmup < 0)
     return 1;
   return guarded("agd_gpu_time_iterations", [&] {
     agd::EngineR &e = *pb->eng;
     e.upload_data(data);
     pb->input_blend();
-    AGD_TYPE lamb = e.initial_step();
-    const agd::Schedule sc = agd::lambda_schedule(initial_factor, n_its);
-    const AGD_TYPE slope = sc.linear_slope * lamb;
-    lamb *= initial_factor;
-    e.threshold_model(lamb);
-    auto lamb_at = [&](int it) {
-      AGD_TYPE l = lamb;
-      for (int k = 1; k <= it; ++k) l = k < sc.first_linear_it ? l * sc.decay : (AGD_TYPE)(n_its - 1 - k) * slope;
-      return l;
-    };
-    int it = 1;
-    auto iterate = [&] {
-      e.forward_traces();
-      e.residual(false);
-      e.adjoint_update(e.rec_r.get(), e.stepsize, lamb_at(it), false);
-      it = it + 1 < n_its ? it + 1 : 1;
-    };
-    for (int i = 0; i < warmup; ++i) iterate();
+    const AGD_TYPE lamb0 = e.initial_step();
+    AGD_TYPE first = 0;
+    const std::vector<AGD_TYPE> sched =
+        agd::EngineR::schedule_table(lamb0, initial_factor, n_its, &first);
+    e.threshold_model(first);
+    // thresholds for every replay: the schedule, repeated if the run is
+    // longer than n_its - 1 iterations
+    const int total = warmup + steps + 2;
+    std::vector<AGD_TYPE> table(total);
+    for (int k = 0; k < total; ++k) table[k] = sched[k % sched.size()];
+    e.load_schedule(table);
+    e.capture_iteration();
+    for (int i = 0; i < warmup; ++i) e.replay_iteration();
     cudaEvent_t ev[4];
     for (auto &v : ev) agd::CK(cudaEventCreate(&v));
     agd::CK(cudaEventRecord(ev[0], e.stream));
-    for (int i = 0; i < steps; ++i) iterate();
+    for (int i = 0; i < steps; ++i) e.replay_iteration();
     agd::CK(cudaEventRecord(ev[1], e.stream));
     // one more iteration split into its forward and adjoint halves
     agd::CK(cudaEventRecord(ev[2], e.stream));
@@ -1283,7 +1362,7 @@ int agd_gpu_time_iterations(agd_gpu_problem *pb, AGD_TYPE const *const *data,
     agd::CK(cudaEventElapsedTime(&ms_total, ev[0], ev[1]));
     agd::CK(cudaEventElapsedTime(&ms_fwd, ev[2], ev[3]));
     agd::CK(cudaEventRecord(ev[2], e.stream));
-    e.adjoint_update(e.rec_r.get(), e.stepsize, lamb_at(it), false);
+    e.adjoint_update(e.rec_r.get(), e.stepsize, table[warmup + steps], false);
     agd::CK(cudaEventRecord(ev[3], e.stream));
     agd::CK(cudaEventSynchronize(ev[3]));
     float ms_adj = 0;

@@ -420,7 +420,8 @@ __global__ void __launch_bounds__(NT, 1) space_fwd_fast(PlaneBatches<R> batches)
 // dense planes.
 template <typename R, int D, int P0, int P1, int P2, int NT, int NP>
 __global__ void __launch_bounds__(NT, 1)
-    space_adj_fast(PlaneBatches<R> batches, int epilogue, R step, R lamb, R *max_out) {
+    space_adj_fast(PlaneBatches<R> batches, int epilogue, R step, R lamb_arg,
+                   const R *lamb_dev, R *max_out) {
   using C = Cx<R>;
   using S = PlaneShape<D, P0, P1, P2>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -437,6 +438,8 @@ __global__ void __launch_bounds__(NT, 1)
                           bt.src + e);
     }
   };
+  // lambda from device memory when replayed from a CUDA graph
+  const R lamb = lamb_dev != nullptr ? *lamb_dev : lamb_arg;
   const R lamb_sq = lamb * lamb;
   R local_max = (R)0;
   const PlaneBatch<R> none{nullptr, nullptr, 0, 0};

@@ -183,7 +183,8 @@ __global__ void __launch_bounds__(kThreads)
     axis_pass(const AxisJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
               const long *__restrict__ cta_line0, int lines_per_cta,
               const FftDesc *__restrict__ descs, const Cx<R> *__restrict__ tw,
-              int inverse, int epilogue, R step, R lamb, R *max_out) {
+              int inverse, int epilogue, R step, R lamb_arg, const R *lamb_dev,
+              R *max_out) {
   using C = Cx<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const AxisJob<R> job = jobs[cta_job[blockIdx.x]];
@@ -222,6 +223,9 @@ __global__ void __launch_bounds__(kThreads)
 
   R local_max = (R)0;
   const int total_out = nl * job.n_out;
+  // the threshold comes from device memory when the launch is replayed from
+  // a CUDA graph (one captured iteration, a different lambda each replay)
+  const R lamb = lamb_dev != nullptr ? *lamb_dev : lamb_arg;
   const R lamb_sq = lamb * lamb;
   for (int idx = threadIdx.x; idx < total_out; idx += blockDim.x) {
     int i, e;
@@ -552,6 +556,17 @@ __global__ void record_sumsq(const R *__restrict__ x, long n, double *out) {
     s += (double)x[i] * (double)x[i];
   s = block_sum(s, red);
   if (threadIdx.x == 0) atomicAdd(out, s);
+}
+
+// Advances the threshold schedule on the device: out = table[*counter],
+// then ++*counter (one thread; captured in the per-iteration CUDA graph).
+template <typename R>
+__global__ void next_lambda(const R *__restrict__ table, int *counter, R *out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    const int k = *counter;
+    *out = table[k];
+    *counter = k + 1;
+  }
 }
 
 template <typename R>

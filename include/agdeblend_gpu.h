@@ -71,8 +71,9 @@ int agd_gpu_solve(agd_gpu_problem *problem, AGD_TYPE initial_factor, int n_its,
                   int print_freq, AGD_TYPE *const *data);
 
 /* Benchmark hook: loads `data`, runs the set-up step, then `warmup` untimed
- * and `steps` timed ISTA iterations with every input resident on the device.
- * Timing uses CUDA events on the library's stream.  timing[0] = total ms of
+ * and `steps` timed ISTA iterations with every input resident on the device,
+ * each iteration a replay of one captured CUDA graph (as agd_gpu_solve runs
+ * them).  Timing uses CUDA events on the library's stream.  timing[0] = total ms of
  * the timed iterations, timing[1] = ms of the forward half, timing[2] = ms of
  * the adjoint half (separately timed pass), timing[3] = iterations timed. */
 int agd_gpu_time_iterations(agd_gpu_problem *problem, AGD_TYPE const *const *data,

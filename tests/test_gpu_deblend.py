@@ -73,6 +73,23 @@ def test_solve_random_problems(seed, kw):
     prob.close()
 
 
+def test_repeated_solves_and_print_path_agree():
+    """Solves replay one captured CUDA graph per problem; a second solve on
+    the same problem (graph reused, longer schedule) and the printing path
+    (launched without the graph) must give the same output."""
+    sv = S.gather_2d(seed=9, n_shots=48, nt=256, window=(16, 128))
+    prob = A.Problem.from_survey(sv)
+    a = prob.solve(sv.data, 1.0, 15)
+    b = prob.solve(sv.data, 1.0, 15)
+    c = prob.solve(sv.data, 1.0, 40)
+    d = prob.solve(sv.data, 1.0, 40, print_freq=7)
+    ref = O.deblend(_plan(sv), sv.data, 1.0, 40)
+    assert np.array_equal(a[0], b[0])
+    assert rel_l2(c[0], d[0]) <= 1e-6
+    assert rel_l2(c[0], ref[0]) <= 1e-3
+    prob.close()
+
+
 def test_double_library_vs_oracle(small_surveys):
     sv = small_surveys["two_volume_3d"]
     data64 = [d.astype(np.float64) for d in sv.data]
