@@ -32,3 +32,23 @@ def load_ops(name):
                record_forward=z["record_forward"], blend_input=z["blend_input"],
                stepsize=float(z["stepsize"]), output=seq("output", n_p))
     return sv, ref
+
+
+def sketch(arrays, k: int = 64, chunk: int = 1 << 20) -> np.ndarray:
+    """k random +-1 projections of the concatenated arrays (float64).  The
+    signs come from a fixed integer hash of (element index, projection), so
+    they need no random generator and are identical on every machine.  For
+    any x, E |sketch(x)|^2 / k = |x|^2, so |sketch(a) - sketch(b)| /
+    |sketch(b)| estimates the relative L2 difference (to about 1/sqrt(k/2))."""
+    flat = np.concatenate([np.asarray(a, np.float64).reshape(-1) for a in arrays])
+    out = np.zeros(k)
+    mult = np.uint64(0x9E3779B97F4A7C15)
+    with np.errstate(over="ignore"):  # the hash wraps modulo 2^64 on purpose
+        for s0 in range(0, flat.size, chunk):
+            x = flat[s0: s0 + chunk]
+            idx = np.arange(s0, s0 + x.size, dtype=np.uint64)
+            for j in range(k):
+                h = (idx + np.uint64(j) * np.uint64(0x632BE59BD9B4E019)) * mult
+                sign = 1.0 - 2.0 * ((h >> np.uint64(63)).astype(np.float64))
+                out[j] += float(np.dot(sign, x))
+    return out

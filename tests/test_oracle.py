@@ -129,3 +129,19 @@ def test_reference_unit_tests_pass_on_shim():
                        capture_output=True, text=True, env=env, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert "0 failed" in r.stdout
+
+
+def test_sketch_estimates_relative_difference():
+    """The sketch used by the full-size parity test: linear, and its relative
+    difference tracks the true relative L2 difference."""
+    from golden_io import sketch
+
+    rng = np.random.default_rng(77)
+    a = [rng.standard_normal((300, 700)), rng.standard_normal(5000)]
+    e = [1e-3 * rng.standard_normal(x.shape) for x in a]
+    b = [x + y for x, y in zip(a, e)]
+    sa, sb, se = sketch(a), sketch(b), sketch(e)
+    np.testing.assert_allclose(sb - sa, se, atol=1e-9)
+    true = np.sqrt(sum(np.sum(y ** 2) for y in e) / sum(np.sum(x ** 2) for x in a))
+    est = np.linalg.norm(sb - sa) / np.linalg.norm(sa)
+    assert 0.5 * true < est < 2.0 * true
