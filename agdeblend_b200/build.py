@@ -17,7 +17,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 SOURCES = ["plan.cpp", "engine.cu", "blend.cu", "blend_noalloc.cu"]
-HEADERS = ["plan.hpp", "fft.cuh", "kernels.cuh", "fast.cuh"]
+HEADERS = ["plan.hpp", "fft.cuh", "kernels.cuh", "fast.cuh", "wavelet_fast.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 LIBS = {

@@ -20,6 +20,7 @@
 #include "fast.cuh"
 #include "kernels.cuh"
 #include "plan.hpp"
+#include "wavelet_fast.cuh"
 
 namespace agd {
 
@@ -219,6 +220,12 @@ class Engine {
   long data_size = 0;
   long out_traces = 0;
   bool wavelets = false;
+  // prime-factor wavelet kernel (wavelet_fast.cuh), used when every window's
+  // trace length factors into supported coprime prime powers
+  bool wav_fast = false;
+  DevArray<WaveletFastJob<R>> wavf_jobs;
+  DevArray<int> kperm;
+  TimeLaunch wavf;
   R stepsize = 0;
 
   explicit Engine(Plan &&p) : plan(std::move(p)) {
@@ -261,7 +268,113 @@ class Engine {
   void set_smem_limits() {
     const int limit = smem_max;
     smem_max = std::min({opt_in(axis_pass<R>, limit), opt_in(time_c2r_ola<R>, limit),
-                         opt_in(time_r2c<R>, limit), opt_in(wavelet_apply<R>, limit)});
+                         opt_in(time_r2c<R>, limit), opt_in(wavelet_apply<R>, limit),
+                         opt_in(wavelet_fast<R>, limit)});
+  }
+
+  // twiddle tables of the register DFTs in constant memory of the current
+  // device (fast.cuh), shared by the fast space, time and wavelet kernels
+  void upload_twiddles() {
+    std::vector<C> tw(kTwTotal);
+    for (int i = 0, off = 0; i < kNumTw; off += kTwSizes[i], ++i)
+      for (int k = 0; k < kTwSizes[i]; ++k) {
+        const double a = -2.0 * 3.14159265358979323846 * (double)k / (double)kTwSizes[i];
+        tw[off + k].x = (R)std::cos(a);
+        tw[off + k].y = (R)std::sin(a);
+      }
+    if (sizeof(R) == sizeof(float))
+      CK(cudaMemcpyToSymbol(c_tw_f, tw.data(), tw.size() * sizeof(C)));
+    else
+      CK(cudaMemcpyToSymbol(c_tw_d, tw.data(), tw.size() * sizeof(C)));
+  }
+
+  // C = product of pairwise coprime prime powers with a register DFT
+  static bool pfa_shape(int N, PfaShape &sh) {
+    static const int kOk[] = {2, 3, 4, 5, 7, 8, 9, 11, 13, 16, 17, 19, 23, 25, 27, 32};
+    sh = PfaShape{};
+    sh.N = N;
+    int n = N;
+    for (int p = 2; n > 1; ++p) {
+      if (n % p) continue;
+      int q = 1;
+      while (n % p == 0) {
+        n /= p;
+        q *= p;
+      }
+      if (std::find(std::begin(kOk), std::end(kOk), q) == std::end(kOk) ||
+          sh.nf == kPfaMaxFactors)
+        return false;
+      sh.f[sh.nf++] = q;
+    }
+    for (int i = 0; i < sh.nf; ++i) {
+      sh.s[i] = N / sh.f[i];
+      sh.inv[i] = 1;
+      while ((long)sh.s[i] * sh.inv[i] % sh.f[i] != 1 % sh.f[i]) ++sh.inv[i];
+    }
+    return true;
+  }
+
+  // position -> frequency after the forward passes (Chinese remainder map)
+  static void pfa_kperm(const PfaShape &sh, std::vector<int> &out) {
+    const long N = sh.N;
+    for (long p = 0; p < N; ++p) {
+      long k = 0;
+      for (int i = 0; i < sh.nf; ++i) {
+        const long ki = p * sh.inv[i] % sh.f[i];
+        const long ei = (long)sh.s[i] * sh.inv[i] % N;
+        k = (k + ki * ei) % N;
+      }
+      out.push_back((int)k);
+    }
+  }
+
+  void build_wavelet_fast(const std::vector<WaveletJob<R>> &wj,
+                          const std::vector<long> &wt_base) {
+    const char *env = std::getenv("AGD_GPU_GENERIC");
+    if (env != nullptr && env[0] == '1') return;
+    const int nw = (int)plan.windows.size();
+    std::vector<WaveletFastJob<R>> jobs(nw);
+    std::vector<int> perm;
+    std::map<int, long> perm_off;
+    int n_max = 1;
+    for (int w = 0; w < nw; ++w) {
+      WaveletFastJob<R> &j = jobs[w];
+      const int N = plan.windows[w].C;
+      if (!pfa_shape(N, j.sh)) return;
+      if (!perm_off.count(N)) {
+        perm_off[N] = (long)perm.size();
+        pfa_kperm(j.sh, perm);
+      }
+      n_max = std::max(n_max, N);
+    }
+    const size_t per_pair = (size_t)n_max * sizeof(C);
+    const int np = (int)std::max<size_t>(1, std::min<size_t>(4, 60000 / per_pair));
+    if (per_pair * np > (size_t)smem_max) return;
+    kperm.upload(perm, stream);
+    std::vector<int> cj, cp;
+    for (int w = 0; w < nw; ++w) {
+      const WindowPlan &W = plan.windows[w];
+      WaveletFastJob<R> &j = jobs[w];
+      j.y = wj[w].y;
+      j.src = wj[w].src;
+      j.kperm = kperm.get() + perm_off[W.C];
+      j.blend_rec = blend_rec.get() + wt_base[w];
+      j.blend_ts = blend_ts.get() + wt_base[w];
+      j.blend_n = blend_n.get() + wt_base[w];
+      j.n_traces = W.n_traces;
+      for (int p = 0; p < (W.n_traces + 1) / 2; p += np) {
+        cj.push_back(w);
+        cp.push_back(p);
+      }
+    }
+    wavf_jobs.upload(jobs, stream);
+    wavf.cta_job.upload(cj, stream);
+    wavf.cta_trace0.upload(cp, stream);
+    wavf.n_cta = (int)cj.size();
+    wavf.nb = np;
+    wavf.smem = per_pair * np;
+    upload_twiddles();
+    wav_fast = true;
   }
 
   // ---------------------------------------------------------------- set-up
@@ -404,18 +517,7 @@ class Engine {
     const int dyn = std::min({opt_in(sp_fwd, limit), opt_in(sp_adj, limit), opt_in(tm_fwd, limit),
                               opt_in(tm_adj, limit)});
     smem_max = std::min(smem_max, dyn);
-    // twiddle tables in constant memory of the current device
-    std::vector<C> tw(kTwTotal);
-    for (int i = 0, off = 0; i < kNumTw; off += kTwSizes[i], ++i)
-      for (int k = 0; k < kTwSizes[i]; ++k) {
-        const double a = -2.0 * 3.14159265358979323846 * (double)k / (double)kTwSizes[i];
-        tw[off + k].x = (R)std::cos(a);
-        tw[off + k].y = (R)std::sin(a);
-      }
-    if (sizeof(R) == sizeof(float))
-      CK(cudaMemcpyToSymbol(c_tw_f, tw.data(), tw.size() * sizeof(C)));
-    else
-      CK(cudaMemcpyToSymbol(c_tw_d, tw.data(), tw.size() * sizeof(C)));
+    upload_twiddles();
     const int nw = (int)plan.windows.size();
     std::vector<PlaneJob<R>> jf(nw), ja(nw);
     const WindowPlan &W0 = plan.windows[0];
@@ -623,6 +725,7 @@ class Engine {
       }
       spectra.upload(sp, stream);
       spec_off.upload(so, stream);
+      build_wavelet_fast(wj, wt_base);
     }
 
     // ---- space-axis passes (generic path)
@@ -836,7 +939,21 @@ class Engine {
     if (wavelets) launch_wavelet(+1);
   }
 
+  // in place on the window traces (direction +1), or from the record into
+  // the window traces (direction -1, prime-factor kernel only)
+  void launch_wavelet_fast(int direction, const R *record) {
+    if (!wavf.n_cta) return;
+    wavelet_fast<R><<<wavf.n_cta, kWavThreads, wavf.smem, stream>>>(
+        wavf_jobs.get(), wavf.cta_job.get(), wavf.cta_trace0.get(), wavf.nb, spectra.get(),
+        spec_off.get(), direction, record);
+    CK(cudaGetLastError());
+  }
+
   void launch_wavelet(int direction) {
+    if (wav_fast) {
+      launch_wavelet_fast(direction, nullptr);
+      return;
+    }
     if (!wav.n_cta) return;
     wavelet_apply<R><<<wav.n_cta, kThreads, wav.smem, stream>>>(
         wav_jobs.get(), wav.cta_job.get(), wav.cta_trace0.get(), wav.nb, d_descs.get(),
@@ -846,7 +963,9 @@ class Engine {
 
   // Z = F_t^H B^H W^H record, per window (before the space passes)
   void adjoint_time(const R *record) {
-    if (wavelets) {
+    if (wavelets && wav_fast) {
+      launch_wavelet_fast(-1, record);
+    } else if (wavelets) {
       if (n_wtraces)
         extract_traces<R><<<(unsigned)n_wtraces, kThreads, 0, stream>>>(
             blend_rec.get(), blend_ts.get(), blend_n.get(), wt_dst.get(), wt_C.get(), record,
@@ -1240,6 +1359,7 @@ int agd_gpu_problem_info(agd_gpu_problem const *pb, long int *info) {
   info[6] = (long)e.device_bytes();
   info[7] = e.g_fwd.n_contrib;
   info[8] = e.fast ? 1 : 0;
+  info[9] = e.wav_fast ? 1 : 0;
   return 0;
 }
 

@@ -30,7 +30,8 @@ namespace agd {
 // ------------------------------------------------------------ twiddle tables
 
 // Transform lengths with a constant twiddle table W_N^k = exp(-2 pi i k / N).
-constexpr int kTwSizes[] = {6, 10, 12, 15, 16, 20, 24, 25, 32, 40, 48, 64, 80, 160, 320};
+constexpr int kTwSizes[] = {6,  7,  9,  10, 11, 12, 13,  15,  16, 17, 19, 20,
+                             23, 24, 25, 27, 32, 40, 48, 64, 80, 160, 320};
 constexpr int kNumTw = (int)(sizeof(kTwSizes) / sizeof(int));
 
 __host__ __device__ constexpr int tw_offset(int n) {
@@ -115,6 +116,49 @@ __host__ __device__ constexpr int small_split(int n) {
 
 template <typename R, int N, bool INV>
 __device__ __forceinline__ void dft(Cx<R> (&v)[N]);
+
+// Odd length N with a twiddle table: the outputs k and N-k share the sums
+// x_j + x_{N-j} (times cos) and x_j - x_{N-j} (times sin), so
+//   X_k = A_k -/+ i B_k,  X_{N-k} = A_k +/- i B_k   (forward / inverse),
+//   A_k = x_0 + sum_j (x_j + x_{N-j}) cos(2 pi j k / N),
+//   B_k = sum_j (x_j - x_{N-j}) sin(2 pi j k / N),   j = 1 .. (N-1)/2.
+template <typename R, int N, bool INV>
+__device__ __forceinline__ void dft_odd(Cx<R> (&v)[N]) {
+  using C = Cx<R>;
+  static_assert(N % 2 == 1, "odd length");
+  constexpr int H = (N - 1) / 2;
+  constexpr int off = tw_offset(N);
+  C sum[H], dif[H];
+  C tot = v[0];
+#pragma unroll
+  for (int j = 1; j <= H; ++j) {
+    sum[j - 1] = cadd(v[j], v[N - j]);
+    dif[j - 1] = csub(v[j], v[N - j]);
+    tot = cadd(tot, sum[j - 1]);
+  }
+  const C x0 = v[0];
+#pragma unroll
+  for (int k = 1; k <= H; ++k) {
+    C a = x0;
+    C b = cmake<C>((R)0, (R)0);
+#pragma unroll
+    for (int j = 1; j <= H; ++j) {
+      const C w = ctw<R>(off + (j * k) % N);  // (cos, -sin) of 2 pi j k / N
+      a.x += sum[j - 1].x * w.x;
+      a.y += sum[j - 1].y * w.x;
+      b.x -= dif[j - 1].x * w.y;
+      b.y -= dif[j - 1].y * w.y;
+    }
+    if (INV) {
+      v[k] = cmake<C>(a.x - b.y, a.y + b.x);
+      v[N - k] = cmake<C>(a.x + b.y, a.y - b.x);
+    } else {
+      v[k] = cmake<C>(a.x + b.y, a.y - b.x);
+      v[N - k] = cmake<C>(a.x - b.y, a.y + b.x);
+    }
+  }
+  v[0] = tot;
+}
 
 // Four-step in registers: N = N1 * N2, natural order in and out.
 template <typename R, int N1, int N2, bool INV>
@@ -209,6 +253,8 @@ __device__ __forceinline__ void dft(Cx<R> (&v)[N]) {
   } else if constexpr (small_split(N) != 0) {
     constexpr int N1 = small_split(N);
     dft_fourstep<R, N1, N / N1, INV>(v);
+  } else if constexpr (tw_offset(N) >= 0) {
+    dft_odd<R, N, INV>(v);
   } else {
     // prime length without a table: direct DFT (only small primes reach here)
     static_assert(N <= 13, "unsupported register DFT length");
