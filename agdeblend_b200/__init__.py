@@ -185,7 +185,7 @@ class Problem:
         if self.lib.agd_gpu_problem_create(*self.args.problem_args(), ctypes.byref(h)):
             raise RuntimeError("agd_gpu_problem_create failed")
         self.h = h
-        info = np.zeros(10, np.int64)
+        info = np.zeros(14, np.int64)
         self.lib.agd_gpu_problem_info(self.h, info.ctypes.data_as(POINTER(c_long)))
         self.info = info
         self.n_windows = int(info[0])

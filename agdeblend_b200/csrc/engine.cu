@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -424,43 +425,201 @@ class Engine {
     L.smem = per_trace * nb;
   }
 
-  // One instantiation of the fast space kernels: padded lengths P0..P2 (the
-  // window lengths are then 4P/5), threads and planes per batch of the
-  // forward (NTF, NPF) and adjoint (NTA, NPA) kernels, chosen so that the
-  // double-buffered stages fill most of the shared memory.
-  template <int D, int P0, int P1, int P2, int NTF, int NPF, int NTA, int NPA>
-  bool space_case(const WindowPlan &W) {
+  // Candidate instantiations of the fast space kernels for one padded shape
+  // P0..P2 (window lengths 4P/5): threads, planes per batch, stages and
+  // blocks per SM.  The two-stage kernels fill most of the shared memory with
+  // one block per SM; the one-stage kernels run two or three blocks per SM
+  // (two for 40-point lines, whose registers do not fit three).  The
+  // fastest of each list is picked by timing on the problem (autotune_space).
+  struct FwdVariant {
+    SpaceFwdFn fn;
+    int nt, np, stages;
+    size_t smem;
+  };
+  struct AdjVariant {
+    SpaceAdjFn fn;
+    int nt, np, stages;
+    size_t smem;
+  };
+  std::vector<FwdVariant> fwd_vars;
+  std::vector<AdjVariant> adj_vars;
+  int fwd_pick = 0, adj_pick = 0;
+
+  template <int D, int P0, int P1, int P2, int NT, int NP, int ST, int MB>
+  void add_fwd() {
     using Sh = PlaneShape<D, P0, P1, P2>;
+    fwd_vars.push_back(FwdVariant{space_fwd_fast<R, D, P0, P1, P2, NT, NP, ST, MB>, NT, NP, ST,
+                                  (size_t)ST * NP * Sh::size * sizeof(C)});
+  }
+
+  template <int D, int P0, int P1, int P2, int NT, int NP, int ST, int MB>
+  void add_adj() {
+    using Sh = PlaneShape<D, P0, P1, P2>;
+    const size_t x = ST == 2 ? (size_t)NP * Sh::dense_P : 0;
+    adj_vars.push_back(AdjVariant{space_adj_fast<R, D, P0, P1, P2, NT, NP, ST, MB>, NT, NP, ST,
+                                  ((size_t)ST * NP * Sh::size + x) * sizeof(C)});
+  }
+
+  template <int D, int P0, int P1, int P2>
+  static bool shape_is(const WindowPlan &W) {
     const int P[3] = {P0, P1, P2};
     if (W.D != D) return false;
     for (int d = 0; d < D; ++d)
       if (W.P[d] != P[d]) return false;
-    sp_fwd = space_fwd_fast<R, D, P0, P1, P2, NTF, NPF>;
-    sp_adj = space_adj_fast<R, D, P0, P1, P2, NTA, NPA>;
-    nt_fwd = NTF;
-    np_fwd = NPF;
-    nt_adj = NTA;
-    np_adj = NPA;
-    smem_fwd = 2 * (size_t)NPF * Sh::size * sizeof(C);
-    smem_adj = (2 * (size_t)NPA * Sh::size + (size_t)NPA * Sh::dense_P) * sizeof(C);
     return true;
   }
 
   bool space_cases(const WindowPlan &W) {
+    fwd_vars.clear();
+    adj_vars.clear();
     if constexpr (sizeof(R) == sizeof(float)) {
-      return space_case<1, 40, 1, 1, 256, 256, 192, 192>(W) ||
-             space_case<1, 20, 1, 1, 256, 256, 256, 256>(W) ||
-             space_case<2, 20, 40, 1, 384, 16, 384, 11>(W) ||
-             space_case<2, 20, 20, 1, 384, 24, 384, 20>(W) ||
-             space_case<2, 40, 40, 1, 320, 8, 256, 5>(W) ||
-             space_case<3, 20, 20, 20, 512, 1, 512, 1>(W);
+      if (shape_is<1, 40, 1, 1>(W)) {
+        add_fwd<1, 40, 1, 1, 256, 256, 2, 1>();
+        add_fwd<1, 40, 1, 1, 256, 96, 1, 2>();
+        add_adj<1, 40, 1, 1, 192, 192, 2, 1>();
+        add_adj<1, 40, 1, 1, 256, 96, 1, 2>();
+      } else if (shape_is<1, 20, 1, 1>(W)) {
+        add_fwd<1, 20, 1, 1, 256, 256, 2, 1>();
+        add_fwd<1, 20, 1, 1, 256, 128, 1, 3>();
+        add_adj<1, 20, 1, 1, 256, 256, 2, 1>();
+        add_adj<1, 20, 1, 1, 256, 128, 1, 3>();
+      } else if (shape_is<2, 20, 40, 1>(W)) {
+        add_fwd<2, 20, 40, 1, 384, 16, 2, 1>();
+        add_fwd<2, 20, 40, 1, 256, 12, 1, 2>();
+        add_adj<2, 20, 40, 1, 384, 11, 2, 1>();
+        add_adj<2, 20, 40, 1, 256, 12, 1, 2>();
+      } else if (shape_is<2, 20, 20, 1>(W)) {
+        add_fwd<2, 20, 20, 1, 384, 24, 2, 1>();
+        add_fwd<2, 20, 20, 1, 256, 12, 1, 3>();
+        add_adj<2, 20, 20, 1, 384, 20, 2, 1>();
+        add_adj<2, 20, 20, 1, 256, 12, 1, 3>();
+      } else if (shape_is<2, 40, 40, 1>(W)) {
+        add_fwd<2, 40, 40, 1, 320, 8, 2, 1>();
+        add_fwd<2, 40, 40, 1, 256, 6, 1, 2>();
+        add_adj<2, 40, 40, 1, 256, 5, 2, 1>();
+        add_adj<2, 40, 40, 1, 256, 6, 1, 2>();
+      } else if (shape_is<3, 20, 20, 20>(W)) {
+        add_fwd<3, 20, 20, 20, 512, 1, 2, 1>();
+        add_fwd<3, 20, 20, 20, 256, 1, 1, 3>();
+        add_adj<3, 20, 20, 20, 512, 1, 2, 1>();
+        add_adj<3, 20, 20, 20, 256, 1, 1, 3>();
+      }
     } else {
-      return space_case<1, 40, 1, 1, 256, 128, 192, 96>(W) ||
-             space_case<1, 20, 1, 1, 256, 256, 256, 160>(W) ||
-             space_case<2, 20, 40, 1, 384, 8, 384, 5>(W) ||
-             space_case<2, 20, 20, 1, 384, 12, 384, 10>(W) ||
-             space_case<2, 40, 40, 1, 320, 4, 256, 2>(W);
+      // double: the two-stage kernels only (one-stage kernels with several
+      // blocks per SM would spill), and one stage for the 20x20x20 planes
+      if (shape_is<1, 40, 1, 1>(W)) {
+        add_fwd<1, 40, 1, 1, 256, 128, 2, 1>();
+        add_adj<1, 40, 1, 1, 192, 96, 2, 1>();
+      } else if (shape_is<1, 20, 1, 1>(W)) {
+        add_fwd<1, 20, 1, 1, 256, 256, 2, 1>();
+        add_adj<1, 20, 1, 1, 256, 160, 2, 1>();
+      } else if (shape_is<2, 20, 40, 1>(W)) {
+        add_fwd<2, 20, 40, 1, 384, 8, 2, 1>();
+        add_adj<2, 20, 40, 1, 384, 5, 2, 1>();
+      } else if (shape_is<2, 20, 20, 1>(W)) {
+        add_fwd<2, 20, 20, 1, 384, 12, 2, 1>();
+        add_adj<2, 20, 20, 1, 384, 10, 2, 1>();
+      } else if (shape_is<2, 40, 40, 1>(W)) {
+        add_fwd<2, 40, 40, 1, 320, 4, 2, 1>();
+        add_adj<2, 40, 40, 1, 256, 2, 2, 1>();
+      } else if (shape_is<3, 20, 20, 20>(W)) {
+        add_fwd<3, 20, 20, 20, 256, 1, 1, 1>();
+        add_adj<3, 20, 20, 20, 256, 1, 1, 1>();
+      }
     }
+    return !fwd_vars.empty() && !adj_vars.empty();
+  }
+
+  // Times every candidate (one warm-up launch, then two timed ones with CUDA
+  // events on the engine's stream, forward X -> S0 and adjoint S0 -> X with
+  // the update epilogue) and keeps the fastest.  Choices are remembered per
+  // shape, precision, problem size class and device, so later problems of
+  // the same kind skip the timing.  AGD_GPU_SPACE_VARIANT="f,a" forces the
+  // candidates (tests).
+  void autotune_space(const std::vector<PlaneJob<R>> &jf, const std::vector<PlaneJob<R>> &ja,
+                      const std::vector<long> &planes) {
+    fwd_pick = adj_pick = 0;
+    const char *env = std::getenv("AGD_GPU_SPACE_VARIANT");
+    if (env != nullptr && env[0] != '\0') {
+      int f = 0, a = 0;
+      if (std::sscanf(env, "%d,%d", &f, &a) == 2) {
+        fwd_pick = std::max(0, std::min(f, (int)fwd_vars.size() - 1));
+        adj_pick = std::max(0, std::min(a, (int)adj_vars.size() - 1));
+        return;
+      }
+    }
+    if (fwd_vars.size() == 1 && adj_vars.size() == 1) return;
+    long total = 0;
+    for (long v : planes) total += v;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    const WindowPlan &W = plan.windows[0];
+    char key[128];
+    std::snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%d", dev, (int)sizeof(R), W.D, W.P[0],
+                  W.D > 1 ? W.P[1] : 1, W.D > 2 ? W.P[2] : 1,
+                  (int)std::log2((double)std::max(1L, total)));
+    static std::mutex mu;
+    static std::map<std::string, std::pair<int, int>> cache;
+    {
+      std::lock_guard<std::mutex> g(mu);
+      auto it = cache.find(key);
+      if (it != cache.end()) {
+        fwd_pick = it->second.first;
+        adj_pick = it->second.second;
+        return;
+      }
+    }
+    CK(cudaMemsetAsync(X.get(), 0, X.bytes(), stream));
+    CK(cudaMemsetAsync(S0.get(), 0, S0.bytes(), stream));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto timed = [&](auto launch) {
+      launch();
+      CK(cudaEventRecord(e0, stream));
+      launch();
+      launch();
+      CK(cudaEventRecord(e1, stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      return ms;
+    };
+    float best = 1e30f;
+    for (size_t v = 0; v < fwd_vars.size(); ++v) {
+      const FwdVariant &fv = fwd_vars[v];
+      if (fv.smem > (size_t)smem_max) continue;
+      PlaneLaunch L;
+      make_plane_launch(L, jf, planes, fv.nt, fv.np, fv.smem, fv.fn);
+      const float ms = timed([&] {
+        fv.fn<<<L.grid, L.nt, L.smem, stream>>>(L.batches());
+        CK(cudaGetLastError());
+      });
+      if (ms < best) {
+        best = ms;
+        fwd_pick = (int)v;
+      }
+    }
+    best = 1e30f;
+    for (size_t v = 0; v < adj_vars.size(); ++v) {
+      const AdjVariant &av = adj_vars[v];
+      if (av.smem > (size_t)smem_max) continue;
+      PlaneLaunch L;
+      make_plane_launch(L, ja, planes, av.nt, av.np, av.smem, av.fn);
+      const float ms = timed([&] {
+        av.fn<<<L.grid, L.nt, L.smem, stream>>>(L.batches(), kUpdateThreshold, (R)0, (R)0,
+                                                 nullptr, scalar.get());
+        CK(cudaGetLastError());
+      });
+      if (ms < best) {
+        best = ms;
+        adj_pick = (int)v;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> g(mu);
+    cache[key] = {fwd_pick, adj_pick};
   }
 
   bool pick_fast() {
@@ -514,8 +673,9 @@ class Engine {
 
   void build_fast(const std::vector<TimeJob<R>> &tj_generic) {
     const int limit = optin_smem();
-    const int dyn = std::min({opt_in(sp_fwd, limit), opt_in(sp_adj, limit), opt_in(tm_fwd, limit),
-                              opt_in(tm_adj, limit)});
+    int dyn = std::min(opt_in(tm_fwd, limit), opt_in(tm_adj, limit));
+    for (const FwdVariant &v : fwd_vars) dyn = std::min(dyn, opt_in(v.fn, limit));
+    for (const AdjVariant &v : adj_vars) dyn = std::min(dyn, opt_in(v.fn, limit));
     smem_max = std::min(smem_max, dyn);
     upload_twiddles();
     const int nw = (int)plan.windows.size();
@@ -544,6 +704,17 @@ class Engine {
       ja[w] = j;
       tj[w].z = S0.get() + W.model_off;
     }
+    autotune_space(jf, ja, planes);
+    const FwdVariant &fv = fwd_vars[fwd_pick];
+    const AdjVariant &av = adj_vars[adj_pick];
+    sp_fwd = fv.fn;
+    sp_adj = av.fn;
+    nt_fwd = fv.nt;
+    np_fwd = fv.np;
+    smem_fwd = fv.smem;
+    nt_adj = av.nt;
+    np_adj = av.np;
+    smem_adj = av.smem;
     make_plane_launch(pl_fwd, jf, planes, nt_fwd, np_fwd, smem_fwd, sp_fwd);
     make_plane_launch(pl_adj, ja, planes, nt_adj, np_adj, smem_adj, sp_adj);
     pending_plane_plain = ja;
@@ -1360,6 +1531,10 @@ int agd_gpu_problem_info(agd_gpu_problem const *pb, long int *info) {
   info[7] = e.g_fwd.n_contrib;
   info[8] = e.fast ? 1 : 0;
   info[9] = e.wav_fast ? 1 : 0;
+  info[10] = e.fast ? e.fwd_pick : -1;
+  info[11] = e.fast ? e.adj_pick : -1;
+  info[12] = (long)e.fwd_vars.size();
+  info[13] = (long)e.adj_vars.size();
   return 0;
 }
 

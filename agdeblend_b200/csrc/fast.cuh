@@ -409,15 +409,19 @@ __device__ __forceinline__ void space_axes(Cx<R> *buf, int np) {
 }
 
 // Forward operator, all space axes: Z[L..] = crop(IFFT_space(X[P..])).
-// Persistent blocks of NT threads walk batches of NP planes; the planes of
-// the next batch are copied into the second shared buffer (cp.async) while
-// the current one is transformed.  Shared memory: 2 NP planes.
-template <typename R, int D, int P0, int P1, int P2, int NT, int NP>
-__global__ void __launch_bounds__(NT, 1) space_fwd_fast(PlaneBatches<R> batches) {
+// Persistent blocks of NT threads walk batches of NP planes.  STAGES = 2:
+// the planes of the next batch are copied into a second shared buffer
+// (cp.async) while the current one is transformed (shared memory: 2 NP
+// planes, one block per SM).  STAGES = 1: one buffer, refilled after each
+// store; MINB blocks share an SM and overlap one another's copies.
+template <typename R, int D, int P0, int P1, int P2, int NT, int NP, int STAGES, int MINB>
+__global__ void __launch_bounds__(NT, MINB) space_fwd_fast(PlaneBatches<R> batches) {
+  static_assert(STAGES == 1 || STAGES == 2, "one or two stages");
   using C = Cx<R>;
   using S = PlaneShape<D, P0, P1, P2>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *stage[2] = {reinterpret_cast<C *>(smem_raw), reinterpret_cast<C *>(smem_raw) + NP * S::size};
+  C *stage[2] = {reinterpret_cast<C *>(smem_raw),
+                 reinterpret_cast<C *>(smem_raw) + (STAGES == 2 ? NP * S::size : 0)};
   auto issue = [&](const PlaneBatch<R> &bt, C *buf) {
     const int n = bt.count * S::dense_P;
     for (int e = threadIdx.x; e < n; e += NT) {
@@ -437,11 +441,15 @@ __global__ void __launch_bounds__(NT, 1) space_fwd_fast(PlaneBatches<R> batches)
     // batch records are loaded one batch ahead of their use
     const int b2 = b + 2 * gridDim.x;
     const PlaneBatch<R> after = b2 < batches.n ? batches.b[b2] : none;
-    if (nxt.count > 0) issue(nxt, stage[(k + 1) & 1]);
-    cp_async_commit();
-    cp_async_wait<1>();
+    if constexpr (STAGES == 2) {
+      if (nxt.count > 0) issue(nxt, stage[(k + 1) & 1]);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
     __syncthreads();
-    C *buf = stage[k & 1];
+    C *buf = stage[STAGES == 2 ? (k & 1) : 0];
     const int np = cur.count;
     space_axes<R, D, P0, P1, P2, NT, NP, true>(buf, np);
     __syncthreads();
@@ -452,6 +460,10 @@ __global__ void __launch_bounds__(NT, 1) space_fwd_fast(PlaneBatches<R> batches)
       dst[e] = buf[p * S::size + plane_pos<D, P0, P1, P2, S::L1, S::L2>(e - p * S::dense_L)];
     }
     __syncthreads();
+    if constexpr (STAGES == 1) {
+      if (nxt.count > 0) issue(nxt, stage[0]);
+      cp_async_commit();
+    }
     cur = nxt;
     nxt = after;
   }
@@ -460,20 +472,22 @@ __global__ void __launch_bounds__(NT, 1) space_fwd_fast(PlaneBatches<R> batches)
 // Adjoint, all space axes, with the ISTA update fused:
 // X <- soft_threshold(X - step * FFT_space(pad(G[L..])), lamb)   (epilogue
 // kUpdateThreshold), X <- X - step * ..., tracking max |X|^2 (kUpdateMax), or
-// X <- FFT_space(pad(G)) (kStore).  Persistent and double buffered like the
-// forward kernel; the model planes of the current batch are copied into a
-// third buffer while its FFTs run.  Shared memory: 2 NP padded planes and NP
-// dense planes.
-template <typename R, int D, int P0, int P1, int P2, int NT, int NP>
-__global__ void __launch_bounds__(NT, 1)
+// X <- FFT_space(pad(G)) (kStore).  Persistent like the forward kernel.
+// STAGES = 2: double buffered, and the model planes of the current batch are
+// copied into a third buffer while its FFTs run (shared memory: 2 NP padded
+// planes and NP dense planes).  STAGES = 1: one padded buffer; the epilogue
+// reads the model planes from global memory, and MINB blocks share an SM.
+template <typename R, int D, int P0, int P1, int P2, int NT, int NP, int STAGES, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
     space_adj_fast(PlaneBatches<R> batches, int epilogue, R step, R lamb_arg,
                    const R *lamb_dev, R *max_out) {
+  static_assert(STAGES == 1 || STAGES == 2, "one or two stages");
   using C = Cx<R>;
   using S = PlaneShape<D, P0, P1, P2>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *base = reinterpret_cast<C *>(smem_raw);
-  C *stage[2] = {base, base + NP * S::size};
-  C *xbuf = base + 2 * NP * S::size;
+  C *stage[2] = {base, base + (STAGES == 2 ? NP * S::size : 0)};
+  C *xbuf = base + STAGES * NP * S::size;
   const bool need_x = epilogue != kStore;
   auto issue = [&](const PlaneBatch<R> &bt, C *buf) {
     const int n = bt.count * S::dense_L;
@@ -497,20 +511,26 @@ __global__ void __launch_bounds__(NT, 1)
   for (int k = 0; b < batches.n; ++k, b += gridDim.x) {
     const int b2 = b + 2 * gridDim.x;
     const PlaneBatch<R> after = b2 < batches.n ? batches.b[b2] : none;
-    if (nxt.count > 0) issue(nxt, stage[(k + 1) & 1]);
-    cp_async_commit();
-    cp_async_wait<1>();
+    if constexpr (STAGES == 2) {
+      if (nxt.count > 0) issue(nxt, stage[(k + 1) & 1]);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
     __syncthreads();
     const int np = cur.count;
     C *dst = cur.dst;
     const int n_store = np * S::dense_P;
-    if (need_x) {
-      for (int e = threadIdx.x; e < n_store; e += NT) cp_async<sizeof(C)>(xbuf + e, dst + e);
+    if constexpr (STAGES == 2) {
+      if (need_x) {
+        for (int e = threadIdx.x; e < n_store; e += NT) cp_async<sizeof(C)>(xbuf + e, dst + e);
+      }
+      cp_async_commit();
     }
-    cp_async_commit();
-    C *buf = stage[k & 1];
+    C *buf = stage[STAGES == 2 ? (k & 1) : 0];
     space_axes<R, D, P0, P1, P2, NT, NP, false>(buf, np);
-    cp_async_wait<0>();
+    if constexpr (STAGES == 2) cp_async_wait<0>();
     __syncthreads();
     for (int e = threadIdx.x; e < n_store; e += NT) {
       const int p = e / S::dense_P;
@@ -518,7 +538,7 @@ __global__ void __launch_bounds__(NT, 1)
       if (epilogue == kStore) {
         dst[e] = g;
       } else {
-        const C x = xbuf[e];
+        const C x = STAGES == 2 ? xbuf[e] : dst[e];
         C xn = cmake<C>(sub_rn<R>(x.x, mul_rn<R>(step, g.x)),
                         sub_rn<R>(x.y, mul_rn<R>(step, g.y)));
         if (epilogue == kUpdateThreshold) {
@@ -531,6 +551,10 @@ __global__ void __launch_bounds__(NT, 1)
       }
     }
     __syncthreads();
+    if constexpr (STAGES == 1) {
+      if (nxt.count > 0) issue(nxt, stage[0]);
+      cp_async_commit();
+    }
     cur = nxt;
     nxt = after;
   }

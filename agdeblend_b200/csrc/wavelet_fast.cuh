@@ -56,18 +56,17 @@ struct WaveletFastJob {
   PfaShape sh;
 };
 
-// One pass along an axis of length F for np sequences of length N.
+// One pass along an axis of length F for np sequences of length N.  Line l
+// starts at position c = F l, whose index along this axis is 0 (a position
+// p holds axis index (p mod F) (N/F)^-1 mod F); as gcd(F, N/F) = 1 these
+// starts meet every line once.  Consecutive threads then read positions F
+// apart, which for odd F are free of shared-memory bank conflicts.
 template <typename R, int F, bool INV>
-__device__ __forceinline__ void pfa_pass(Cx<R> *buf, int np, int N, int s, int inv) {
+__device__ __forceinline__ void pfa_pass(Cx<R> *buf, int np, int N, int s) {
   using C = Cx<R>;
   for (int idx = threadIdx.x; idx < np * s; idx += blockDim.x) {
     const int pr = idx / s;
-    const int l = idx - pr * s;
-    // the coset {l + j s} holds axis index (l inv + j) mod F at l + j s;
-    // start the line at axis index 0
-    const int n0 = (l * inv) % F;
-    int c = l - n0 * s;
-    if (c < 0) c += N;
+    const int c = F * (idx - pr * s);
     C *b = buf + (long)pr * N;
     C v[F];
     int pos = c;
@@ -89,24 +88,24 @@ __device__ __forceinline__ void pfa_pass(Cx<R> *buf, int np, int N, int s, int i
 }
 
 template <typename R, bool INV>
-__device__ void pfa_pass_any(int F, Cx<R> *buf, int np, int N, int s, int inv) {
+__device__ void pfa_pass_any(int F, Cx<R> *buf, int np, int N, int s) {
   switch (F) {
-    case 2: pfa_pass<R, 2, INV>(buf, np, N, s, inv); break;
-    case 3: pfa_pass<R, 3, INV>(buf, np, N, s, inv); break;
-    case 4: pfa_pass<R, 4, INV>(buf, np, N, s, inv); break;
-    case 5: pfa_pass<R, 5, INV>(buf, np, N, s, inv); break;
-    case 7: pfa_pass<R, 7, INV>(buf, np, N, s, inv); break;
-    case 8: pfa_pass<R, 8, INV>(buf, np, N, s, inv); break;
-    case 9: pfa_pass<R, 9, INV>(buf, np, N, s, inv); break;
-    case 11: pfa_pass<R, 11, INV>(buf, np, N, s, inv); break;
-    case 13: pfa_pass<R, 13, INV>(buf, np, N, s, inv); break;
-    case 16: pfa_pass<R, 16, INV>(buf, np, N, s, inv); break;
-    case 17: pfa_pass<R, 17, INV>(buf, np, N, s, inv); break;
-    case 19: pfa_pass<R, 19, INV>(buf, np, N, s, inv); break;
-    case 23: pfa_pass<R, 23, INV>(buf, np, N, s, inv); break;
-    case 25: pfa_pass<R, 25, INV>(buf, np, N, s, inv); break;
-    case 27: pfa_pass<R, 27, INV>(buf, np, N, s, inv); break;
-    case 32: pfa_pass<R, 32, INV>(buf, np, N, s, inv); break;
+    case 2: pfa_pass<R, 2, INV>(buf, np, N, s); break;
+    case 3: pfa_pass<R, 3, INV>(buf, np, N, s); break;
+    case 4: pfa_pass<R, 4, INV>(buf, np, N, s); break;
+    case 5: pfa_pass<R, 5, INV>(buf, np, N, s); break;
+    case 7: pfa_pass<R, 7, INV>(buf, np, N, s); break;
+    case 8: pfa_pass<R, 8, INV>(buf, np, N, s); break;
+    case 9: pfa_pass<R, 9, INV>(buf, np, N, s); break;
+    case 11: pfa_pass<R, 11, INV>(buf, np, N, s); break;
+    case 13: pfa_pass<R, 13, INV>(buf, np, N, s); break;
+    case 16: pfa_pass<R, 16, INV>(buf, np, N, s); break;
+    case 17: pfa_pass<R, 17, INV>(buf, np, N, s); break;
+    case 19: pfa_pass<R, 19, INV>(buf, np, N, s); break;
+    case 23: pfa_pass<R, 23, INV>(buf, np, N, s); break;
+    case 25: pfa_pass<R, 25, INV>(buf, np, N, s); break;
+    case 27: pfa_pass<R, 27, INV>(buf, np, N, s); break;
+    case 32: pfa_pass<R, 32, INV>(buf, np, N, s); break;
     default: break;  // the host only builds shapes from the factors above
   }
 }
@@ -130,7 +129,7 @@ __device__ __forceinline__ Cx<R> spectrum_at(const Cx<R> *sp, int k, int N, bool
 // window's last CTA).  direction +1: convolution in place on the traces;
 // -1: correlation of the traces gathered from `record`, written to y.
 template <typename R>
-__global__ void __launch_bounds__(kWavThreads, 2)
+__global__ void __launch_bounds__(kWavThreads, sizeof(R) == 4 ? 2 : 1)
     wavelet_fast(const WaveletFastJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
                  const int *__restrict__ cta_pair0, int np_max,
                  const Cx<R> *__restrict__ spectra, const long *__restrict__ spec_off,
@@ -145,7 +144,8 @@ __global__ void __launch_bounds__(kWavThreads, 2)
   const int pair0 = cta_pair0[blockIdx.x];
   const int np = min(np_max, ((n_tr + 1) >> 1) - pair0);
 
-  // ---- load: trace a -> real part, trace b -> imaginary part
+  // ---- load: trace a -> real part, trace b -> imaginary part (unrolled so
+  // that several global loads are in flight per thread)
   for (int pr = 0; pr < np; ++pr) {
     const int ta = 2 * (pair0 + pr);
     const bool has_b = ta + 1 < n_tr;
@@ -161,6 +161,7 @@ __global__ void __launch_bounds__(kWavThreads, 2)
         sb = job.blend_ts[ta + 1];
         nb = job.blend_n[ta + 1];
       }
+#pragma unroll 4
       for (int e = threadIdx.x; e < N; e += blockDim.x) {
         const R va = (ra >= 0 && e >= sa && e < sa + na) ? record[ra + (e - sa)] : (R)0;
         const R vb = (rb >= 0 && e >= sb && e < sb + nb) ? record[rb + (e - sb)] : (R)0;
@@ -168,6 +169,7 @@ __global__ void __launch_bounds__(kWavThreads, 2)
       }
     } else {
       const R *ya = job.y + (long)ta * N;
+#pragma unroll 4
       for (int e = threadIdx.x; e < N; e += blockDim.x)
         b[e] = cmake<C>(ya[e], has_b ? ya[N + e] : (R)0);
     }
@@ -175,7 +177,7 @@ __global__ void __launch_bounds__(kWavThreads, 2)
   __syncthreads();
 
   for (int i = 0; i < nf; ++i) {
-    pfa_pass_any<R, false>(job.sh.f[i], buf, np, N, job.sh.s[i], job.sh.inv[i]);
+    pfa_pass_any<R, false>(job.sh.f[i], buf, np, N, job.sh.s[i]);
     __syncthreads();
   }
 
@@ -212,7 +214,7 @@ __global__ void __launch_bounds__(kWavThreads, 2)
   __syncthreads();
 
   for (int i = 0; i < nf; ++i) {
-    pfa_pass_any<R, true>(job.sh.f[i], buf, np, N, job.sh.s[i], job.sh.inv[i]);
+    pfa_pass_any<R, true>(job.sh.f[i], buf, np, N, job.sh.s[i]);
     __syncthreads();
   }
 

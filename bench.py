@@ -1,9 +1,14 @@
 """Benchmark of the deblending hot path: ISTA iterations per second.
 
-Workload (default): the two-volume 3-D survey, 2 x (64 channels x 128 shots x
-1024 samples) float32, windows (16, 32, 256), 8 % bad/missing traces, two
-3 s record gaps, n_its 200 - synthetic, seeded, generated by
-agdeblend_b200.synthetic.two_volume_3d.
+Workloads (synthetic, seeded, agdeblend_b200.synthetic):
+  two_volume_3d (default)  2 x (64 channels x 128 shots x 1024 samples)
+      float32, windows (16, 32, 256), 8 % bad/missing traces, two 3 s record
+      gaps, n_its 200;
+  vibroseis_4d  32 sourceY x 64 sourceX x 32 channels x 2048 samples float32,
+      one 256-sample 8-80 Hz sweep wavelet (trace length 2431), windows
+      (16, 16, 16, 256), n_its 150;
+  *_small  reduced versions of both (still larger than L2) for multi-pass
+      ncu captures.
 
 One step = one ISTA iteration (forward operator, residual, adjoint, update,
 soft threshold) over the whole survey.
@@ -38,35 +43,50 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "ISTA iterations/s (plain FP32 deblending, two-volume 3-D survey)"
 UNIT = "iterations/s"
 
-
+# name -> (generator, keyword arguments, label of the metric)
 WORKLOADS = {
     # the benchmark workload
-    "two_volume_3d": dict(n_ch=64, n_shots=128, nt=1024),
+    "two_volume_3d": ("two_volume_3d", dict(n_ch=64, n_shots=128, nt=1024),
+                      "two-volume 3-D survey"),
     # the same survey at a quarter of the traces (model 167 MB, still larger
     # than L2): the case for multi-pass ncu captures
-    "two_volume_3d_small": dict(n_ch=32, n_shots=64, nt=1024),
+    "two_volume_3d_small": ("two_volume_3d", dict(n_ch=32, n_shots=64, nt=1024),
+                            "two-volume 3-D survey, quarter size"),
+    # the 4-D vibroseis survey with a source wavelet (model 10.4 GB)
+    "vibroseis_4d": ("vibroseis_4d", dict(n_sy=32, n_sx=64, n_ch=32, nt=2048),
+                     "4-D vibroseis survey with sweep wavelet"),
+    # a quarter of its sources (9 windows, model 1.5 GB) for multi-pass ncu
+    # captures
+    "vibroseis_4d_small": ("vibroseis_4d", dict(n_sy=16, n_sx=32, n_ch=32, nt=2048),
+                           "4-D vibroseis survey with sweep wavelet, quarter size"),
 }
+SEEDS = {"two_volume_3d": 1001, "vibroseis_4d": 1002}
+
+
+def metric_of(name):
+    return f"ISTA iterations/s (plain FP32 deblending, {WORKLOADS[name][2]})"
 
 
 def workload(name="two_volume_3d", seed_offset=0):
     from agdeblend_b200 import synthetic as S
 
-    return S.two_volume_3d(seed=1001 + seed_offset, **WORKLOADS[name])
+    gen, kw, _ = WORKLOADS[name]
+    return getattr(S, gen)(seed=SEEDS[gen] + seed_offset, **kw)
 
 
 def config_of(sv, name="two_volume_3d"):
-    w = WORKLOADS[name]
-    return {
-        "workload": f"{name}: 2 volumes x ({w['n_ch']} ch x {w['n_shots']} shots x "
-                    f"{w['nt']} samples) f32, windows (16,32,256), 4% bad + 4% missing "
-                    "traces, 2 record gaps",
-        "n_its": sv.n_its,
-        "initial_factor": sv.initial_factor,
-        "l2": "inputs larger than L2",
-    }
+    gen, w, _ = WORKLOADS[name]
+    if gen == "two_volume_3d":
+        desc = (f"{name}: 2 volumes x ({w['n_ch']} ch x {w['n_shots']} shots x "
+                f"{w['nt']} samples) f32, windows (16,32,256), 4% bad + 4% missing "
+                "traces, 2 record gaps")
+    else:
+        desc = (f"{name}: {w['n_sy']} sY x {w['n_sx']} sX x {w['n_ch']} ch x {w['nt']} "
+                "samples f32, 256-sample 8-80 Hz sweep wavelet, windows (16,16,16,256)")
+    return {"workload": desc, "n_its": sv.n_its, "initial_factor": sv.initial_factor,
+            "l2": "inputs larger than L2"}
 
 
 def hbm_peak():
@@ -133,12 +153,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def profiled_traffic(kernel: str):
-    """DRAM bytes per launch of `kernel` on the benchmark workload, from the
-    committed ncu summary (profiles/space_time_fast_two_volume_3d_small.md)."""
+PROFILES = {"two_volume_3d": "space_time_fast_two_volume_3d_small.md",
+            "vibroseis_4d": "kernels_vibroseis_4d_small.md"}
+
+
+def profiled_traffic(kernel: str, name: str):
+    """DRAM bytes per launch of `kernel` on workload `name`, scaled from the
+    committed ncu summary of its small case (profiles/)."""
     import re
 
-    path = os.path.join(ROOT, "profiles", "space_time_fast_two_volume_3d_small.md")
+    if name not in PROFILES:
+        return None
+    path = os.path.join(ROOT, "profiles", PROFILES[name])
     try:
         text = open(path).read()
     except OSError:
@@ -161,7 +187,8 @@ def cpu_reference_rate(sv, its: int, lib_name="libagdeblend_ref.so"):
     times = []
     for n in (1, 1 + its):
         args = DeblendArgs(sv.volumes, sv.n_dims, sv.window_shapes, sv.coords, sv.shapes,
-                           sv.shottimes, sv.channels, sv.trace_types, sv.data, dtype=np.float32)
+                           sv.shottimes, sv.channels, sv.trace_types, sv.data,
+                           sv.wavelet_lengths, sv.wavelet_idxs, sv.wavelets, dtype=np.float32)
         t0 = time.perf_counter()
         rc = ref_bind.ref_deblend(args, sv.initial_factor, n, 0, lib_name=lib_name)
         times.append(time.perf_counter() - t0)
@@ -180,7 +207,8 @@ def cpu_port_rate(sv, its: int):
     import agd_oracle as O
 
     plan = O.make_plan(sv.volumes, sv.n_dims, sv.window_shapes, sv.coords, sv.shapes,
-                       sv.shottimes, sv.channels, sv.trace_types)
+                       sv.shottimes, sv.channels, sv.trace_types, sv.wavelet_lengths,
+                       sv.wavelet_idxs, sv.wavelets)
     x = plan.zero_model()
     d = O.blend_input(plan, sv.data)
     t0 = time.perf_counter()
@@ -238,7 +266,7 @@ def run_reference(args, rank, world):
     res = cpu_reference_rate(sv, steps)
     if res is None:
         res = cpu_port_rate(sv, max(1, min(steps, 3)))
-    line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT,
+    line = {"impl": "reference", "metric": metric_of(args.workload), "value": res["value"], "unit": UNIT,
             "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": config_of(sv, args.workload),
@@ -273,16 +301,19 @@ def run_gpu(args, rank, world, local):
 
     # e2e: the public agd_deblend call with host buffers, one full solve
     e2e_s, snr = float("nan"), None
+    wavelet_kw = {}
+    if sv.wavelets is not None:
+        wavelet_kw = dict(wavelet_idxs=sv.wavelet_idxs, wavelets=sv.wavelets)
     if not args.no_e2e:
         # one untimed call first: the first call in a process also pays the
         # one-time mapping of fresh device memory
         A.deblend(sv.volumes, sv.window_shapes, sv.coords, sv.shottimes, sv.channels,
-                  sv.trace_types, sv.initial_factor, 2, 0, sv.data)
+                  sv.trace_types, sv.initial_factor, 2, 0, sv.data, **wavelet_kw)
         torch.cuda.synchronize()
         barrier(world)
         t0 = time.perf_counter()
         out = A.deblend(sv.volumes, sv.window_shapes, sv.coords, sv.shottimes, sv.channels,
-                        sv.trace_types, sv.initial_factor, sv.n_its, 0, sv.data)
+                        sv.trace_types, sv.initial_factor, sv.n_its, 0, sv.data, **wavelet_kw)
         torch.cuda.synchronize()
         e2e_s = barrier_max(world, time.perf_counter() - t0)
         from agdeblend_b200.synthetic import snr_db
@@ -303,9 +334,15 @@ def run_gpu(args, rank, world, local):
     # intermediates (0 algorithmic bytes).
     nf = int(prof[14])
     fast = int(info[8]) == 1
+    wav = sv.wavelets is not None
+    wav_fast = int(info[9]) == 1
     names = (("space_fwd_fast", "time_fwd_fast", "blend_gather", "time_adj_fast",
               "space_adj_fast") if fast else
              ("axis_pass_fwd0", "time_c2r_ola", "blend_gather", "time_r2c", "axis_pass_adj_last"))
+    if wav:
+        # the adjoint time phase then also holds the wavelet correlation
+        names = names[:3] + (names[3] + "+" + ("wavelet_fast" if wav_fast else "wavelet_apply"),
+                             names[4])
     phases = {
         names[0]: (prof[6], 8.0 * M),
         names[1]: (prof[1], 0.0),
@@ -313,12 +350,14 @@ def run_gpu(args, rank, world, local):
         names[3]: (prof[4], 4.0 * Rn),
         names[4]: (prof[10 + nf - 1], 16.0 * M),
     }
+    if wav:
+        phases["wavelet_fast" if wav_fast else "wavelet_apply"] = (prof[2], 0.0)
     dom = max(phases, key=lambda k: phases[k][0])
     dom_ms, dom_bytes = phases[dom]
     iter_bytes = 3 * 8.0 * M + 4 * 4.0 * Rn
     ms_iter = ms / args.steps
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 and dom_bytes > 0 else 0.0
-    traffic = profiled_traffic(dom) if args.workload == "two_volume_3d" else None
+    traffic = profiled_traffic(dom, args.workload)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "algorithmic_bytes": dom_bytes, "peak_source": peak_kind,
@@ -330,8 +369,11 @@ def run_gpu(args, rank, world, local):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference_rate(sv, args.cpu_its) or cpu_port_rate(sv, 1)
     if rank == 0:
-        launches = args.steps * (2 * nf + 3)
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        # per iteration: space passes both ways, time kernels both ways, the
+        # blend gather, the threshold-schedule step, wavelet kernels
+        per_it = 2 * nf + 4 + ((2 if wav_fast else 3) if wav else 0)
+        launches = args.steps * per_it
+        line = {"metric": metric_of(args.workload), "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_iter,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic", "config": config_of(sv, args.workload),

@@ -40,11 +40,14 @@ int agd_gpu_problem_create(int n_patches, int const *volumes, int const *n_dims,
 
 void agd_gpu_problem_destroy(agd_gpu_problem *problem);
 
-/* info (10 values): [0] windows, [1] model complex elements, [2] record
+/* info (14 values): [0] windows, [1] model complex elements, [2] record
  * samples, [3] window traces (all windows), [4] record segments, [5] mute
  * spans, [6] device bytes held, [7] blend contributions per forward,
  * [8] 1 if the shape-specialised kernels serve this problem, [9] 1 if the
- * prime-factor wavelet kernel serves it. */
+ * prime-factor wavelet kernel serves it, [10] and [11] the space-kernel
+ * candidates picked by the set-up timing for the forward and adjoint
+ * (-1 without the shape-specialised kernels), [12] and [13] the number of
+ * candidates. */
 int agd_gpu_problem_info(agd_gpu_problem const *problem, long int *info);
 
 /* Step size 0.5 / max blend fold (reference get_stepsize, src/model.c:1230-1312). */

@@ -1,6 +1,7 @@
 """The shape-specialised kernels (agdeblend_b200/csrc/fast.cuh) against the
-oracle, for every instantiated window shape, and against the generic kernels
-(forced with AGD_GPU_GENERIC=1) on the same problem."""
+oracle, for every instantiated window shape and every candidate of the
+space-kernel autotuner (forced with AGD_GPU_SPACE_VARIANT), and against the
+generic kernels (forced with AGD_GPU_GENERIC=1) on the same problem."""
 import os
 
 import numpy as np
@@ -38,28 +39,22 @@ def _interleave(x):
     return np.stack([x.real, x.imag], -1).reshape(-1)
 
 
-def _problem(sv, generic=False, dtype=np.float32):
-    old = os.environ.get("AGD_GPU_GENERIC")
-    os.environ["AGD_GPU_GENERIC"] = "1" if generic else "0"
+def _problem(sv, generic=False, dtype=np.float32, variant=None):
+    env = {"AGD_GPU_GENERIC": "1" if generic else "0",
+           "AGD_GPU_SPACE_VARIANT": "" if variant is None else f"{variant[0]},{variant[1]}"}
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
     try:
         return A.Problem.from_survey(sv, dtype)
     finally:
-        if old is None:
-            del os.environ["AGD_GPU_GENERIC"]
-        else:
-            os.environ["AGD_GPU_GENERIC"] = old
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
 
 
-@pytest.mark.parametrize("dtype", [np.float32, np.float64])
-@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
-def test_fast_operators_vs_oracle(name, make, dtype):
-    tol = 1e-5 if dtype == np.float32 else 1e-11
-    sv = make()
-    prob = _problem(sv, dtype=dtype)
-    # a double-precision 20x20x20 plane does not fit two shared-memory stages;
-    # that case runs on the generic kernels
-    expect_fast = not (name == "3d_P20x20x20" and dtype == np.float64)
-    assert prob.info[8] == (1 if expect_fast else 0)
+def _check_operators(sv, prob, tol):
     plan = _plan(sv)
     rng = np.random.default_rng(1)
     rec = rng.standard_normal(prob.record_size)
@@ -77,7 +72,34 @@ def test_fast_operators_vs_oracle(name, make, dtype):
     ref_out = O.set_output(plan, O.flat_to_model(plan, x_ref[0::2] + 1j * x_ref[1::2]))
     for o, r in zip(outs, ref_out):
         assert rel_l2(o, r) <= tol
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+def test_fast_operators_vs_oracle(name, make, dtype):
+    tol = 1e-5 if dtype == np.float32 else 1e-11
+    sv = make()
+    prob = _problem(sv, dtype=dtype)
+    assert prob.info[8] == 1
+    assert 0 <= prob.info[10] < prob.info[12] and 0 <= prob.info[11] < prob.info[13]
+    _check_operators(sv, prob, tol)
     prob.close()
+
+
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+def test_every_space_candidate_vs_oracle(name, make):
+    """Each forward/adjoint candidate the set-up timing may pick."""
+    sv = make()
+    probe = _problem(sv)
+    n_f, n_a = int(probe.info[12]), int(probe.info[13])
+    probe.close()
+    assert n_f >= 1 and n_a >= 1
+    for v in range(max(n_f, n_a)):
+        pick = (min(v, n_f - 1), min(v, n_a - 1))
+        prob = _problem(sv, variant=pick)
+        assert (prob.info[10], prob.info[11]) == pick
+        _check_operators(sv, prob, 1e-5)
+        prob.close()
 
 
 @pytest.mark.parametrize("name,make", CASES[:3], ids=[c[0] for c in CASES[:3]])
