@@ -72,9 +72,17 @@ def _bind_extension(lib, dtype):
     lib.agd_gpu_profile_iteration.restype = c_int
     lib.agd_plan_export.argtypes = problem_args + [POINTER(c_long), POINTER(c_int),
                                                    POINTER(c_long)]
+    ip = POINTER(c_int)
+    lip = POINTER(c_long)
+    lib.agd_gpu_batch_create.argtypes = [
+        c_int, ip, POINTER(ip), POINTER(ip), POINTER(POINTER(ip)), POINTER(POINTER(ip)),
+        POINTER(POINTER(ip)), POINTER(POINTER(lip)), POINTER(POINTER(ip)), POINTER(POINTER(ip)),
+        POINTER(ip), POINTER(POINTER(ip)), POINTER(POINTER(rp)), POINTER(c_void_p)]
+    lib.agd_gpu_problem_steps.argtypes = [c_void_p, rp]
     for name in ("agd_gpu_problem_info", "agd_gpu_stepsize", "agd_gpu_forward",
                  "agd_gpu_adjoint", "agd_gpu_blend_input", "agd_gpu_set_output",
-                 "agd_gpu_solve", "agd_gpu_time_iterations", "agd_plan_export"):
+                 "agd_gpu_solve", "agd_gpu_time_iterations", "agd_plan_export",
+                 "agd_gpu_batch_create", "agd_gpu_problem_steps"):
         getattr(lib, name).restype = c_int
 
 
@@ -95,14 +103,11 @@ def _n_dims(volumes, data):
     return n_dims
 
 
-def deblend(volumes, window_shapes, coords, shottimes, channels, trace_types, initial_factor,
-            n_its, print_freq, data, wavelet_idxs=None, wavelets=None, comm=None):
-    """Deblends seismic data; same arguments and result as the reference's
-    ``agdeblend.deblend`` (serial form: ``comm`` must be None)."""
-    if comm is not None:
-        raise RuntimeError("MPI communicators are not supported: the problem runs on one GPU")
-    dtype = _dtype_of(data)
-    lib = load_library(dtype)
+def _deblend_args(volumes, window_shapes, coords, shottimes, channels, trace_types, data,
+                  wavelet_idxs=None, wavelets=None, dtype=None):
+    """Checks and converts the arguments of ``deblend`` (the reference
+    wrapper's, wrappers/python/agdeblend/agdeblend.py:71-146)."""
+    dtype = _dtype_of(data) if dtype is None else np.dtype(dtype)
     if len(volumes) != len(data):
         raise RuntimeError("volumes must have the same length as data")
     for name, arr in (("coords", coords), ("shottimes", shottimes), ("channels", channels),
@@ -121,13 +126,46 @@ def deblend(volumes, window_shapes, coords, shottimes, channels, trace_types, in
     if wavelets is not None:
         wavelet_lengths = [len(w) for w in wavelets]
     shapes = [list(np.asarray(d).shape) for d in data]
-    args = capi.DeblendArgs(volumes, _n_dims(volumes, data), window_shapes, coords, shapes,
+    return capi.DeblendArgs(volumes, _n_dims(volumes, data), window_shapes, coords, shapes,
                             shottimes, channels, trace_types, data, wavelet_lengths,
                             wavelet_idxs, wavelets, dtype=dtype)
+
+
+def deblend(volumes, window_shapes, coords, shottimes, channels, trace_types, initial_factor,
+            n_its, print_freq, data, wavelet_idxs=None, wavelets=None, comm=None):
+    """Deblends seismic data; same arguments and result as the reference's
+    ``agdeblend.deblend`` (serial form: ``comm`` must be None)."""
+    if comm is not None:
+        raise RuntimeError("MPI communicators are not supported: the problem runs on one GPU")
+    dtype = _dtype_of(data)
+    lib = load_library(dtype)
+    args = _deblend_args(volumes, window_shapes, coords, shottimes, channels, trace_types, data,
+                         wavelet_idxs, wavelets, dtype)
     fn = lib.agd_deblend
     if capi.call_deblend(fn, args, initial_factor, n_its, print_freq):
         raise RuntimeError("Error in call to agd_deblend")
     return [d.astype(dtype) for d in args.data]
+
+
+def deblend_batch(problems, initial_factor, n_its):
+    """Deblends independent problems together (agd_deblend_batch, an
+    addition of this library).  ``problems``: one dict per problem with the
+    keys of ``deblend`` (volumes, window_shapes, coords, shottimes, channels,
+    trace_types, data, optionally wavelet_idxs and wavelets), all with the
+    same data type.  Returns the deblended data of every problem, each as
+    ``deblend`` would return it for that problem alone."""
+    if not problems:
+        return []
+    dtype = _dtype_of(problems[0]["data"])
+    lib = load_library(dtype)
+    args = [_deblend_args(p["volumes"], p["window_shapes"], p["coords"], p["shottimes"],
+                          p["channels"], p["trace_types"], p["data"], p.get("wavelet_idxs"),
+                          p.get("wavelets"), dtype) for p in problems]
+    batch = capi.BatchArgs(args)
+    fn = capi.bind_deblend_batch(lib, dtype)
+    if fn(*batch.problem_args(), initial_factor, n_its, batch.data_p):
+        raise RuntimeError("Error in call to agd_deblend_batch")
+    return [[d.astype(dtype) for d in a.data] for a in args]
 
 
 def blend(shottimes, channels, trace_types, data, blend_mode, taper_length=0, n_times_out=None,
@@ -185,7 +223,31 @@ class Problem:
         if self.lib.agd_gpu_problem_create(*self.args.problem_args(), ctypes.byref(h)):
             raise RuntimeError("agd_gpu_problem_create failed")
         self.h = h
-        info = np.zeros(14, np.int64)
+        self._finish_init()
+
+    @classmethod
+    def from_batch(cls, surveys, dtype=np.float32):
+        """A handle over independent problems solved together
+        (agd_gpu_batch_create); its patches are all surveys' patches in
+        order."""
+        self = cls.__new__(cls)
+        self.dtype = np.dtype(dtype)
+        self.lib = load_library(self.dtype)
+        self.sub_args = [capi.DeblendArgs(sv.volumes, sv.n_dims, sv.window_shapes, sv.coords,
+                                          sv.shapes, sv.shottimes, sv.channels, sv.trace_types,
+                                          None, sv.wavelet_lengths, sv.wavelet_idxs,
+                                          sv.wavelets, dtype=self.dtype) for sv in surveys]
+        self.args = capi.BatchArgs(self.sub_args)
+        self.shapes = [tuple(int(v) for v in s) for sv in surveys for s in sv.shapes]
+        h = c_void_p()
+        if self.lib.agd_gpu_batch_create(*self.args.problem_args(), ctypes.byref(h)):
+            raise RuntimeError("agd_gpu_batch_create failed")
+        self.h = h
+        self._finish_init()
+        return self
+
+    def _finish_init(self):
+        info = np.zeros(17, np.int64)
         self.lib.agd_gpu_problem_info(self.h, info.ctypes.data_as(POINTER(c_long)))
         self.info = info
         self.n_windows = int(info[0])
@@ -196,6 +258,13 @@ class Problem:
         self.lib.agd_gpu_stepsize(self.h, ctypes.byref(s))
         self.stepsize = float(s.value)
         self._rp = POINTER(rc)
+
+    def steps(self) -> np.ndarray:
+        """Step size of every problem of the handle."""
+        n = len(getattr(self, "sub_args", [None]))
+        out = np.zeros(n, self.dtype)
+        self.lib.agd_gpu_problem_steps(self.h, out.ctypes.data_as(self._rp))
+        return out
 
     @classmethod
     def from_survey(cls, sv, dtype=np.float32):

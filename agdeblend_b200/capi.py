@@ -143,3 +143,66 @@ def call_blend(fn, dtype, n_times, shottimes, channels, trace_types, data, blend
     rc = fn(n_patches, nt_p, ntm_p, st_p, ch_p, tt_p, d_p, blend_mode, taper_length,
             len(shottimes_out), nto_p, ntmo_p, sto_p, cho_p, tto_p, do_p)
     return rc, data_out
+
+
+def bind_deblend_batch(lib: ctypes.CDLL, dtype, name: str = "agd_deblend_batch"):
+    """agd_deblend_batch (include/agdeblend_gpu.h): every argument an array
+    over the problems of the agd_deblend argument."""
+    fn = getattr(lib, name)
+    rc = real_ctype(dtype)
+    rp = POINTER(rc)
+    fn.restype = c_int
+    fn.argtypes = [c_int, _c_int_p, POINTER(_c_int_p), POINTER(_c_int_p),
+                   POINTER(POINTER(_c_int_p)), POINTER(POINTER(_c_int_p)),
+                   POINTER(POINTER(_c_int_p)), POINTER(POINTER(_c_long_p)),
+                   POINTER(POINTER(_c_int_p)), POINTER(POINTER(_c_int_p)), POINTER(_c_int_p),
+                   POINTER(POINTER(_c_int_p)), POINTER(POINTER(rp)), rc, c_int,
+                   POINTER(POINTER(rp))]
+    return fn
+
+
+class BatchArgs:
+    """Per-problem DeblendArgs gathered into the pointer arrays of
+    agd_deblend_batch / agd_gpu_batch_create."""
+
+    def __init__(self, problems):
+        self.problems = list(problems)
+        n = len(self.problems)
+        self.dtype = self.problems[0].dtype
+        rc = real_ctype(self.dtype)
+        rp = POINTER(rc)
+        self.n_problems = n
+        self.n_patches_p, self._np = _vec([a.n_patches for a in self.problems], np.int32, c_int)
+
+        def arr(ctype, values):
+            a = (ctype * max(n, 1))()
+            for i, v in enumerate(values):
+                a[i] = ctypes.cast(v, ctype) if v is not None else ctype()
+            return a
+
+        P = self.problems
+        self.volumes_p = arr(_c_int_p, [a.volumes_p for a in P])
+        self.n_dims_p = arr(_c_int_p, [a.n_dims_p for a in P])
+        self.window_shapes_p = arr(POINTER(_c_int_p), [a.window_shapes_p for a in P])
+        self.coords_p = arr(POINTER(_c_int_p), [a.coords_p for a in P])
+        self.shapes_p = arr(POINTER(_c_int_p), [a.shapes_p for a in P])
+        self.shottimes_p = arr(POINTER(_c_long_p), [a.shottimes_p for a in P])
+        self.channels_p = arr(POINTER(_c_int_p), [a.channels_p for a in P])
+        self.trace_types_p = arr(POINTER(_c_int_p), [a.trace_types_p for a in P])
+        if any(a.wavelets_p is not None for a in P):
+            self.wavelet_lengths_p = arr(_c_int_p, [a.wavelet_lengths_p for a in P])
+            self.wavelet_idxs_p = arr(POINTER(_c_int_p), [a.wavelet_idxs_p for a in P])
+            self.wavelets_p = arr(POINTER(rp), [a.wavelets_p for a in P])
+        else:
+            self.wavelet_lengths_p = self.wavelet_idxs_p = self.wavelets_p = None
+        if all(a.data is not None for a in P):
+            self.data_p = arr(POINTER(rp), [a.data_p for a in P])
+        else:
+            self.data_p = None
+
+    def problem_args(self):
+        """The 13 leading arguments of agd_deblend_batch / agd_gpu_batch_create."""
+        return (self.n_problems, self.n_patches_p, self.volumes_p, self.n_dims_p,
+                self.window_shapes_p, self.coords_p, self.shapes_p, self.shottimes_p,
+                self.channels_p, self.trace_types_p, self.wavelet_lengths_p,
+                self.wavelet_idxs_p, self.wavelets_p)

@@ -188,10 +188,12 @@ class Engine {
   std::vector<AxisLaunch> fwd, adj_update, adj_plain;
   TimeLaunch time_fwd, time_adj, wav;
 
-  // shape-specialised path (fast.cuh), used when every window has the same
-  // space and time FFT lengths and an instantiation exists
+  // Shape-specialised kernels (fast.cuh).  Windows are grouped into classes
+  // of equal padded space and time lengths; every class with an
+  // instantiation runs the fast kernels, the remaining windows run the
+  // generic ones (kernels.cuh).
   using SpaceFwdFn = void (*)(PlaneBatches<R>);
-  using SpaceAdjFn = void (*)(PlaneBatches<R>, int, R, R, const R *, R *);
+  using SpaceAdjFn = void (*)(PlaneBatches<R>, int, R, R, const R *, const R *, R *);
   using TimeFwdFn = void (*)(const TimeJob<R> *, const int *, const int *);
   using TimeAdjFn = void (*)(const TimeJob<R> *, const int *, const int *, const R *, int);
   static constexpr int kTimeNB = 32;  // traces per block of the fast time kernels
@@ -203,16 +205,35 @@ class Engine {
     size_t smem = 0;
     PlaneBatches<R> batches() const { return PlaneBatches<R>{batch.get(), n_batch}; }
   };
-  bool fast = false;
-  SpaceFwdFn sp_fwd = nullptr;
-  SpaceAdjFn sp_adj = nullptr;
-  TimeFwdFn tm_fwd = nullptr;
-  TimeAdjFn tm_adj = nullptr;
-  int nt_fwd = 0, np_fwd = 0, nt_adj = 0, np_adj = 0;  // threads, planes per batch
-  size_t smem_fwd = 0, smem_adj = 0;
+  struct FwdVariant {
+    SpaceFwdFn fn;
+    int nt, np, stages;
+    size_t smem;
+  };
+  struct AdjVariant {
+    SpaceAdjFn fn;
+    int nt, np, stages;
+    size_t smem;
+  };
+  struct FastClass {
+    std::vector<int> win;  // windows of the class
+    std::vector<FwdVariant> fwd_vars;
+    std::vector<AdjVariant> adj_vars;
+    int fwd_pick = 0, adj_pick = 0;
+    TimeFwdFn tm_fwd = nullptr;
+    TimeAdjFn tm_adj = nullptr;
+    PlaneLaunch pl_fwd, pl_adj, pl_adj_plain;
+    std::vector<PlaneJob<R>> plain_jobs;  // adjoint jobs without the update
+    std::vector<long> planes;             // (t, f) planes per window
+    TimeLaunch tf, ta;
+    const FwdVariant &fv() const { return fwd_vars[fwd_pick]; }
+    const AdjVariant &av() const { return adj_vars[adj_pick]; }
+  };
+  std::vector<std::unique_ptr<FastClass>> classes;
+  std::vector<int> win_class;  // per window: its class, or -1 (generic kernels)
+  int n_generic = 0;           // windows on the generic kernels
+  int max_d_generic = 0;       // space dimensions of the generic windows
   int n_sm = 148;
-  PlaneLaunch pl_fwd, pl_adj, pl_adj_plain;
-  TimeLaunch tf_fast, ta_fast;
   DevArray<TimeJob<R>> time_jobs_fast;
   GatherLaunch g_fwd, g_input;
   std::vector<long> trace_off;   // per window, in reals
@@ -221,6 +242,11 @@ class Engine {
   long data_size = 0;
   long out_traces = 0;
   bool wavelets = false;
+  // independent problems solved together (plan.n_problems > 1): step sizes,
+  // thresholds and maxima are per problem, read by the adjoint kernels
+  bool multi = false;
+  std::vector<R> steps;        // per problem
+  DevArray<R> step_dev, pmax;  // per problem
   // prime-factor wavelet kernel (wavelet_fast.cuh), used when every window's
   // trace length factors into supported coprime prime powers
   bool wav_fast = false;
@@ -406,13 +432,16 @@ class Engine {
     L.smem = per_line * lpc;
   }
 
-  void make_time_launch(TimeLaunch &L, size_t per_trace, int nb_cap) {
+  // CTAs of nb traces over every window, or (generic_only) over the windows
+  // of the generic kernels
+  void make_time_launch(TimeLaunch &L, size_t per_trace, int nb_cap, bool generic_only) {
     int nb = nb_cap;
     while (nb > 1 && per_trace * nb > (size_t)std::min(smem_max, 160 * 1024)) nb /= 2;
     if (per_trace * nb > (size_t)smem_max)
       throw DeviceError("time window or trace too long for shared memory");
     std::vector<int> cj, ct;
     for (size_t w = 0; w < plan.windows.size(); ++w) {
+      if (generic_only && win_class[w] >= 0) continue;
       for (int t = 0; t < plan.windows[w].n_traces; t += nb) {
         cj.push_back((int)w);
         ct.push_back(t);
@@ -431,33 +460,19 @@ class Engine {
   // one block per SM; the one-stage kernels run two or three blocks per SM
   // (two for 40-point lines, whose registers do not fit three).  The
   // fastest of each list is picked by timing on the problem (autotune_space).
-  struct FwdVariant {
-    SpaceFwdFn fn;
-    int nt, np, stages;
-    size_t smem;
-  };
-  struct AdjVariant {
-    SpaceAdjFn fn;
-    int nt, np, stages;
-    size_t smem;
-  };
-  std::vector<FwdVariant> fwd_vars;
-  std::vector<AdjVariant> adj_vars;
-  int fwd_pick = 0, adj_pick = 0;
-
   template <int D, int P0, int P1, int P2, int NT, int NP, int ST, int MB>
-  void add_fwd() {
+  static void add_fwd(FastClass &c) {
     using Sh = PlaneShape<D, P0, P1, P2>;
-    fwd_vars.push_back(FwdVariant{space_fwd_fast<R, D, P0, P1, P2, NT, NP, ST, MB>, NT, NP, ST,
-                                  (size_t)ST * NP * Sh::size * sizeof(C)});
+    c.fwd_vars.push_back(FwdVariant{space_fwd_fast<R, D, P0, P1, P2, NT, NP, ST, MB>, NT, NP,
+                                    ST, (size_t)ST * NP * Sh::size * sizeof(C)});
   }
 
   template <int D, int P0, int P1, int P2, int NT, int NP, int ST, int MB>
-  void add_adj() {
+  static void add_adj(FastClass &c) {
     using Sh = PlaneShape<D, P0, P1, P2>;
     const size_t x = ST == 2 ? (size_t)NP * Sh::dense_P : 0;
-    adj_vars.push_back(AdjVariant{space_adj_fast<R, D, P0, P1, P2, NT, NP, ST, MB>, NT, NP, ST,
-                                  ((size_t)ST * NP * Sh::size + x) * sizeof(C)});
+    c.adj_vars.push_back(AdjVariant{space_adj_fast<R, D, P0, P1, P2, NT, NP, ST, MB>, NT, NP,
+                                    ST, ((size_t)ST * NP * Sh::size + x) * sizeof(C)});
   }
 
   template <int D, int P0, int P1, int P2>
@@ -469,91 +484,153 @@ class Engine {
     return true;
   }
 
-  bool space_cases(const WindowPlan &W) {
-    fwd_vars.clear();
-    adj_vars.clear();
+  static bool space_cases(const WindowPlan &W, FastClass &c) {
+    c.fwd_vars.clear();
+    c.adj_vars.clear();
     if constexpr (sizeof(R) == sizeof(float)) {
       if (shape_is<1, 40, 1, 1>(W)) {
-        add_fwd<1, 40, 1, 1, 256, 256, 2, 1>();
-        add_fwd<1, 40, 1, 1, 256, 96, 1, 2>();
-        add_adj<1, 40, 1, 1, 192, 192, 2, 1>();
-        add_adj<1, 40, 1, 1, 256, 96, 1, 2>();
+        add_fwd<1, 40, 1, 1, 256, 256, 2, 1>(c);
+        add_fwd<1, 40, 1, 1, 256, 96, 1, 2>(c);
+        add_adj<1, 40, 1, 1, 192, 192, 2, 1>(c);
+        add_adj<1, 40, 1, 1, 256, 96, 1, 2>(c);
       } else if (shape_is<1, 20, 1, 1>(W)) {
-        add_fwd<1, 20, 1, 1, 256, 256, 2, 1>();
-        add_fwd<1, 20, 1, 1, 256, 128, 1, 3>();
-        add_adj<1, 20, 1, 1, 256, 256, 2, 1>();
-        add_adj<1, 20, 1, 1, 256, 128, 1, 3>();
+        add_fwd<1, 20, 1, 1, 256, 256, 2, 1>(c);
+        add_fwd<1, 20, 1, 1, 256, 128, 1, 3>(c);
+        add_adj<1, 20, 1, 1, 256, 256, 2, 1>(c);
+        add_adj<1, 20, 1, 1, 256, 128, 1, 3>(c);
       } else if (shape_is<2, 20, 40, 1>(W)) {
-        add_fwd<2, 20, 40, 1, 384, 16, 2, 1>();
-        add_fwd<2, 20, 40, 1, 256, 12, 1, 2>();
-        add_adj<2, 20, 40, 1, 384, 11, 2, 1>();
-        add_adj<2, 20, 40, 1, 256, 12, 1, 2>();
+        add_fwd<2, 20, 40, 1, 384, 16, 2, 1>(c);
+        add_fwd<2, 20, 40, 1, 256, 12, 1, 2>(c);
+        add_adj<2, 20, 40, 1, 384, 11, 2, 1>(c);
+        add_adj<2, 20, 40, 1, 256, 12, 1, 2>(c);
       } else if (shape_is<2, 20, 20, 1>(W)) {
-        add_fwd<2, 20, 20, 1, 384, 24, 2, 1>();
-        add_fwd<2, 20, 20, 1, 256, 12, 1, 3>();
-        add_adj<2, 20, 20, 1, 384, 20, 2, 1>();
-        add_adj<2, 20, 20, 1, 256, 12, 1, 3>();
+        add_fwd<2, 20, 20, 1, 384, 24, 2, 1>(c);
+        add_fwd<2, 20, 20, 1, 256, 12, 1, 3>(c);
+        add_adj<2, 20, 20, 1, 384, 20, 2, 1>(c);
+        add_adj<2, 20, 20, 1, 256, 12, 1, 3>(c);
       } else if (shape_is<2, 40, 40, 1>(W)) {
-        add_fwd<2, 40, 40, 1, 320, 8, 2, 1>();
-        add_fwd<2, 40, 40, 1, 256, 6, 1, 2>();
-        add_adj<2, 40, 40, 1, 256, 5, 2, 1>();
-        add_adj<2, 40, 40, 1, 256, 6, 1, 2>();
+        add_fwd<2, 40, 40, 1, 320, 8, 2, 1>(c);
+        add_fwd<2, 40, 40, 1, 256, 6, 1, 2>(c);
+        add_adj<2, 40, 40, 1, 256, 5, 2, 1>(c);
+        add_adj<2, 40, 40, 1, 256, 6, 1, 2>(c);
       } else if (shape_is<3, 20, 20, 20>(W)) {
-        add_fwd<3, 20, 20, 20, 512, 1, 2, 1>();
-        add_fwd<3, 20, 20, 20, 256, 1, 1, 3>();
-        add_adj<3, 20, 20, 20, 512, 1, 2, 1>();
-        add_adj<3, 20, 20, 20, 256, 1, 1, 3>();
+        add_fwd<3, 20, 20, 20, 512, 1, 2, 1>(c);
+        add_fwd<3, 20, 20, 20, 256, 1, 1, 3>(c);
+        add_adj<3, 20, 20, 20, 512, 1, 2, 1>(c);
+        add_adj<3, 20, 20, 20, 256, 1, 1, 3>(c);
       }
     } else {
       // double: the two-stage kernels only (one-stage kernels with several
       // blocks per SM would spill), and one stage for the 20x20x20 planes
       if (shape_is<1, 40, 1, 1>(W)) {
-        add_fwd<1, 40, 1, 1, 256, 128, 2, 1>();
-        add_adj<1, 40, 1, 1, 192, 96, 2, 1>();
+        add_fwd<1, 40, 1, 1, 256, 128, 2, 1>(c);
+        add_adj<1, 40, 1, 1, 192, 96, 2, 1>(c);
       } else if (shape_is<1, 20, 1, 1>(W)) {
-        add_fwd<1, 20, 1, 1, 256, 256, 2, 1>();
-        add_adj<1, 20, 1, 1, 256, 160, 2, 1>();
+        add_fwd<1, 20, 1, 1, 256, 256, 2, 1>(c);
+        add_adj<1, 20, 1, 1, 256, 160, 2, 1>(c);
       } else if (shape_is<2, 20, 40, 1>(W)) {
-        add_fwd<2, 20, 40, 1, 384, 8, 2, 1>();
-        add_adj<2, 20, 40, 1, 384, 5, 2, 1>();
+        add_fwd<2, 20, 40, 1, 384, 8, 2, 1>(c);
+        add_adj<2, 20, 40, 1, 384, 5, 2, 1>(c);
       } else if (shape_is<2, 20, 20, 1>(W)) {
-        add_fwd<2, 20, 20, 1, 384, 12, 2, 1>();
-        add_adj<2, 20, 20, 1, 384, 10, 2, 1>();
+        add_fwd<2, 20, 20, 1, 384, 12, 2, 1>(c);
+        add_adj<2, 20, 20, 1, 384, 10, 2, 1>(c);
       } else if (shape_is<2, 40, 40, 1>(W)) {
-        add_fwd<2, 40, 40, 1, 320, 4, 2, 1>();
-        add_adj<2, 40, 40, 1, 256, 2, 2, 1>();
+        add_fwd<2, 40, 40, 1, 320, 4, 2, 1>(c);
+        add_adj<2, 40, 40, 1, 256, 2, 2, 1>(c);
       } else if (shape_is<3, 20, 20, 20>(W)) {
-        add_fwd<3, 20, 20, 20, 256, 1, 1, 1>();
-        add_adj<3, 20, 20, 20, 256, 1, 1, 1>();
+        add_fwd<3, 20, 20, 20, 256, 1, 1, 1>(c);
+        add_adj<3, 20, 20, 20, 256, 1, 1, 1>(c);
       }
     }
-    return !fwd_vars.empty() && !adj_vars.empty();
+    return !c.fwd_vars.empty() && !c.adj_vars.empty();
   }
 
-  // Times every candidate (one warm-up launch, then two timed ones with CUDA
-  // events on the engine's stream, forward X -> S0 and adjoint S0 -> X with
-  // the update epilogue) and keeps the fastest.  Choices are remembered per
-  // shape, precision, problem size class and device, so later problems of
-  // the same kind skip the timing.  AGD_GPU_SPACE_VARIANT="f,a" forces the
-  // candidates (tests).
-  void autotune_space(const std::vector<PlaneJob<R>> &jf, const std::vector<PlaneJob<R>> &ja,
-                      const std::vector<long> &planes) {
-    fwd_pick = adj_pick = 0;
+  // time-axis kernels for the window's padded time length
+  static bool time_case(const WindowPlan &W, FastClass &c) {
+    if (W.Pt == 320) {
+      c.tm_fwd = time_fwd_fast<R, 16, 10, kTimeNB>;
+      c.tm_adj = time_adj_fast<R, 16, 10, kTimeNB>;
+    } else if (W.Pt == 160) {
+      c.tm_fwd = time_fwd_fast<R, 8, 10, kTimeNB>;
+      c.tm_adj = time_adj_fast<R, 8, 10, kTimeNB>;
+    } else {
+      return false;
+    }
+    return true;
+  }
+
+  // the fast kernels assume L = 4P/5 in space and Lt = 2h = 4Pt/5 in time
+  static bool fast_eligible(const WindowPlan &W) {
+    if (W.Lt % 2 != 0 || W.Lt * 5 != W.Pt * 4) return false;
+    for (int d = 0; d < W.D; ++d)
+      if (W.L[d] * 5 != W.P[d] * 4) return false;
+    return true;
+  }
+
+  // Groups the windows into fast classes (AGD_GPU_GENERIC=1: none).
+  void pick_classes() {
+    const int nw = (int)plan.windows.size();
+    win_class.assign(nw, -1);
+    classes.clear();
+    const char *env = std::getenv("AGD_GPU_GENERIC");
+    const bool generic_only = env != nullptr && env[0] == '1';
+    std::map<std::vector<int>, int> by_key;  // -1: no instantiation
+    for (int w = 0; w < nw && !generic_only; ++w) {
+      const WindowPlan &W = plan.windows[w];
+      if (!fast_eligible(W)) continue;
+      std::vector<int> key{W.D, W.Pt};
+      for (int d = 0; d < W.D; ++d) key.push_back(W.P[d]);
+      auto it = by_key.find(key);
+      int k;
+      if (it == by_key.end()) {
+        std::unique_ptr<FastClass> c(new FastClass());
+        if (space_cases(W, *c) && time_case(W, *c)) {
+          k = (int)classes.size();
+          classes.push_back(std::move(c));
+        } else {
+          k = -1;
+        }
+        by_key[key] = k;
+      } else {
+        k = it->second;
+      }
+      if (k < 0) continue;
+      win_class[w] = k;
+      classes[k]->win.push_back(w);
+    }
+    n_generic = 0;
+    max_d_generic = 0;
+    for (int w = 0; w < nw; ++w)
+      if (win_class[w] < 0) {
+        ++n_generic;
+        max_d_generic = std::max(max_d_generic, plan.windows[w].D);
+      }
+  }
+
+  // Times every candidate of a class (one warm-up launch, then two timed ones
+  // with CUDA events on the engine's stream, forward X -> S0 and adjoint
+  // S0 -> X with the update epilogue) and keeps the fastest.  Choices are
+  // remembered per shape, precision, problem size class and device, so later
+  // problems of the same kind skip the timing.  AGD_GPU_SPACE_VARIANT="f,a"
+  // forces the candidates (tests).
+  void autotune_space(FastClass &c, const std::vector<PlaneJob<R>> &jf,
+                      const std::vector<PlaneJob<R>> &ja) {
+    c.fwd_pick = c.adj_pick = 0;
     const char *env = std::getenv("AGD_GPU_SPACE_VARIANT");
     if (env != nullptr && env[0] != '\0') {
       int f = 0, a = 0;
       if (std::sscanf(env, "%d,%d", &f, &a) == 2) {
-        fwd_pick = std::max(0, std::min(f, (int)fwd_vars.size() - 1));
-        adj_pick = std::max(0, std::min(a, (int)adj_vars.size() - 1));
+        c.fwd_pick = std::max(0, std::min(f, (int)c.fwd_vars.size() - 1));
+        c.adj_pick = std::max(0, std::min(a, (int)c.adj_vars.size() - 1));
         return;
       }
     }
-    if (fwd_vars.size() == 1 && adj_vars.size() == 1) return;
+    if (c.fwd_vars.size() == 1 && c.adj_vars.size() == 1) return;
     long total = 0;
-    for (long v : planes) total += v;
+    for (long v : c.planes) total += v;
     int dev = 0;
     CK(cudaGetDevice(&dev));
-    const WindowPlan &W = plan.windows[0];
+    const WindowPlan &W = plan.windows[c.win[0]];
     char key[128];
     std::snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%d", dev, (int)sizeof(R), W.D, W.P[0],
                   W.D > 1 ? W.P[1] : 1, W.D > 2 ? W.P[2] : 1,
@@ -564,8 +641,8 @@ class Engine {
       std::lock_guard<std::mutex> g(mu);
       auto it = cache.find(key);
       if (it != cache.end()) {
-        fwd_pick = it->second.first;
-        adj_pick = it->second.second;
+        c.fwd_pick = it->second.first;
+        c.adj_pick = it->second.second;
         return;
       }
     }
@@ -586,68 +663,43 @@ class Engine {
       return ms;
     };
     float best = 1e30f;
-    for (size_t v = 0; v < fwd_vars.size(); ++v) {
-      const FwdVariant &fv = fwd_vars[v];
+    for (size_t v = 0; v < c.fwd_vars.size(); ++v) {
+      const FwdVariant &fv = c.fwd_vars[v];
       if (fv.smem > (size_t)smem_max) continue;
       PlaneLaunch L;
-      make_plane_launch(L, jf, planes, fv.nt, fv.np, fv.smem, fv.fn);
+      make_plane_launch(L, jf, c.planes, fv.nt, fv.np, fv.smem, fv.fn);
       const float ms = timed([&] {
         fv.fn<<<L.grid, L.nt, L.smem, stream>>>(L.batches());
         CK(cudaGetLastError());
       });
       if (ms < best) {
         best = ms;
-        fwd_pick = (int)v;
+        c.fwd_pick = (int)v;
       }
     }
     best = 1e30f;
-    for (size_t v = 0; v < adj_vars.size(); ++v) {
-      const AdjVariant &av = adj_vars[v];
+    for (size_t v = 0; v < c.adj_vars.size(); ++v) {
+      const AdjVariant &av = c.adj_vars[v];
       if (av.smem > (size_t)smem_max) continue;
       PlaneLaunch L;
-      make_plane_launch(L, ja, planes, av.nt, av.np, av.smem, av.fn);
+      make_plane_launch(L, ja, c.planes, av.nt, av.np, av.smem, av.fn);
       const float ms = timed([&] {
         av.fn<<<L.grid, L.nt, L.smem, stream>>>(L.batches(), kUpdateThreshold, (R)0, (R)0,
-                                                 nullptr, scalar.get());
+                                                 nullptr, nullptr, scalar.get());
         CK(cudaGetLastError());
       });
       if (ms < best) {
         best = ms;
-        adj_pick = (int)v;
+        c.adj_pick = (int)v;
       }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     std::lock_guard<std::mutex> g(mu);
-    cache[key] = {fwd_pick, adj_pick};
+    cache[key] = {c.fwd_pick, c.adj_pick};
   }
 
-  bool pick_fast() {
-    if (plan.windows.empty()) return false;
-    const char *env = std::getenv("AGD_GPU_GENERIC");
-    if (env != nullptr && env[0] == '1') return false;
-    const WindowPlan &W0 = plan.windows[0];
-    for (const WindowPlan &W : plan.windows) {
-      if (W.D != W0.D || W.Pt != W0.Pt || W.Lt != W0.Lt || W.Lt % 2 != 0) return false;
-      // the kernels assume L = 4P/5 in space and Lt = 2h = 4Pt/5 in time
-      if (W.Lt * 5 != W.Pt * 4) return false;
-      for (int d = 0; d < W.D; ++d)
-        if (W.P[d] != W0.P[d] || W.L[d] * 5 != W.P[d] * 4) return false;
-    }
-    if (!space_cases(W0)) return false;
-    if (W0.Pt == 320) {
-      tm_fwd = time_fwd_fast<R, 16, 10, kTimeNB>;
-      tm_adj = time_adj_fast<R, 16, 10, kTimeNB>;
-    } else if (W0.Pt == 160) {
-      tm_fwd = time_fwd_fast<R, 8, 10, kTimeNB>;
-      tm_adj = time_adj_fast<R, 8, 10, kTimeNB>;
-    } else {
-      return false;
-    }
-    return true;
-  }
-
-  // Persistent, double-buffered batches of np planes; grid = resident blocks.
+  // Persistent batches of np planes; grid = resident blocks.
   template <typename K>
   void make_plane_launch(PlaneLaunch &L, const std::vector<PlaneJob<R>> &jobs,
                          const std::vector<long> &planes, int nt, int np, size_t smem,
@@ -660,6 +712,7 @@ class Engine {
         x.src = jobs[i].src + q * jobs[i].src_plane;
         x.dst = jobs[i].dst + q * jobs[i].dst_plane;
         x.count = (int)std::min<long>(np, planes[i] - q);
+        x.pid = jobs[i].pid;
         bt.push_back(x);
       }
     L.batch.upload(bt, stream);
@@ -671,72 +724,61 @@ class Engine {
     L.grid = std::max(1, std::min(L.n_batch, std::max(per_sm, 1) * n_sm));
   }
 
-  void build_fast(const std::vector<TimeJob<R>> &tj_generic) {
+  // shared-memory opt-in of every fast kernel of every class
+  void opt_in_classes() {
     const int limit = optin_smem();
-    int dyn = std::min(opt_in(tm_fwd, limit), opt_in(tm_adj, limit));
-    for (const FwdVariant &v : fwd_vars) dyn = std::min(dyn, opt_in(v.fn, limit));
-    for (const AdjVariant &v : adj_vars) dyn = std::min(dyn, opt_in(v.fn, limit));
+    int dyn = smem_max;
+    for (const auto &cp : classes) {
+      dyn = std::min({dyn, opt_in(cp->tm_fwd, limit), opt_in(cp->tm_adj, limit)});
+      for (const FwdVariant &v : cp->fwd_vars) dyn = std::min(dyn, opt_in(v.fn, limit));
+      for (const AdjVariant &v : cp->adj_vars) dyn = std::min(dyn, opt_in(v.fn, limit));
+    }
     smem_max = std::min(smem_max, dyn);
-    upload_twiddles();
-    const int nw = (int)plan.windows.size();
-    std::vector<PlaneJob<R>> jf(nw), ja(nw);
-    const WindowPlan &W0 = plan.windows[0];
+  }
+
+  void build_class(FastClass &c) {
+    const WindowPlan &W0 = plan.windows[c.win[0]];
     long dense_P = 1, dense_L = 1;
     for (int d = 0; d < W0.D; ++d) {
       dense_P *= W0.P[d];
       dense_L *= W0.L[d];
     }
-    std::vector<long> planes(nw);
-    std::vector<TimeJob<R>> tj = tj_generic;
-    for (int w = 0; w < nw; ++w) {
+    std::vector<PlaneJob<R>> jf, ja;
+    c.planes.clear();
+    for (int w : c.win) {
       const WindowPlan &W = plan.windows[w];
-      planes[w] = (long)W.T * W.F;
+      c.planes.push_back((long)W.T * W.F);
       PlaneJob<R> j{};
+      j.pid = W.problem;
       j.src = X.get() + W.model_off;
       j.dst = S0.get() + W.model_off;
       j.src_plane = dense_P;
       j.dst_plane = dense_L;
-      jf[w] = j;
+      jf.push_back(j);
       j.src = S0.get() + W.model_off;
       j.dst = X.get() + W.model_off;
       j.src_plane = dense_L;
       j.dst_plane = dense_P;
-      ja[w] = j;
-      tj[w].z = S0.get() + W.model_off;
+      ja.push_back(j);
     }
-    autotune_space(jf, ja, planes);
-    const FwdVariant &fv = fwd_vars[fwd_pick];
-    const AdjVariant &av = adj_vars[adj_pick];
-    sp_fwd = fv.fn;
-    sp_adj = av.fn;
-    nt_fwd = fv.nt;
-    np_fwd = fv.np;
-    smem_fwd = fv.smem;
-    nt_adj = av.nt;
-    np_adj = av.np;
-    smem_adj = av.smem;
-    make_plane_launch(pl_fwd, jf, planes, nt_fwd, np_fwd, smem_fwd, sp_fwd);
-    make_plane_launch(pl_adj, ja, planes, nt_adj, np_adj, smem_adj, sp_adj);
-    pending_plane_plain = ja;
-    pending_planes = planes;
-    time_jobs_fast.upload(tj, stream);
-    const int h = plan.windows[0].h;
-    const int LS = plan.windows[0].Pt / 2 + 1;
+    autotune_space(c, jf, ja);
+    make_plane_launch(c.pl_fwd, jf, c.planes, c.fv().nt, c.fv().np, c.fv().smem, c.fv().fn);
+    make_plane_launch(c.pl_adj, ja, c.planes, c.av().nt, c.av().np, c.av().smem, c.av().fn);
+    c.plain_jobs = ja;
+    const int h = W0.h;
+    const int LS = W0.Pt / 2 + 1;
     const size_t per_fwd = 2 * (size_t)LS * sizeof(C) + (size_t)h * sizeof(R);
     const size_t per_adj = (size_t)LS * sizeof(C) + 2 * (size_t)(2 * h) * sizeof(R);
-    make_fixed_time_launch(tf_fast, per_fwd * kTimeNB);
-    make_fixed_time_launch(ta_fast, per_adj * kTimeNB);
+    make_fixed_time_launch(c.tf, per_fwd * kTimeNB, c.win);
+    make_fixed_time_launch(c.ta, per_adj * kTimeNB, c.win);
   }
 
-  std::vector<PlaneJob<R>> pending_plane_plain;
-  std::vector<long> pending_planes;
-
-  void make_fixed_time_launch(TimeLaunch &L, size_t smem) {
+  void make_fixed_time_launch(TimeLaunch &L, size_t smem, const std::vector<int> &wins) {
     if (smem > (size_t)smem_max) throw DeviceError("time window too long for shared memory");
     std::vector<int> cj, ct;
-    for (size_t w = 0; w < plan.windows.size(); ++w)
+    for (int w : wins)
       for (int t = 0; t < plan.windows[w].n_traces; t += kTimeNB) {
-        cj.push_back((int)w);
+        cj.push_back(w);
         ct.push_back(t);
       }
     L.cta_job.upload(cj, stream);
@@ -830,15 +872,20 @@ class Engine {
     wt_dst.upload(wdst, stream);
     wt_C.upload(wC, stream);
 
-    fast = pick_fast();
+    pick_classes();
     X.alloc(M);
     S0.alloc(M);
-    if (!fast) S1.alloc(M);
+    if (n_generic) S1.alloc(M);
     Y.alloc(toff);
     rec_d.alloc(plan.record_size);
     rec_r.alloc(plan.record_size);
     scalar.alloc(1);
     dscalar.alloc(1);
+    multi = plan.n_problems > 1;
+    if (multi) {
+      step_dev.alloc(plan.n_problems);
+      pmax.alloc(plan.n_problems);
+    }
     {
       std::vector<uint8_t> m(plan.record_size, 0);
       for (const auto &mu : plan.mute)
@@ -875,13 +922,21 @@ class Engine {
       v.fft = wavelets ? fft.get(W.C) : 0;
     }
     time_jobs.upload(tj, stream);
-    if (fast) build_fast(tj);
+    if (!classes.empty()) {
+      std::vector<TimeJob<R>> tjf = tj;
+      for (int w = 0; w < nw; ++w)
+        if (win_class[w] >= 0) tjf[w].z = S0.get() + plan.windows[w].model_off;
+      time_jobs_fast.upload(tjf, stream);
+      opt_in_classes();
+      upload_twiddles();
+      for (auto &c : classes) build_class(*c);
+    }
     const size_t per_trace_time = 2 * (size_t)Pt_max * sizeof(C) + (size_t)C_max * sizeof(R);
-    make_time_launch(time_fwd, per_trace_time, 16);
-    make_time_launch(time_adj, per_trace_time, 16);
+    make_time_launch(time_fwd, per_trace_time, 16, true);
+    make_time_launch(time_adj, per_trace_time, 16, true);
     if (wavelets) {
       wav_jobs.upload(wj, stream);
-      make_time_launch(wav, 2 * (size_t)C_max * sizeof(C), 8);
+      make_time_launch(wav, 2 * (size_t)C_max * sizeof(C), 8, false);
       // spectra table
       std::vector<C> sp;
       std::vector<long> so;
@@ -900,7 +955,7 @@ class Engine {
     }
 
     // ---- space-axis passes (generic path)
-    if (fast) maxD = 0;
+    maxD = max_d_generic;
     fwd.resize(maxD);
     adj_update.resize(maxD);
     adj_plain.resize(maxD);
@@ -908,7 +963,7 @@ class Engine {
       std::vector<AxisJob<R>> jf, ju, jp;
       for (int w = 0; w < nw; ++w) {
         const WindowPlan &W = plan.windows[w];
-        if (W.D <= k) continue;
+        if (W.D <= k || win_class[w] >= 0) continue;
         const long TF = (long)W.T * W.F;
         {  // forward: axis D-1-k, inverse FFT, crop P -> L
           const int a = W.D - 1 - k;
@@ -924,6 +979,7 @@ class Engine {
           j.n_in = W.P[a];
           j.n_out = W.L[a];
           j.fft = fft.get(W.P[a]);
+          j.pid = W.problem;
           jf.push_back(j);
         }
         {  // adjoint: axis k, zero-pad L -> P, forward FFT
@@ -939,6 +995,7 @@ class Engine {
           j.n_in = W.L[a];
           j.n_out = W.P[a];
           j.fft = fft.get(W.P[a]);
+          j.pid = W.problem;
           const bool last = (k == W.D - 1);
           j.last = last ? 1 : 0;
           j.dst = last ? X.get() + W.model_off : Sb[(W.D + k) & 1] + W.model_off;
@@ -1020,19 +1077,20 @@ class Engine {
   void ensure_plain_adjoint() {
     if (G.get() != nullptr || plan.model_size == 0) return;
     G.alloc(plan.model_size);
-    if (fast) {
-      std::vector<PlaneJob<R>> jobs = pending_plane_plain;
-      for (size_t w = 0; w < jobs.size(); ++w) jobs[w].dst = G.get() + plan.windows[w].model_off;
-      make_plane_launch(pl_adj_plain, jobs, pending_planes, nt_adj, np_adj, smem_adj, sp_adj);
-      CK(cudaStreamSynchronize(stream));
-      return;
+    for (auto &cp : classes) {
+      FastClass &c = *cp;
+      std::vector<PlaneJob<R>> jobs = c.plain_jobs;
+      for (size_t i = 0; i < jobs.size(); ++i)
+        jobs[i].dst = G.get() + plan.windows[c.win[i]].model_off;
+      make_plane_launch(c.pl_adj_plain, jobs, c.planes, c.av().nt, c.av().np, c.av().smem,
+                        c.av().fn);
     }
     for (size_t k = 0; k < pending_plain.size(); ++k) {
       auto jobs = pending_plain[k];
       size_t i = 0;
       for (int w = 0; w < (int)plan.windows.size(); ++w) {
         const WindowPlan &W = plan.windows[w];
-        if (W.D <= (int)k) continue;
+        if (W.D <= (int)k || win_class[w] >= 0) continue;
         if ((int)k == W.D - 1) jobs[i].dst = G.get() + W.model_off;
         ++i;
       }
@@ -1052,7 +1110,8 @@ class Engine {
     if (L.n_cta == 0) return;
     axis_pass<R><<<L.n_cta, kThreads, L.smem, stream>>>(
         L.jobs.get(), L.cta_job.get(), L.cta_line0.get(), L.lpc, d_descs.get(), d_tw.get(),
-        inverse, epilogue, step, lamb, lamb_dev, scalar.get());
+        inverse, epilogue, step, lamb, multi ? step_dev.get() : nullptr, lamb_dev,
+        multi ? pmax.get() : scalar.get());
     CK(cudaGetLastError());
   }
 
@@ -1065,48 +1124,72 @@ class Engine {
     CK(cudaGetLastError());
   }
 
-  void launch_space_fwd() {
-    if (pl_fwd.n_batch == 0) return;
-    sp_fwd<<<pl_fwd.grid, pl_fwd.nt, pl_fwd.smem, stream>>>(pl_fwd.batches());
+  void launch_space_fwd(const FastClass &c) {
+    if (c.pl_fwd.n_batch == 0) return;
+    c.fv().fn<<<c.pl_fwd.grid, c.pl_fwd.nt, c.pl_fwd.smem, stream>>>(c.pl_fwd.batches());
     CK(cudaGetLastError());
   }
 
-  void launch_space_adj(const PlaneLaunch &L, int epilogue, R step, R lamb,
+  void launch_space_adj(const FastClass &c, const PlaneLaunch &L, int epilogue, R step, R lamb,
                         const R *lamb_dev = nullptr) {
     if (L.n_batch == 0) return;
-    sp_adj<<<L.grid, L.nt, L.smem, stream>>>(L.batches(), epilogue, step, lamb, lamb_dev,
-                                             scalar.get());
+    c.av().fn<<<L.grid, L.nt, L.smem, stream>>>(L.batches(), epilogue, step, lamb,
+                                                 multi ? step_dev.get() : nullptr, lamb_dev,
+                                                 multi ? pmax.get() : scalar.get());
     CK(cudaGetLastError());
   }
 
+  // time c2r + taper + overlap-add of every window (fast classes, then the
+  // generic windows)
   void launch_time_fwd() {
-    if (fast) {
-      if (tf_fast.n_cta)
-        tm_fwd<<<tf_fast.n_cta, kThreads, tf_fast.smem, stream>>>(
-            time_jobs_fast.get(), tf_fast.cta_job.get(), tf_fast.cta_trace0.get());
-    } else if (time_fwd.n_cta) {
-      time_c2r_ola<R><<<time_fwd.n_cta, kThreads, time_fwd.smem, stream>>>(
-          time_jobs.get(), time_fwd.cta_job.get(), time_fwd.cta_trace0.get(), time_fwd.nb,
-          d_descs.get(), d_tw.get());
+    for (const auto &cp : classes) {
+      const FastClass &c = *cp;
+      if (!c.tf.n_cta) continue;
+      c.tm_fwd<<<c.tf.n_cta, kThreads, c.tf.smem, stream>>>(
+          time_jobs_fast.get(), c.tf.cta_job.get(), c.tf.cta_trace0.get());
+      CK(cudaGetLastError());
     }
-    CK(cudaGetLastError());
-  }
-
-  // Y = W F X  (window traces of the current model)
-  void forward_traces() {
-    if (fast) {
-      launch_space_fwd();
-      launch_time_fwd();
-      if (wavelets) launch_wavelet(+1);
-      return;
-    }
-    for (size_t k = 0; k < fwd.size(); ++k) launch_axis(fwd[k], 1, kStore, 0, 0);
     if (time_fwd.n_cta) {
       time_c2r_ola<R><<<time_fwd.n_cta, kThreads, time_fwd.smem, stream>>>(
           time_jobs.get(), time_fwd.cta_job.get(), time_fwd.cta_trace0.get(), time_fwd.nb,
           d_descs.get(), d_tw.get());
       CK(cudaGetLastError());
     }
+  }
+
+  // blend adjoint gather + taper + time r2c of every window, from the record
+  // (from_record) or from the window traces (after the wavelet correlation)
+  void launch_time_adj(const R *record, int from_record) {
+    for (const auto &cp : classes) {
+      const FastClass &c = *cp;
+      if (!c.ta.n_cta) continue;
+      c.tm_adj<<<c.ta.n_cta, kThreads, c.ta.smem, stream>>>(
+          time_jobs_fast.get(), c.ta.cta_job.get(), c.ta.cta_trace0.get(), record, from_record);
+      CK(cudaGetLastError());
+    }
+    if (time_adj.n_cta) {
+      time_r2c<R><<<time_adj.n_cta, kThreads, time_adj.smem, stream>>>(
+          time_jobs.get(), time_adj.cta_job.get(), time_adj.cta_trace0.get(), time_adj.nb,
+          d_descs.get(), d_tw.get(), record, from_record);
+      CK(cudaGetLastError());
+    }
+  }
+
+  void launch_space_fwd_all() {
+    for (const auto &cp : classes) launch_space_fwd(*cp);
+    for (size_t k = 0; k < fwd.size(); ++k) launch_axis(fwd[k], 1, kStore, 0, 0);
+  }
+
+  void launch_space_adj_all(int epilogue, R step, R lamb, const R *lamb_dev) {
+    for (const auto &cp : classes) launch_space_adj(*cp, cp->pl_adj, epilogue, step, lamb, lamb_dev);
+    for (size_t k = 0; k < adj_update.size(); ++k)
+      launch_axis(adj_update[k], 0, epilogue, step, lamb, lamb_dev);
+  }
+
+  // Y = W F X  (window traces of the current model)
+  void forward_traces() {
+    launch_space_fwd_all();
+    launch_time_fwd();
     if (wavelets) launch_wavelet(+1);
   }
 
@@ -1144,18 +1227,7 @@ class Engine {
       CK(cudaGetLastError());
       launch_wavelet(-1);
     }
-    if (fast) {
-      if (ta_fast.n_cta)
-        tm_adj<<<ta_fast.n_cta, kThreads, ta_fast.smem, stream>>>(
-            time_jobs_fast.get(), ta_fast.cta_job.get(), ta_fast.cta_trace0.get(), record,
-            wavelets ? 0 : 1);
-      CK(cudaGetLastError());
-    } else if (time_adj.n_cta) {
-      time_r2c<R><<<time_adj.n_cta, kThreads, time_adj.smem, stream>>>(
-          time_jobs.get(), time_adj.cta_job.get(), time_adj.cta_trace0.get(), time_adj.nb,
-          d_descs.get(), d_tw.get(), record, wavelets ? 0 : 1);
-      CK(cudaGetLastError());
-    }
+    launch_time_adj(record, wavelets ? 0 : 1);
   }
 
   // X <- threshold(X - step * A^H record, lamb); lambda is read from
@@ -1163,13 +1235,18 @@ class Engine {
   void adjoint_update(const R *record, R step, R lamb, bool track_max,
                       const R *lamb_dev = nullptr) {
     adjoint_time(record);
-    if (fast) {
-      launch_space_adj(pl_adj, track_max ? kUpdateMax : kUpdateThreshold, step, lamb, lamb_dev);
-      return;
-    }
-    for (size_t k = 0; k < adj_update.size(); ++k)
-      launch_axis(adj_update[k], 0, track_max ? kUpdateMax : kUpdateThreshold, step, lamb,
-                  lamb_dev);
+    launch_space_adj_all(track_max ? kUpdateMax : kUpdateThreshold, step, lamb, lamb_dev);
+  }
+
+  // kernels launched by one ISTA iteration (iteration_body)
+  int kernels_per_iteration() const {
+    int n = 2 * (int)classes.size();  // space passes, forward and adjoint
+    for (const auto &cp : classes) n += (cp->tf.n_cta ? 1 : 0) + (cp->ta.n_cta ? 1 : 0);
+    n += (int)fwd.size() + (int)adj_update.size();
+    n += (time_fwd.n_cta ? 1 : 0) + (time_adj.n_cta ? 1 : 0);
+    n += (g_fwd.n_chunk ? 1 : 0) + 1;  // residual gather, threshold schedule
+    if (wavelets) n += wav_fast ? 2 : 3;
+    return n;
   }
 
   // ---------------------------------------------------------------- graphs
@@ -1188,7 +1265,8 @@ class Engine {
     }
   }
 
-  // table[k] = lambda used after iteration k + 1.  The captured graph holds
+  // table[k * n_problems + p] = lambda of problem p used after iteration
+  // k + 1.  The captured graph holds
   // the table's address, so the table keeps its allocation while it is
   // large enough; growing it drops the graph (re-captured on next use).
   void load_schedule(const std::vector<R> &table) {
@@ -1199,7 +1277,7 @@ class Engine {
     }
     CK(cudaMemcpyAsync(lamb_table.get(), table.data(), table.size() * sizeof(R),
                        cudaMemcpyHostToDevice, stream));
-    if (lamb_cur.get() == nullptr) lamb_cur.alloc(1);
+    if (lamb_cur.get() == nullptr) lamb_cur.alloc(plan.n_problems);
     if (lamb_counter.get() == nullptr) lamb_counter.alloc(1);
     CK(cudaMemsetAsync(lamb_counter.get(), 0, sizeof(int), stream));
   }
@@ -1207,7 +1285,8 @@ class Engine {
   void iteration_body(bool want_norm) {
     forward_traces();
     residual(want_norm);
-    next_lambda<R><<<1, 32, 0, stream>>>(lamb_table.get(), lamb_counter.get(), lamb_cur.get());
+    next_lambda<R><<<1, 256, 0, stream>>>(lamb_table.get(), lamb_counter.get(), lamb_cur.get(),
+                                          plan.n_problems);
     CK(cudaGetLastError());
     adjoint_update(rec_r.get(), stepsize, (R)0, false, lamb_cur.get());
   }
@@ -1277,6 +1356,25 @@ class Engine {
       CK(cudaGetLastError());
     }
     launch_gather(g_fwd, Y.get(), rec_r.get(), kGatherSum, false, nullptr, nullptr, 0, nullptr);
+    if (multi) {  // one maximum per problem, over its record range
+      const int np = plan.n_problems;
+      std::vector<R> fac(np, (R)1);
+      CK(cudaMemcpyAsync(pmax.get(), fac.data(), np * sizeof(R), cudaMemcpyHostToDevice,
+                         stream));
+      for (int p = 0; p < np; ++p)
+        if (plan.problem_rec_size[p])
+          record_max<R><<<grid_for(plan.problem_rec_size[p]), kThreads, 0, stream>>>(
+              rec_r.get() + plan.problem_rec_off[p], plan.problem_rec_size[p], pmax.get() + p);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(fac.data(), pmax.get(), np * sizeof(R), cudaMemcpyDeviceToHost,
+                         stream));
+      CK(cudaStreamSynchronize(stream));
+      steps.resize(np);
+      for (int p = 0; p < np; ++p) steps[p] = (R)0.5 / fac[p];
+      step_dev.upload(steps, stream);
+      stepsize = steps[0];
+      return stepsize;
+    }
     R one = (R)1;
     CK(cudaMemcpyAsync(scalar.get(), &one, sizeof(R), cudaMemcpyHostToDevice, stream));
     if (plan.record_size)
@@ -1285,6 +1383,7 @@ class Engine {
     CK(cudaGetLastError());
     const R factor = read_scalar();
     stepsize = (R)0.5 / factor;
+    steps.assign(1, stepsize);
     return stepsize;
   }
 
@@ -1315,8 +1414,10 @@ class Engine {
       for (int p = 0; p < plan.n_patches; ++p) {
         const int nt = plan.n_times[p];
         for (int t = 0; t < plan.n_traces[p]; ++t) {
-          const BlendCoord b = plan.coord_of(shottimes[p][t], nt, channels[p][t],
-                                             (int)trace_types[p][t]);
+          const BlendCoord b = !plan.input_coord.empty()
+                                   ? plan.input_coord[p][t]
+                                   : plan.coord_of(shottimes[p][t], nt, channels[p][t],
+                                                   (int)trace_types[p][t]);
           if (b.rec < 0) continue;
           list.push_back(Contrib{b.rec, patch_off[p] + (long)t * nt + b.trace_start, b.n, 0});
         }
@@ -1351,6 +1452,43 @@ class Engine {
     CK(cudaGetLastError());
   }
 
+  // Initial step of problems solved together: x = -step_p A^H d per problem,
+  // lambda_0 of each problem from its own model range
+  std::vector<R> initial_steps() {
+    const int np = plan.n_problems;
+    if (plan.model_size) CK(cudaMemsetAsync(X.get(), 0, X.bytes(), stream));
+    CK(cudaMemsetAsync(pmax.get(), 0, np * sizeof(R), stream));
+    adjoint_update(rec_d.get(), stepsize, (R)0, true);
+    std::vector<R> m(np);
+    CK(cudaMemcpyAsync(m.data(), pmax.get(), np * sizeof(R), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    for (R &v : m) v = (R)std::sqrt(v);
+    return m;
+  }
+
+  // Initial step, first threshold and the device schedule of every problem:
+  // returns the table loaded on the device, rows x n_problems (the schedule
+  // repeated when rows exceeds n_its - 1).
+  std::vector<R> start_schedule(R initial_factor, int n_its, int rows) {
+    const int np = plan.n_problems;
+    const std::vector<R> lamb0 = multi ? initial_steps() : std::vector<R>{initial_step()};
+    std::vector<R> table((size_t)rows * np);
+    for (int p = 0; p < np; ++p) {
+      R first = 0;
+      const std::vector<R> t = schedule_table(lamb0[p], initial_factor, n_its, &first);
+      if (!multi) {
+        threshold_model(first);
+      } else if (plan.problem_model_size[p]) {
+        model_threshold<R><<<grid_for(plan.problem_model_size[p]), kThreads, 0, stream>>>(
+            X.get() + plan.problem_model_off[p], plan.problem_model_size[p], first);
+        CK(cudaGetLastError());
+      }
+      for (int r = 0; r < rows; ++r) table[(size_t)r * np + p] = t[r % t.size()];
+    }
+    load_schedule(table);
+    return table;
+  }
+
   // Thresholds after the initial step: the schedule of src/agdeblend.c:
   // 526-533,588-589,623-627 evaluated in AGD_TYPE on the host.
   static std::vector<R> schedule_table(R lamb0, R initial_factor, int n_its, R *first) {
@@ -1372,11 +1510,7 @@ class Engine {
   // the solver of agd_deblend (src/agdeblend.c:584-633); iterations replay a
   // captured CUDA graph unless residuals are printed
   void solve(R initial_factor, int n_its, int print_freq) {
-    R lamb0 = initial_step();
-    R first = 0;
-    const std::vector<R> table = schedule_table(lamb0, initial_factor, n_its, &first);
-    threshold_model(first);
-    load_schedule(table);
+    start_schedule(initial_factor, n_its, std::max(1, n_its - 1));
     if (print_freq > 0) {
       const double r = record_norm(rec_d.get());
       std::printf("Iteration 0 Residual %f\n", r);
@@ -1454,20 +1588,22 @@ agd::ProblemArgs make_args(int n_patches, int const *volumes, int const *n_dims,
                           trace_types, wavelet_lengths, wavelet_idxs, wavelets};
 }
 
-int create_problem(const agd::ProblemArgs &a, agd_gpu_problem **out) {
+// A problem handle over a plan of one or more problems (args in problem
+// order; their patches follow one another in the plan).
+int create_from_plan(const std::vector<agd::ProblemArgs> &args, agd::Plan &&plan,
+                     agd_gpu_problem **out) {
   *out = nullptr;
-  agd::Plan plan;
-  if (agd::build_plan(a, plan)) return 1;
   auto *pb = new agd_gpu_problem();
   try {
-    pb->shottimes.resize(a.n_patches);
-    pb->channels.resize(a.n_patches);
-    pb->trace_types.resize(a.n_patches);
-    for (int p = 0; p < a.n_patches; ++p) {
-      const int n = plan.n_traces[p];
-      pb->shottimes[p].assign(a.shottimes[p], a.shottimes[p] + n);
-      pb->channels[p].assign(a.channels[p], a.channels[p] + n);
-      pb->trace_types[p].assign(a.trace_types[p], a.trace_types[p] + n);
+    int gp = 0;
+    for (const agd::ProblemArgs &a : args)
+      for (int p = 0; p < a.n_patches; ++p, ++gp) {
+        const int n = plan.n_traces[gp];
+        pb->shottimes.emplace_back(a.shottimes[p], a.shottimes[p] + n);
+        pb->channels.emplace_back(a.channels[p], a.channels[p] + n);
+        pb->trace_types.emplace_back(a.trace_types[p], a.trace_types[p] + n);
+      }
+    for (int p = 0; p < gp; ++p) {
       pb->st_p.push_back(pb->shottimes[p].data());
       pb->ch_p.push_back(pb->channels[p].data());
       pb->tt_p.push_back(pb->trace_types[p].data());
@@ -1481,6 +1617,37 @@ int create_problem(const agd::ProblemArgs &a, agd_gpu_problem **out) {
   }
   *out = pb;
   return 0;
+}
+
+int create_problem(const agd::ProblemArgs &a, agd_gpu_problem **out) {
+  *out = nullptr;
+  agd::Plan plan;
+  if (agd::build_plan(a, plan)) return 1;
+  return create_from_plan({a}, std::move(plan), out);
+}
+
+// Arguments of problem q of a batch call (each argument is an array over
+// the problems of agd_deblend's argument).
+agd::ProblemArgs batch_args(int q, int const *n_patches, int const *const *volumes,
+                            int const *const *n_dims, int const *const *const *window_shapes,
+                            int const *const *const *coords, int const *const *const *shapes,
+                            long int const *const *const *shottimes,
+                            int const *const *const *channels,
+                            enum AGDTraceType const *const *const *trace_types,
+                            int const *const *wavelet_lengths,
+                            int const *const *const *wavelet_idxs,
+                            AGD_TYPE const *const *const *wavelets) {
+  return make_args(n_patches[q], volumes[q], n_dims[q], window_shapes[q], coords[q], shapes[q],
+                   shottimes[q], channels[q], trace_types[q],
+                   wavelet_lengths ? wavelet_lengths[q] : nullptr,
+                   wavelet_idxs ? wavelet_idxs[q] : nullptr, wavelets ? wavelets[q] : nullptr);
+}
+
+int create_batch(const std::vector<agd::ProblemArgs> &args, agd_gpu_problem **out) {
+  *out = nullptr;
+  agd::Plan plan;
+  if (agd::build_batch_plan(args, plan)) return 1;
+  return create_from_plan(args, std::move(plan), out);
 }
 
 template <typename F>
@@ -1529,12 +1696,18 @@ int agd_gpu_problem_info(agd_gpu_problem const *pb, long int *info) {
   info[5] = (long)e.plan.mute.size();
   info[6] = (long)e.device_bytes();
   info[7] = e.g_fwd.n_contrib;
-  info[8] = e.fast ? 1 : 0;
+  long n_fast = 0;
+  for (int c : e.win_class) n_fast += c >= 0 ? 1 : 0;
+  const long nw = (long)e.plan.windows.size();
+  info[8] = (nw > 0 && n_fast == nw) ? 1 : (n_fast > 0 ? 2 : 0);
   info[9] = e.wav_fast ? 1 : 0;
-  info[10] = e.fast ? e.fwd_pick : -1;
-  info[11] = e.fast ? e.adj_pick : -1;
-  info[12] = (long)e.fwd_vars.size();
-  info[13] = (long)e.adj_vars.size();
+  info[10] = e.classes.empty() ? -1 : e.classes[0]->fwd_pick;
+  info[11] = e.classes.empty() ? -1 : e.classes[0]->adj_pick;
+  info[12] = e.classes.empty() ? 0 : (long)e.classes[0]->fwd_vars.size();
+  info[13] = e.classes.empty() ? 0 : (long)e.classes[0]->adj_vars.size();
+  info[14] = e.kernels_per_iteration();
+  info[15] = (long)e.classes.size();
+  info[16] = n_fast;
   return 0;
 }
 
@@ -1569,7 +1742,7 @@ int agd_gpu_adjoint(agd_gpu_problem *pb, AGD_TYPE const *record, AGD_TYPE *model
       agd::CK(cudaMemcpyAsync(e.rec_r.get(), record, e.rec_r.bytes(), cudaMemcpyHostToDevice,
                               e.stream));
     e.adjoint_time(e.rec_r.get());
-    if (e.fast) e.launch_space_adj(e.pl_adj_plain, agd::kStore, 0, 0);
+    for (const auto &cp : e.classes) e.launch_space_adj(*cp, cp->pl_adj_plain, agd::kStore, 0, 0);
     for (size_t k = 0; k < e.adj_plain.size(); ++k)
       e.launch_axis(e.adj_plain[k], 0, agd::kStore, 0, 0);
     e.model_to_ref(e.G.get(), model);
@@ -1629,17 +1802,10 @@ int agd_gpu_time_iterations(agd_gpu_problem *pb, AGD_TYPE const *const *data,
     agd::EngineR &e = *pb->eng;
     e.upload_data(data);
     pb->input_blend();
-    const AGD_TYPE lamb0 = e.initial_step();
-    AGD_TYPE first = 0;
-    const std::vector<AGD_TYPE> sched =
-        agd::EngineR::schedule_table(lamb0, initial_factor, n_its, &first);
-    e.threshold_model(first);
     // thresholds for every replay: the schedule, repeated if the run is
     // longer than n_its - 1 iterations
-    const int total = warmup + steps + 2;
-    std::vector<AGD_TYPE> table(total);
-    for (int k = 0; k < total; ++k) table[k] = sched[k % sched.size()];
-    e.load_schedule(table);
+    const std::vector<AGD_TYPE> table =
+        e.start_schedule(initial_factor, n_its, warmup + steps + 2);
     e.capture_iteration();
     for (int i = 0; i < warmup; ++i) e.replay_iteration();
     cudaEvent_t ev[4];
@@ -1657,7 +1823,8 @@ int agd_gpu_time_iterations(agd_gpu_problem *pb, AGD_TYPE const *const *data,
     agd::CK(cudaEventElapsedTime(&ms_total, ev[0], ev[1]));
     agd::CK(cudaEventElapsedTime(&ms_fwd, ev[2], ev[3]));
     agd::CK(cudaEventRecord(ev[2], e.stream));
-    e.adjoint_update(e.rec_r.get(), e.stepsize, table[warmup + steps], false);
+    e.adjoint_update(e.rec_r.get(), e.stepsize,
+                     table[(size_t)(warmup + steps) * e.plan.n_problems], false);
     agd::CK(cudaEventRecord(ev[3], e.stream));
     agd::CK(cudaEventSynchronize(ev[3]));
     float ms_adj = 0;
@@ -1683,15 +1850,9 @@ int agd_gpu_profile_iteration(agd_gpu_problem *pb, AGD_TYPE lamb, double *ms) {
       agd::CK(cudaEventRecord(v, e.stream));
       ev.push_back(v);
     };
-    const int nf = e.fast ? 1 : (int)e.fwd.size();
     mark();
-    for (int k = 0; k < nf; ++k) {
-      if (e.fast)
-        e.launch_space_fwd();
-      else
-        e.launch_axis(e.fwd[k], 1, agd::kStore, 0, 0);
-      mark();
-    }
+    e.launch_space_fwd_all();
+    mark();
     e.launch_time_fwd();
     mark();
     if (e.wavelets) e.launch_wavelet(+1);
@@ -1700,32 +1861,23 @@ int agd_gpu_profile_iteration(agd_gpu_problem *pb, AGD_TYPE lamb, double *ms) {
     mark();
     e.adjoint_time(e.rec_r.get());
     mark();
-    for (int k = 0; k < nf; ++k) {
-      if (e.fast)
-        e.launch_space_adj(e.pl_adj, agd::kUpdateThreshold, e.stepsize, lamb);
-      else
-        e.launch_axis(e.adj_update[k], 0, agd::kUpdateThreshold, e.stepsize, lamb);
-      mark();
-    }
+    e.launch_space_adj_all(agd::kUpdateThreshold, e.stepsize, lamb, nullptr);
+    mark();
     agd::CK(cudaEventSynchronize(ev.back()));
     auto dt = [&](int a, int b) {
       float v = 0;
       agd::CK(cudaEventElapsedTime(&v, ev[a], ev[b]));
       return (double)v;
     };
-    // [0] forward space passes, [1] time c2r + overlap-add, [2] wavelet
-    // forward, [3] blend gather + residual, [4] adjoint time (incl. gather
-    // and wavelet), [5] adjoint space passes incl. update, [6..9] forward
-    // passes by index, [10..13] adjoint passes by index, [14] passes count
-    for (int k = 0; k < nf && k < 4; ++k) ms[6 + k] = dt(k, k + 1);
-    ms[0] = dt(0, nf);
-    ms[1] = dt(nf, nf + 1);
-    ms[2] = dt(nf + 1, nf + 2);
-    ms[3] = dt(nf + 2, nf + 3);
-    ms[4] = dt(nf + 3, nf + 4);
-    for (int k = 0; k < nf && k < 4; ++k) ms[10 + k] = dt(nf + 4 + k, nf + 5 + k);
-    ms[5] = dt(nf + 4, nf + 4 + nf);
-    ms[14] = nf;
+    // [0] space passes of the forward operator (all windows), [1] time c2r +
+    // overlap-add, [2] wavelet convolution, [3] blend gather + residual,
+    // [4] adjoint time (incl. blend gather and wavelet correlation),
+    // [5] adjoint space passes incl. the update; [6] = [0], [10] = [5] and
+    // [14] = 1 (the space phases counted as one pass)
+    for (int k = 0; k < 6; ++k) ms[k] = dt(k, k + 1);
+    ms[6] = ms[0];
+    ms[10] = ms[5];
+    ms[14] = 1;
     for (auto v : ev) cudaEventDestroy(v);
     return 0;
   });
@@ -1815,6 +1967,76 @@ int agd_deblend(int n_patches, int const *volumes, int const *n_dims,
   if (pb->eng->stepsize > (AGD_TYPE)0.3)
     std::printf("WARNING: There does not appear to be any overlap between shots\n");
   const int rc = agd_gpu_solve(pb, initial_factor, n_its, print_freq, data);
+  delete pb;
+  return rc;
+}
+
+int agd_gpu_batch_create(int n_problems, int const *n_patches, int const *const *volumes,
+                         int const *const *n_dims, int const *const *const *window_shapes,
+                         int const *const *const *coords, int const *const *const *shapes,
+                         long int const *const *const *shottimes,
+                         int const *const *const *channels,
+                         enum AGDTraceType const *const *const *trace_types,
+                         int const *const *wavelet_lengths, int const *const *const *wavelet_idxs,
+                         AGD_TYPE const *const *const *wavelets, agd_gpu_problem **problem) {
+  if (problem == nullptr || n_problems <= 0 || n_patches == nullptr || volumes == nullptr ||
+      n_dims == nullptr || window_shapes == nullptr || coords == nullptr || shapes == nullptr ||
+      shottimes == nullptr || channels == nullptr || trace_types == nullptr) {
+    std::fprintf(stderr, "ERROR: invalid batch arguments\nERROR in agd_gpu_batch_create\n");
+    return 1;
+  }
+  std::vector<agd::ProblemArgs> args;
+  for (int q = 0; q < n_problems; ++q) {
+    args.push_back(batch_args(q, n_patches, volumes, n_dims, window_shapes, coords, shapes,
+                              shottimes, channels, trace_types, wavelet_lengths, wavelet_idxs,
+                              wavelets));
+    std::vector<AGD_TYPE *> dummy(n_patches[q] > 0 ? n_patches[q] : 1, (AGD_TYPE *)1);
+    if (agd::check_deblend_inputs(args.back(), (AGD_TYPE)1, 1, dummy.data())) {
+      std::fprintf(stderr, "ERROR in problem %d of agd_gpu_batch_create\n", q);
+      return 1;
+    }
+  }
+  return create_batch(args, problem);
+}
+
+int agd_gpu_problem_steps(agd_gpu_problem const *pb, AGD_TYPE *steps) {
+  if (pb == nullptr || steps == nullptr) return 1;
+  const agd::EngineR &e = *pb->eng;
+  for (size_t q = 0; q < e.steps.size(); ++q) steps[q] = e.steps[q];
+  return 0;
+}
+
+int agd_deblend_batch(int n_problems, int const *n_patches, int const *const *volumes,
+                      int const *const *n_dims, int const *const *const *window_shapes,
+                      int const *const *const *coords, int const *const *const *shapes,
+                      long int const *const *const *shottimes, int const *const *const *channels,
+                      enum AGDTraceType const *const *const *trace_types,
+                      int const *const *wavelet_lengths, int const *const *const *wavelet_idxs,
+                      AGD_TYPE const *const *const *wavelets, AGD_TYPE initial_factor,
+                      int n_its, AGD_TYPE *const *const *data) {
+  if (n_problems <= 0 || n_patches == nullptr || data == nullptr) {
+    std::fprintf(stderr, "ERROR: invalid batch arguments\nERROR in agd_deblend_batch\n");
+    return 1;
+  }
+  std::vector<AGD_TYPE *> all_data;
+  for (int q = 0; q < n_problems; ++q) {
+    const agd::ProblemArgs a =
+        batch_args(q, n_patches, volumes, n_dims, window_shapes, coords, shapes, shottimes,
+                   channels, trace_types, wavelet_lengths, wavelet_idxs, wavelets);
+    if (data[q] == nullptr || agd::check_deblend_inputs(a, initial_factor, n_its, data[q])) {
+      std::fprintf(stderr, "ERROR in problem %d of agd_deblend_batch\n", q);
+      return 1;
+    }
+    for (int p = 0; p < n_patches[q]; ++p) all_data.push_back(data[q][p]);
+  }
+  agd_gpu_problem *pb = nullptr;
+  if (agd_gpu_batch_create(n_problems, n_patches, volumes, n_dims, window_shapes, coords,
+                           shapes, shottimes, channels, trace_types, wavelet_lengths,
+                           wavelet_idxs, wavelets, &pb)) {
+    std::fprintf(stderr, "ERROR in agd_deblend_batch\n");
+    return 1;
+  }
+  const int rc = agd_gpu_solve(pb, initial_factor, n_its, 0, all_data.data());
   delete pb;
   return rc;
 }

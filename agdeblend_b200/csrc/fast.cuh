@@ -286,16 +286,19 @@ struct PlaneJob {
   Cx<R> *dst;        // forward: Z planes [L..]; adjoint: model planes (update)
   long src_plane;    // complex per input plane
   long dst_plane;    // complex per output plane
+  int pid;           // problem of the window
 };
 
 // One batch of planes for the persistent space kernels: `count` planes
-// starting at src (input planes) and dst (output planes).
+// starting at src (input planes) and dst (output planes), of the window of
+// problem `pid` (independent problems solved together keep their own step
+// size and threshold).
 template <typename R>
 struct PlaneBatch {
   const Cx<R> *src;
   Cx<R> *dst;
   int count;
-  int pad;
+  int pid;
 };
 
 template <typename R>
@@ -477,10 +480,13 @@ __global__ void __launch_bounds__(NT, MINB) space_fwd_fast(PlaneBatches<R> batch
 // copied into a third buffer while its FFTs run (shared memory: 2 NP padded
 // planes and NP dense planes).  STAGES = 1: one padded buffer; the epilogue
 // reads the model planes from global memory, and MINB blocks share an SM.
+// With step_dev (independent problems solved together) the step, the
+// threshold (lamb_dev) and the tracked maximum (max_out) are per problem,
+// indexed by the batch's pid.
 template <typename R, int D, int P0, int P1, int P2, int NT, int NP, int STAGES, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
-    space_adj_fast(PlaneBatches<R> batches, int epilogue, R step, R lamb_arg,
-                   const R *lamb_dev, R *max_out) {
+    space_adj_fast(PlaneBatches<R> batches, int epilogue, R step_arg, R lamb_arg,
+                   const R *step_dev, const R *lamb_dev, R *max_out) {
   static_assert(STAGES == 1 || STAGES == 2, "one or two stages");
   using C = Cx<R>;
   using S = PlaneShape<D, P0, P1, P2>;
@@ -498,9 +504,7 @@ __global__ void __launch_bounds__(NT, MINB)
                           bt.src + e);
     }
   };
-  // lambda from device memory when replayed from a CUDA graph
-  const R lamb = lamb_dev != nullptr ? *lamb_dev : lamb_arg;
-  const R lamb_sq = lamb * lamb;
+  const bool multi = step_dev != nullptr;
   R local_max = (R)0;
   const PlaneBatch<R> none{nullptr, nullptr, 0, 0};
   int b = blockIdx.x;
@@ -522,6 +526,10 @@ __global__ void __launch_bounds__(NT, MINB)
     const int np = cur.count;
     C *dst = cur.dst;
     const int n_store = np * S::dense_P;
+    // lambda from device memory when replayed from a CUDA graph
+    const R step = multi ? step_dev[cur.pid] : step_arg;
+    const R lamb = lamb_dev != nullptr ? lamb_dev[multi ? cur.pid : 0] : lamb_arg;
+    const R lamb_sq = lamb * lamb;
     if constexpr (STAGES == 2) {
       if (need_x) {
         for (int e = threadIdx.x; e < n_store; e += NT) cp_async<sizeof(C)>(xbuf + e, dst + e);
@@ -551,6 +559,12 @@ __global__ void __launch_bounds__(NT, MINB)
       }
     }
     __syncthreads();
+    if (multi && epilogue == kUpdateMax) {  // one maximum per problem
+      __shared__ R red_b[32];
+      const R m = block_max<R>(local_max, red_b);
+      if (threadIdx.x == 0) atomic_max_nonneg(max_out + cur.pid, m);
+      local_max = (R)0;
+    }
     if constexpr (STAGES == 1) {
       if (nxt.count > 0) issue(nxt, stage[0]);
       cp_async_commit();
@@ -558,7 +572,7 @@ __global__ void __launch_bounds__(NT, MINB)
     cur = nxt;
     nxt = after;
   }
-  if (epilogue == kUpdateMax) {
+  if (!multi && epilogue == kUpdateMax) {
     __shared__ R red[32];
     const R m = block_max<R>(local_max, red);
     if (threadIdx.x == 0) atomic_max_nonneg(max_out, m);

@@ -37,6 +37,7 @@ struct AxisJob {
   int n_out;  // elements per line written (first n_out of the FFT output)
   int fft;    // FftDesc index
   int last;   // 1: the window's final pass, which takes the launch's epilogue
+  int pid;    // problem of the window (per-problem step, threshold, maximum)
 };
 
 enum AxisEpilogue : int {
@@ -183,8 +184,8 @@ __global__ void __launch_bounds__(kThreads)
     axis_pass(const AxisJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
               const long *__restrict__ cta_line0, int lines_per_cta,
               const FftDesc *__restrict__ descs, const Cx<R> *__restrict__ tw,
-              int inverse, int epilogue, R step, R lamb_arg, const R *lamb_dev,
-              R *max_out) {
+              int inverse, int epilogue, R step_arg, R lamb_arg, const R *step_dev,
+              const R *lamb_dev, R *max_out) {
   using C = Cx<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const AxisJob<R> job = jobs[cta_job[blockIdx.x]];
@@ -224,8 +225,11 @@ __global__ void __launch_bounds__(kThreads)
   R local_max = (R)0;
   const int total_out = nl * job.n_out;
   // the threshold comes from device memory when the launch is replayed from
-  // a CUDA graph (one captured iteration, a different lambda each replay)
-  const R lamb = lamb_dev != nullptr ? *lamb_dev : lamb_arg;
+  // a CUDA graph (one captured iteration, a different lambda each replay);
+  // step_dev: independent problems solved together, per-problem scalars
+  const bool multi = step_dev != nullptr;
+  const R step = multi ? step_dev[job.pid] : step_arg;
+  const R lamb = lamb_dev != nullptr ? lamb_dev[multi ? job.pid : 0] : lamb_arg;
   const R lamb_sq = lamb * lamb;
   for (int idx = threadIdx.x; idx < total_out; idx += blockDim.x) {
     int i, e;
@@ -260,7 +264,7 @@ __global__ void __launch_bounds__(kThreads)
   if (epi == kUpdateMax) {
     __shared__ R red[32];
     const R m = block_max<R>(local_max, red);
-    if (threadIdx.x == 0) atomic_max_nonneg(max_out, m);
+    if (threadIdx.x == 0) atomic_max_nonneg(max_out + (multi ? job.pid : 0), m);
   }
 }
 
@@ -558,15 +562,15 @@ __global__ void record_sumsq(const R *__restrict__ x, long n, double *out) {
   if (threadIdx.x == 0) atomicAdd(out, s);
 }
 
-// Advances the threshold schedule on the device: out = table[*counter],
-// then ++*counter (one thread; captured in the per-iteration CUDA graph).
+// Advances the threshold schedule on the device: out[0..n) = row *counter
+// of table (n thresholds per iteration, one per problem solved together),
+// then ++*counter.  One block; captured in the per-iteration CUDA graph.
 template <typename R>
-__global__ void next_lambda(const R *__restrict__ table, int *counter, R *out) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    const int k = *counter;
-    *out = table[k];
-    *counter = k + 1;
-  }
+__global__ void next_lambda(const R *__restrict__ table, int *counter, R *out, int n) {
+  const int k = *counter;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) out[i] = table[(long)k * n + i];
+  __syncthreads();
+  if (threadIdx.x == 0) *counter = k + 1;
 }
 
 template <typename R>

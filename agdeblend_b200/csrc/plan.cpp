@@ -588,3 +588,66 @@ int build_plan(const ProblemArgs &a, Plan &plan) {
 }
 
 }  // namespace agd
+
+namespace agd {
+
+int build_batch_plan(const std::vector<ProblemArgs> &args, Plan &out) {
+  out = Plan{};
+  out.n_problems = (int)args.size();
+  // the wavelet stage runs on every window of a plan or on none
+  for (const ProblemArgs &a : args)
+    if ((a.wavelet_idxs != nullptr) != (args[0].wavelet_idxs != nullptr))
+      return fail("ERROR: the problems of a batch must all have wavelets or all have none\n");
+  for (size_t q = 0; q < args.size(); ++q) {
+    const ProblemArgs &a = args[q];
+    Plan sub;
+    if (build_plan(a, sub)) return 1;
+    const int patch_base = out.n_patches;
+    const long rec_base = out.record_size;
+    const long model_base = out.model_size;
+    const int spec_base = (int)out.spectra.size();
+    out.problem_rec_off.push_back(rec_base);
+    out.problem_rec_size.push_back(sub.record_size);
+    out.problem_model_off.push_back(model_base);
+    out.problem_model_size.push_back(sub.model_size);
+    out.n_patches += sub.n_patches;
+    auto append = [](auto &dst, const auto &src) { dst.insert(dst.end(), src.begin(), src.end()); };
+    append(out.volume, sub.volume);
+    append(out.n_space, sub.n_space);
+    append(out.shape, sub.shape);
+    append(out.n_traces, sub.n_traces);
+    append(out.n_times, sub.n_times);
+    append(out.n_fk, sub.n_fk);
+    append(out.conv, sub.conv);
+    append(out.lt, sub.lt);
+    append(out.intervals, sub.intervals);
+    append(out.wavelet_n, sub.wavelet_n);
+    append(out.spectra, sub.spectra);
+    for (const auto &m : sub.mute) out.mute.emplace_back(m.first + rec_base, m.second);
+    // blend coordinates of the patch traces at their raw shot times
+    for (int p = 0; p < sub.n_patches; ++p) {
+      std::vector<BlendCoord> c(sub.n_traces[p]);
+      for (int t = 0; t < sub.n_traces[p]; ++t) {
+        c[t] = sub.coord_of(a.shottimes[p][t], sub.n_times[p], a.channels[p][t],
+                            (int)a.trace_types[p][t]);
+        if (c[t].rec >= 0) c[t].rec += rec_base;
+      }
+      out.input_coord.push_back(std::move(c));
+    }
+    for (WindowPlan &W : sub.windows) {
+      W.patch += patch_base;
+      W.problem = (int)q;
+      W.model_off += model_base;
+      for (BlendCoord &b : W.blend)
+        if (b.rec >= 0) b.rec += rec_base;
+      for (int &s : W.wavelet_src)
+        if (s >= 0) s += spec_base;
+      out.windows.push_back(std::move(W));
+    }
+    out.record_size += sub.record_size;
+    out.model_size += sub.model_size;
+  }
+  return 0;
+}
+
+}  // namespace agd

@@ -36,6 +36,7 @@ struct BlendCoord {
 // One space window with its FK operator constants (src/fk.c:75-169).
 struct WindowPlan {
   int patch = 0;
+  int problem = 0;             // independent problem (batches of problems)
   int D = 0;                   // number of space dimensions
   int coords[kMaxSpaceDims] = {0};
   int L[kMaxSpaceDims] = {0};  // window length per space dim
@@ -85,6 +86,17 @@ struct Plan {
   std::vector<int> wavelet_n;                      // transform length
   std::vector<std::vector<std::complex<double>>> spectra;
 
+  // Independent problems planned together (build_batch_plan): each keeps
+  // its record range, model range, step size and threshold schedule.  A
+  // single agd_deblend problem has n_problems = 1 and empty tables.
+  int n_problems = 1;
+  std::vector<long> problem_rec_off, problem_rec_size;
+  std::vector<long> problem_model_off, problem_model_size;
+  // blend coordinates of every patch trace at its raw shot time (the
+  // pseudo-deblending input), when the channel tables above do not hold
+  // every problem
+  std::vector<std::vector<BlendCoord>> input_coord;
+
   int channel_index(int value, int trace_type) const;
   BlendCoord coord_of(long shottime, int n_times, int channel, int trace_type) const;
 };
@@ -111,6 +123,11 @@ int check_deblend_inputs(const ProblemArgs &a, real initial_factor, int n_its,
 
 // set_model + the wavelet spectra; returns 1 (after printing) on failure.
 int build_plan(const ProblemArgs &a, Plan &plan);
+
+// Plans independent problems one by one and concatenates them: patches,
+// windows, records and models follow one another in problem order, each
+// window tagged with its problem.  Returns 1 (after printing) on failure.
+int build_batch_plan(const std::vector<ProblemArgs> &args, Plan &plan);
 
 // Blend configuration of arbitrary trace sets (used by agd_blend and by
 // build_plan): set_blend_config, src/blend.c:629-691.

@@ -40,14 +40,16 @@ int agd_gpu_problem_create(int n_patches, int const *volumes, int const *n_dims,
 
 void agd_gpu_problem_destroy(agd_gpu_problem *problem);
 
-/* info (14 values): [0] windows, [1] model complex elements, [2] record
+/* info (17 values): [0] windows, [1] model complex elements, [2] record
  * samples, [3] window traces (all windows), [4] record segments, [5] mute
  * spans, [6] device bytes held, [7] blend contributions per forward,
- * [8] 1 if the shape-specialised kernels serve this problem, [9] 1 if the
- * prime-factor wavelet kernel serves it, [10] and [11] the space-kernel
- * candidates picked by the set-up timing for the forward and adjoint
- * (-1 without the shape-specialised kernels), [12] and [13] the number of
- * candidates. */
+ * [8] 1 if the shape-specialised kernels serve every window, 2 if they
+ * serve some, 0 if none, [9] 1 if the prime-factor wavelet kernel serves
+ * the problem, [10] and [11] the space-kernel candidates picked by the
+ * set-up timing for the forward and adjoint of the first window class (-1
+ * without shape-specialised kernels), [12] and [13] that class's number of
+ * candidates, [14] kernels launched per iteration, [15] window classes on
+ * the shape-specialised kernels, [16] windows on them. */
 int agd_gpu_problem_info(agd_gpu_problem const *problem, long int *info);
 
 /* Step size 0.5 / max blend fold (reference get_stepsize, src/model.c:1230-1312). */
@@ -86,11 +88,10 @@ int agd_gpu_time_iterations(agd_gpu_problem *problem, AGD_TYPE const *const *dat
 
 /* Benchmark hook: one ISTA iteration on the current device state with CUDA
  * events between its launch groups (call after agd_gpu_time_iterations).
- * ms[0] forward space passes, [1] time c2r + overlap-add, [2] wavelet
- * forward, [3] blend gather + residual, [4] adjoint time axis (with its
- * record gather and wavelet), [5] adjoint space passes with the update,
- * [6..9] forward passes by index, [10..13] adjoint passes by index,
- * [14] number of space passes. */
+ * ms[0] forward space passes (all windows), [1] time c2r + overlap-add,
+ * [2] wavelet forward, [3] blend gather + residual, [4] adjoint time axis
+ * (with its record gather and wavelet), [5] adjoint space passes with the
+ * update; [6] = [0], [10] = [5], [14] = 1 (ms has 16 entries). */
 int agd_gpu_profile_iteration(agd_gpu_problem *problem, AGD_TYPE lamb, double *ms);
 
 /* Host planning only (no device use): writes the plan's size summary
@@ -105,6 +106,43 @@ int agd_plan_export(int n_patches, int const *volumes, int const *n_dims,
                     int const *wavelet_lengths, int const *const *wavelet_idxs,
                     AGD_TYPE const *const *wavelets, long int *info, int *win,
                     long int *blend);
+
+/* Independent problems solved together (no counterpart in the reference,
+ * whose agd_deblend solves one problem per call).  Each argument is an
+ * array over the n_problems problems of the corresponding agd_deblend
+ * argument (n_patches[q] patches for problem q; the three wavelet arrays may
+ * be NULL, or hold NULL for problems without wavelets).  initial_factor and
+ * n_its are shared.  Every problem keeps its own step size, initial
+ * threshold and threshold schedule, so data[q] ends as agd_deblend would
+ * leave it for problem q alone; all problems run in the same kernel
+ * launches, one captured CUDA graph per iteration.  No residual printing. */
+int agd_deblend_batch(int n_problems, int const *n_patches, int const *const *volumes,
+                      int const *const *n_dims, int const *const *const *window_shapes,
+                      int const *const *const *coords, int const *const *const *shapes,
+                      long int const *const *const *shottimes, int const *const *const *channels,
+                      enum AGDTraceType const *const *const *trace_types,
+                      int const *const *wavelet_lengths, int const *const *const *wavelet_idxs,
+                      AGD_TYPE const *const *const *wavelets, AGD_TYPE initial_factor,
+                      int n_its, AGD_TYPE *const *const *data);
+
+/* The persistent handle of a batch (arguments as agd_deblend_batch up to
+ * the wavelets).  The handle's patches are all problems' patches in
+ * problem order: agd_gpu_solve, agd_gpu_blend_input, agd_gpu_set_output and
+ * agd_gpu_time_iterations take data for all of them; the model and record
+ * of agd_gpu_forward / agd_gpu_adjoint are the problems' models and records
+ * one after another. */
+int agd_gpu_batch_create(int n_problems, int const *n_patches, int const *const *volumes,
+                         int const *const *n_dims, int const *const *const *window_shapes,
+                         int const *const *const *coords, int const *const *const *shapes,
+                         long int const *const *const *shottimes,
+                         int const *const *const *channels,
+                         enum AGDTraceType const *const *const *trace_types,
+                         int const *const *wavelet_lengths, int const *const *const *wavelet_idxs,
+                         AGD_TYPE const *const *const *wavelets, agd_gpu_problem **problem);
+
+/* Step size of every problem of the handle (one value for a single
+ * problem). */
+int agd_gpu_problem_steps(agd_gpu_problem const *problem, AGD_TYPE *steps);
 
 /* agd_blend for callers that cannot allocate device memory (code running
  * inside a CUDA stream capture, hosts whose pool owns all device memory,
