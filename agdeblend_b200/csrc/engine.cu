@@ -215,26 +215,33 @@ class Engine {
     int nt, np, stages;
     size_t smem;
   };
+  // windows of one padded space shape on the fast space kernels
   struct FastClass {
     std::vector<int> win;  // windows of the class
     std::vector<FwdVariant> fwd_vars;
     std::vector<AdjVariant> adj_vars;
     int fwd_pick = 0, adj_pick = 0;
-    TimeFwdFn tm_fwd = nullptr;
-    TimeAdjFn tm_adj = nullptr;
     PlaneLaunch pl_fwd, pl_adj, pl_adj_plain;
     std::vector<PlaneJob<R>> plain_jobs;  // adjoint jobs without the update
     std::vector<long> planes;             // (t, f) planes per window
-    TimeLaunch tf, ta;
     const FwdVariant &fv() const { return fwd_vars[fwd_pick]; }
     const AdjVariant &av() const { return adj_vars[adj_pick]; }
   };
+  // windows of one padded time length on the fast time kernels (whatever
+  // kernels serve their space axes)
+  struct TimeGroup {
+    std::vector<int> win;
+    TimeFwdFn tm_fwd = nullptr;
+    TimeAdjFn tm_adj = nullptr;
+    TimeLaunch tf, ta;
+  };
   std::vector<std::unique_ptr<FastClass>> classes;
-  std::vector<int> win_class;  // per window: its class, or -1 (generic kernels)
-  int n_generic = 0;           // windows on the generic kernels
-  int max_d_generic = 0;       // space dimensions of the generic windows
+  std::vector<std::unique_ptr<TimeGroup>> tgroups;
+  std::vector<int> win_class;   // per window: its space class, or -1 (generic)
+  std::vector<int> win_tgroup;  // per window: its time group, or -1 (generic)
+  int n_generic = 0;            // windows on the generic space kernels
+  int max_d_generic = 0;        // space dimensions of those windows
   int n_sm = 148;
-  DevArray<TimeJob<R>> time_jobs_fast;
   GatherLaunch g_fwd, g_input;
   std::vector<long> trace_off;   // per window, in reals
   std::vector<long> patch_off;   // per patch, in reals
@@ -441,7 +448,7 @@ class Engine {
       throw DeviceError("time window or trace too long for shared memory");
     std::vector<int> cj, ct;
     for (size_t w = 0; w < plan.windows.size(); ++w) {
-      if (generic_only && win_class[w] >= 0) continue;
+      if (generic_only && win_tgroup[w] >= 0) continue;
       for (int t = 0; t < plan.windows[w].n_traces; t += nb) {
         cj.push_back((int)w);
         ct.push_back(t);
@@ -546,45 +553,68 @@ class Engine {
   }
 
   // time-axis kernels for the window's padded time length
-  static bool time_case(const WindowPlan &W, FastClass &c) {
+  static bool time_case(const WindowPlan &W, TimeGroup &g) {
     if (W.Pt == 320) {
-      c.tm_fwd = time_fwd_fast<R, 16, 10, kTimeNB>;
-      c.tm_adj = time_adj_fast<R, 16, 10, kTimeNB>;
+      g.tm_fwd = time_fwd_fast<R, 16, 10, kTimeNB>;
+      g.tm_adj = time_adj_fast<R, 16, 10, kTimeNB>;
     } else if (W.Pt == 160) {
-      c.tm_fwd = time_fwd_fast<R, 8, 10, kTimeNB>;
-      c.tm_adj = time_adj_fast<R, 8, 10, kTimeNB>;
+      g.tm_fwd = time_fwd_fast<R, 8, 10, kTimeNB>;
+      g.tm_adj = time_adj_fast<R, 8, 10, kTimeNB>;
     } else {
       return false;
     }
     return true;
   }
 
-  // the fast kernels assume L = 4P/5 in space and Lt = 2h = 4Pt/5 in time
-  static bool fast_eligible(const WindowPlan &W) {
-    if (W.Lt % 2 != 0 || W.Lt * 5 != W.Pt * 4) return false;
+  // the fast space kernels assume L = 4P/5 on every space axis, the fast
+  // time kernels Lt = 2h = 4Pt/5
+  static bool space_eligible(const WindowPlan &W) {
     for (int d = 0; d < W.D; ++d)
       if (W.L[d] * 5 != W.P[d] * 4) return false;
     return true;
   }
+  static bool time_eligible(const WindowPlan &W) {
+    return W.Lt % 2 == 0 && W.Lt * 5 == W.Pt * 4;
+  }
 
-  // Groups the windows into fast classes (AGD_GPU_GENERIC=1: none).
+  // Groups the windows into fast space classes and fast time groups
+  // (AGD_GPU_GENERIC=1: none).
   void pick_classes() {
     const int nw = (int)plan.windows.size();
     win_class.assign(nw, -1);
+    win_tgroup.assign(nw, -1);
     classes.clear();
+    tgroups.clear();
     const char *env = std::getenv("AGD_GPU_GENERIC");
     const bool generic_only = env != nullptr && env[0] == '1';
     std::map<std::vector<int>, int> by_key;  // -1: no instantiation
+    std::map<int, int> by_pt;
     for (int w = 0; w < nw && !generic_only; ++w) {
       const WindowPlan &W = plan.windows[w];
-      if (!fast_eligible(W)) continue;
-      std::vector<int> key{W.D, W.Pt};
+      if (time_eligible(W)) {
+        auto it = by_pt.find(W.Pt);
+        int k;
+        if (it == by_pt.end()) {
+          std::unique_ptr<TimeGroup> g(new TimeGroup());
+          k = time_case(W, *g) ? (int)tgroups.size() : -1;
+          if (k >= 0) tgroups.push_back(std::move(g));
+          by_pt[W.Pt] = k;
+        } else {
+          k = it->second;
+        }
+        if (k >= 0) {
+          win_tgroup[w] = k;
+          tgroups[k]->win.push_back(w);
+        }
+      }
+      if (!space_eligible(W)) continue;
+      std::vector<int> key{W.D};
       for (int d = 0; d < W.D; ++d) key.push_back(W.P[d]);
       auto it = by_key.find(key);
       int k;
       if (it == by_key.end()) {
         std::unique_ptr<FastClass> c(new FastClass());
-        if (space_cases(W, *c) && time_case(W, *c)) {
+        if (space_cases(W, *c)) {
           k = (int)classes.size();
           classes.push_back(std::move(c));
         } else {
@@ -607,9 +637,10 @@ class Engine {
       }
   }
 
-  // Times every candidate of a class (one warm-up launch, then two timed ones
-  // with CUDA events on the engine's stream, forward X -> S0 and adjoint
-  // S0 -> X with the update epilogue) and keeps the fastest.  Choices are
+  // Times every candidate of a class (three rounds over the candidates, each
+  // one warm-up launch and two timed ones with CUDA events on the engine's
+  // stream; forward X -> S0, adjoint S0 -> X with the update epilogue) and
+  // keeps the fastest.  Choices are
   // remembered per shape, precision, problem size class and device, so later
   // problems of the same kind skip the timing.  AGD_GPU_SPACE_VARIANT="f,a"
   // forces the candidates (tests).
@@ -662,37 +693,41 @@ class Engine {
       CK(cudaEventElapsedTime(&ms, e0, e1));
       return ms;
     };
-    float best = 1e30f;
-    for (size_t v = 0; v < c.fwd_vars.size(); ++v) {
-      const FwdVariant &fv = c.fwd_vars[v];
-      if (fv.smem > (size_t)smem_max) continue;
-      PlaneLaunch L;
-      make_plane_launch(L, jf, c.planes, fv.nt, fv.np, fv.smem, fv.fn);
-      const float ms = timed([&] {
-        fv.fn<<<L.grid, L.nt, L.smem, stream>>>(L.batches());
-        CK(cudaGetLastError());
-      });
-      if (ms < best) {
-        best = ms;
-        c.fwd_pick = (int)v;
+    // three rounds over all candidates, the best time of each counts
+    const size_t nf = c.fwd_vars.size(), na = c.adj_vars.size();
+    std::vector<PlaneLaunch> lf(nf), la(na);
+    std::vector<float> tf(nf, 1e30f), ta(na, 1e30f);
+    for (size_t v = 0; v < nf; ++v)
+      if (c.fwd_vars[v].smem <= (size_t)smem_max)
+        make_plane_launch(lf[v], jf, c.planes, c.fwd_vars[v].nt, c.fwd_vars[v].np,
+                          c.fwd_vars[v].smem, c.fwd_vars[v].fn);
+    for (size_t v = 0; v < na; ++v)
+      if (c.adj_vars[v].smem <= (size_t)smem_max)
+        make_plane_launch(la[v], ja, c.planes, c.adj_vars[v].nt, c.adj_vars[v].np,
+                          c.adj_vars[v].smem, c.adj_vars[v].fn);
+    for (int round = 0; round < 3; ++round) {
+      for (size_t v = 0; v < nf; ++v) {
+        const PlaneLaunch &L = lf[v];
+        if (L.n_batch == 0) continue;
+        const SpaceFwdFn fn = c.fwd_vars[v].fn;
+        tf[v] = std::min(tf[v], timed([&] {
+          fn<<<L.grid, L.nt, L.smem, stream>>>(L.batches());
+          CK(cudaGetLastError());
+        }));
+      }
+      for (size_t v = 0; v < na; ++v) {
+        const PlaneLaunch &L = la[v];
+        if (L.n_batch == 0) continue;
+        const SpaceAdjFn fn = c.adj_vars[v].fn;
+        ta[v] = std::min(ta[v], timed([&] {
+          fn<<<L.grid, L.nt, L.smem, stream>>>(L.batches(), kUpdateThreshold, (R)0, (R)0,
+                                               nullptr, nullptr, scalar.get());
+          CK(cudaGetLastError());
+        }));
       }
     }
-    best = 1e30f;
-    for (size_t v = 0; v < c.adj_vars.size(); ++v) {
-      const AdjVariant &av = c.adj_vars[v];
-      if (av.smem > (size_t)smem_max) continue;
-      PlaneLaunch L;
-      make_plane_launch(L, ja, c.planes, av.nt, av.np, av.smem, av.fn);
-      const float ms = timed([&] {
-        av.fn<<<L.grid, L.nt, L.smem, stream>>>(L.batches(), kUpdateThreshold, (R)0, (R)0,
-                                                 nullptr, nullptr, scalar.get());
-        CK(cudaGetLastError());
-      });
-      if (ms < best) {
-        best = ms;
-        c.adj_pick = (int)v;
-      }
-    }
+    c.fwd_pick = (int)(std::min_element(tf.begin(), tf.end()) - tf.begin());
+    c.adj_pick = (int)(std::min_element(ta.begin(), ta.end()) - ta.begin());
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     std::lock_guard<std::mutex> g(mu);
@@ -728,8 +763,9 @@ class Engine {
   void opt_in_classes() {
     const int limit = optin_smem();
     int dyn = smem_max;
+    for (const auto &gp : tgroups)
+      dyn = std::min({dyn, opt_in(gp->tm_fwd, limit), opt_in(gp->tm_adj, limit)});
     for (const auto &cp : classes) {
-      dyn = std::min({dyn, opt_in(cp->tm_fwd, limit), opt_in(cp->tm_adj, limit)});
       for (const FwdVariant &v : cp->fwd_vars) dyn = std::min(dyn, opt_in(v.fn, limit));
       for (const AdjVariant &v : cp->adj_vars) dyn = std::min(dyn, opt_in(v.fn, limit));
     }
@@ -765,12 +801,16 @@ class Engine {
     make_plane_launch(c.pl_fwd, jf, c.planes, c.fv().nt, c.fv().np, c.fv().smem, c.fv().fn);
     make_plane_launch(c.pl_adj, ja, c.planes, c.av().nt, c.av().np, c.av().smem, c.av().fn);
     c.plain_jobs = ja;
+  }
+
+  void build_time_group(TimeGroup &g) {
+    const WindowPlan &W0 = plan.windows[g.win[0]];
     const int h = W0.h;
     const int LS = W0.Pt / 2 + 1;
     const size_t per_fwd = 2 * (size_t)LS * sizeof(C) + (size_t)h * sizeof(R);
     const size_t per_adj = (size_t)LS * sizeof(C) + 2 * (size_t)(2 * h) * sizeof(R);
-    make_fixed_time_launch(c.tf, per_fwd * kTimeNB, c.win);
-    make_fixed_time_launch(c.ta, per_adj * kTimeNB, c.win);
+    make_fixed_time_launch(g.tf, per_fwd * kTimeNB, g.win);
+    make_fixed_time_launch(g.ta, per_adj * kTimeNB, g.win);
   }
 
   void make_fixed_time_launch(TimeLaunch &L, size_t smem, const std::vector<int> &wins) {
@@ -894,11 +934,12 @@ class Engine {
     }
     C *Sb[2] = {S0.get(), S1.get()};
 
-    // ---- time-axis jobs
+    // ---- time-axis jobs (the space-axis intermediate: S0 for the fast
+    // space kernels, the generic passes' last buffer otherwise)
     for (int w = 0; w < nw; ++w) {
       const WindowPlan &W = plan.windows[w];
       TimeJob<R> &j = tj[w];
-      j.z = Sb[(W.D - 1) & 1] + W.model_off;
+      j.z = (win_class[w] >= 0 ? S0.get() : Sb[(W.D - 1) & 1]) + W.model_off;
       j.y = Y.get() + trace_off[w];
       j.space_scale = space_scale.get() + wt_base[w];
       j.time_taper = time_taper.get() + ttaper_off[w];
@@ -922,14 +963,11 @@ class Engine {
       v.fft = wavelets ? fft.get(W.C) : 0;
     }
     time_jobs.upload(tj, stream);
-    if (!classes.empty()) {
-      std::vector<TimeJob<R>> tjf = tj;
-      for (int w = 0; w < nw; ++w)
-        if (win_class[w] >= 0) tjf[w].z = S0.get() + plan.windows[w].model_off;
-      time_jobs_fast.upload(tjf, stream);
+    if (!classes.empty() || !tgroups.empty()) {
       opt_in_classes();
       upload_twiddles();
       for (auto &c : classes) build_class(*c);
+      for (auto &g : tgroups) build_time_group(*g);
     }
     const size_t per_trace_time = 2 * (size_t)Pt_max * sizeof(C) + (size_t)C_max * sizeof(R);
     make_time_launch(time_fwd, per_trace_time, 16, true);
@@ -1139,14 +1177,14 @@ class Engine {
     CK(cudaGetLastError());
   }
 
-  // time c2r + taper + overlap-add of every window (fast classes, then the
-  // generic windows)
+  // time c2r + taper + overlap-add of every window (fast time groups, then
+  // the generic windows)
   void launch_time_fwd() {
-    for (const auto &cp : classes) {
-      const FastClass &c = *cp;
-      if (!c.tf.n_cta) continue;
-      c.tm_fwd<<<c.tf.n_cta, kThreads, c.tf.smem, stream>>>(
-          time_jobs_fast.get(), c.tf.cta_job.get(), c.tf.cta_trace0.get());
+    for (const auto &gp : tgroups) {
+      const TimeGroup &g = *gp;
+      if (!g.tf.n_cta) continue;
+      g.tm_fwd<<<g.tf.n_cta, kThreads, g.tf.smem, stream>>>(time_jobs.get(), g.tf.cta_job.get(),
+                                                            g.tf.cta_trace0.get());
       CK(cudaGetLastError());
     }
     if (time_fwd.n_cta) {
@@ -1160,11 +1198,11 @@ class Engine {
   // blend adjoint gather + taper + time r2c of every window, from the record
   // (from_record) or from the window traces (after the wavelet correlation)
   void launch_time_adj(const R *record, int from_record) {
-    for (const auto &cp : classes) {
-      const FastClass &c = *cp;
-      if (!c.ta.n_cta) continue;
-      c.tm_adj<<<c.ta.n_cta, kThreads, c.ta.smem, stream>>>(
-          time_jobs_fast.get(), c.ta.cta_job.get(), c.ta.cta_trace0.get(), record, from_record);
+    for (const auto &gp : tgroups) {
+      const TimeGroup &g = *gp;
+      if (!g.ta.n_cta) continue;
+      g.tm_adj<<<g.ta.n_cta, kThreads, g.ta.smem, stream>>>(
+          time_jobs.get(), g.ta.cta_job.get(), g.ta.cta_trace0.get(), record, from_record);
       CK(cudaGetLastError());
     }
     if (time_adj.n_cta) {
@@ -1241,7 +1279,7 @@ class Engine {
   // kernels launched by one ISTA iteration (iteration_body)
   int kernels_per_iteration() const {
     int n = 2 * (int)classes.size();  // space passes, forward and adjoint
-    for (const auto &cp : classes) n += (cp->tf.n_cta ? 1 : 0) + (cp->ta.n_cta ? 1 : 0);
+    for (const auto &gp : tgroups) n += (gp->tf.n_cta ? 1 : 0) + (gp->ta.n_cta ? 1 : 0);
     n += (int)fwd.size() + (int)adj_update.size();
     n += (time_fwd.n_cta ? 1 : 0) + (time_adj.n_cta ? 1 : 0);
     n += (g_fwd.n_chunk ? 1 : 0) + 1;  // residual gather, threshold schedule

@@ -169,12 +169,15 @@ __device__ Cx<R> *block_fft(Cx<R> *a, Cx<R> *b, int nl, const FftDesc &d,
         out[base + 3 * ns] = csub(a2, b2);
       } else {
         // direct R-point DFT with the twiddle folded in:
-        // X_q = sum_r in[j + r m] W_n^{r (k tws + q m)}
+        // X_q = sum_r in[j + r m] W_n^{r (k tws + q m)}; the exponent
+        // r e mod n advances by e < n per term
         for (int q = 0; q < radix; ++q) {
-          const long e = tk + (long)q * m;
+          const int e = (int)(tk + (long)q * m);
           C acc = in[j];
+          int ti = 0;
           for (int r = 1; r < radix; ++r) {
-            const long ti = ((long)r * e) % n;
+            ti += e;
+            if (ti >= n) ti -= n;
             acc = cadd(acc, cmul(in[j + r * m], twiddle(tw, ti, inverse)));
           }
           out[base + q * ns] = acc;

@@ -8,7 +8,11 @@ Workloads (synthetic, seeded, agdeblend_b200.synthetic):
       one 256-sample 8-80 Hz sweep wavelet (trace length 2431), windows
       (16, 16, 16, 256), n_its 150;
   *_small  reduced versions of both (still larger than L2) for multi-pass
-      ncu captures.
+      ncu captures;
+  uneven_gathers  96 independent 2-D receiver gathers (shots U{100..400},
+      time U{512..2048}, windows from {(16,128), (32,256), (64,256)}), n_its
+      100, solved together in one set of launches per iteration; compared
+      with the same gathers solved one after another (per-gather loop).
 
 One step = one ISTA iteration (forward operator, residual, adjoint, update,
 soft threshold) over the whole survey.
@@ -63,10 +67,16 @@ WORKLOADS = {
                            "4-D vibroseis survey with sweep wavelet, quarter size"),
 }
 SEEDS = {"two_volume_3d": 1001, "vibroseis_4d": 1002}
+# batches of independent problems: name -> (number of gathers, label)
+BATCHES = {"uneven_gathers": (96, "96 uneven 2-D gathers solved together")}
+
+
+def metric_label(name):
+    return WORKLOADS[name][2] if name in WORKLOADS else BATCHES[name][1]
 
 
 def metric_of(name):
-    return f"ISTA iterations/s (plain FP32 deblending, {WORKLOADS[name][2]})"
+    return f"ISTA iterations/s (plain FP32 deblending, {metric_label(name)})"
 
 
 def workload(name="two_volume_3d", seed_offset=0):
@@ -261,15 +271,24 @@ def barrier(world):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    sv = workload(args.workload)
     steps = max(1, args.steps)
-    res = cpu_reference_rate(sv, steps)
-    if res is None:
-        res = cpu_port_rate(sv, max(1, min(steps, 3)))
-    line = {"impl": "reference", "metric": metric_of(args.workload), "value": res["value"], "unit": UNIT,
-            "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+    if args.workload in BATCHES:
+        gathers = batch_workload(args.workload)
+        config = batch_config(gathers, args.workload)
+        res = cpu_batch_rate(gathers, 1)
+        if res is None:
+            res = {"value": float("nan"), "cores": 0, "kind": "port",
+                   "sample": "reference build absent"}
+    else:
+        sv = workload(args.workload)
+        config = config_of(sv, args.workload)
+        res = cpu_reference_rate(sv, steps)
+        if res is None:
+            res = cpu_port_rate(sv, max(1, min(steps, 3)))
+    line = {"impl": "reference", "metric": metric_of(args.workload), "value": res["value"],
+            "unit": UNIT, "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": config_of(sv, args.workload),
+            "data": "synthetic", "config": config,
             "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": res["cores"],
                              "kind": res["kind"], "sample": res["sample"]},
             "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -369,10 +388,10 @@ def run_gpu(args, rank, world, local):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference_rate(sv, args.cpu_its) or cpu_port_rate(sv, 1)
     if rank == 0:
-        # per iteration: space passes both ways, time kernels both ways, the
-        # blend gather, the threshold-schedule step, wavelet kernels
-        per_it = 2 * nf + 4 + ((2 if wav_fast else 3) if wav else 0)
-        launches = args.steps * per_it
+        # kernels per iteration as the library counts them (space and time
+        # kernels both ways per window class, generic passes, the blend
+        # gather, the threshold-schedule step, wavelet kernels)
+        launches = args.steps * int(info[14])
         line = {"metric": metric_of(args.workload), "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_iter,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -389,6 +408,130 @@ def run_gpu(args, rank, world, local):
     prob.close()
 
 
+def batch_workload(name, seed_offset=0):
+    from agdeblend_b200 import synthetic as S
+
+    n, _ = BATCHES[name]
+    return S.uneven_gathers(n, base_seed=3000 + 1000 * seed_offset)
+
+
+def batch_config(gathers, name):
+    wins = sorted({tuple(g.window_shapes[0]) for g in gathers})
+    return {"workload": f"{name}: {len(gathers)} 2-D gathers, shots U{{100..400}}, time "
+                        f"U{{512..2048}}, windows {wins}, f32",
+            "n_its": gathers[0].n_its, "initial_factor": 1.0, "gathers": len(gathers),
+            "l2": "inputs larger than L2"}
+
+
+def cpu_batch_rate(gathers, its: int):
+    """Reference CPU path over the gathers: agd_deblend n_its = 1 and 1 + its
+    per gather; one batch iteration = one iteration of every gather."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from agdeblend_b200.capi import DeblendArgs
+
+    import ref_bind
+
+    if not ref_bind.available("libagdeblend_ref.so"):
+        return None
+    total = 0.0
+    for g in gathers:
+        times = []
+        for n in (1, 1 + its):
+            args = DeblendArgs(g.volumes, g.n_dims, g.window_shapes, g.coords, g.shapes,
+                               g.shottimes, g.channels, g.trace_types, g.data, dtype=np.float32)
+            t0 = time.perf_counter()
+            if ref_bind.ref_deblend(args, 1.0, n, 0):
+                raise RuntimeError("reference agd_deblend failed")
+            times.append(time.perf_counter() - t0)
+        total += max(times[1] - times[0], 1e-9)
+    return {"value": its / total, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+            "sample": f"agd_deblend n_its=1 vs 1+{its} on each of the {len(gathers)} gathers "
+                      f"(sum of differences {total:.1f} s), OpenMP over windows"}
+
+
+def run_gpu_batch(args, rank, world, local):
+    import torch
+
+    import agdeblend_b200 as A
+
+    gathers = batch_workload(args.workload, seed_offset=rank)
+    torch.cuda.set_device(local)
+    n_its = gathers[0].n_its
+    data = [d for g in gathers for d in g.data]
+    prob = A.Problem.from_batch(gathers)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t = prob.time_iterations(data, 1.0, n_its, args.warmup, args.steps)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(world)
+    ms = barrier_max(world, float(t[0]))
+    value = world * args.steps / (ms / 1e3)
+    prof = prob.profile_iteration(1e-3)
+    info = prob.info
+    # the same gathers one after another (one problem handle each, the same
+    # timed iterations): the per-gather launch loop
+    loop_ms = 0.0
+    for g in gathers:
+        p1 = A.Problem.from_survey(g)
+        loop_ms += float(p1.time_iterations(g.data, 1.0, n_its, args.warmup, args.steps)[0])
+        p1.close()
+    loop_ms = barrier_max(world, loop_ms)
+    e2e_s = float("nan")
+    if not args.no_e2e:
+        kw = [dict(volumes=g.volumes, window_shapes=g.window_shapes, coords=g.coords,
+                   shottimes=g.shottimes, channels=g.channels, trace_types=g.trace_types,
+                   data=g.data) for g in gathers]
+        A.deblend_batch(kw, 1.0, 2)
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        A.deblend_batch(kw, 1.0, n_its)
+        torch.cuda.synchronize()
+        e2e_s = barrier_max(world, time.perf_counter() - t0)
+    M, Rn = int(info[1]), int(info[2])
+    peak, peak_kind = hbm_peak()
+    phases = {"space_fwd": (prof[0], 8.0 * M), "time_fwd": (prof[1], 0.0),
+              "blend_gather": (prof[3], 8.0 * Rn), "time_adj": (prof[4], 4.0 * Rn),
+              "space_adj": (prof[5], 16.0 * M)}
+    dom = max(phases, key=lambda k: phases[k][0])
+    dom_ms, dom_bytes = phases[dom]
+    iter_bytes = 3 * 8.0 * M + 4 * 4.0 * Rn
+    ms_iter = ms / args.steps
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "algorithmic_bytes": dom_bytes,
+                "peak_source": peak_kind, "phase_ms": {k: v[0] for k, v in phases.items()},
+                "iteration_algorithmic_GB": iter_bytes / 1e9,
+                "iteration_achieved_GBs": iter_bytes / (ms_iter / 1e3) / 1e9,
+                "iteration_frac": iter_bytes / (ms_iter / 1e3) / 1e9 / peak}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_batch_rate(gathers, 1)
+    if rank == 0:
+        data_bytes = sum(d.nbytes for d in data)
+        line = {"metric": metric_of(args.workload), "value": value, "unit": UNIT,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms_iter, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": batch_config(gathers, args.workload),
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                "clocks": clk,
+                "per_gather_loop": {"value": world * args.steps / (loop_ms / 1e3), "unit": UNIT,
+                                    "ms_per_step": loop_ms / args.steps},
+                "e2e": {"value": world * n_its / e2e_s, "unit": UNIT,
+                        "h2d_bytes_per_step": data_bytes / n_its,
+                        "d2h_bytes_per_step": data_bytes / n_its, "call_s": e2e_s,
+                        "n_its": n_its},
+                "gpu_launches": args.steps * int(info[14]), "roofline": roofline,
+                "cpu_baseline": cpu, "window_classes_fast": int(info[15]),
+                "windows_fast": int(info[16]), "windows": int(info[0])}
+        print(json.dumps(line), flush=True)
+    prob.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -398,7 +541,8 @@ def main():
     ap.add_argument("--cpu-its", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="two_volume_3d", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="two_volume_3d",
+                    choices=sorted(WORKLOADS) + sorted(BATCHES))
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -407,7 +551,10 @@ def main():
         return
     rank, world, local = dist_setup(args.gpus)
     try:
-        run_gpu(args, rank, world, local)
+        if args.workload in BATCHES:
+            run_gpu_batch(args, rank, world, local)
+        else:
+            run_gpu(args, rank, world, local)
     finally:
         if world > 1:
             import torch.distributed as dist
