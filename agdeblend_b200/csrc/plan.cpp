@@ -1,10 +1,12 @@
 // Host planning for the deblending path.  See plan.hpp.
 #include "plan.hpp"
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <set>
 
 namespace agd {
 
@@ -80,36 +82,85 @@ bool adjacent(const Interval &a, const Interval &b) {
   return a.start == b.stop || a.stop == b.start;
 }
 
-// Merge one trace span into a channel's interval list.  The scan order is
-// the reference's (src/blend.c:113-151): the first overlapping-or-adjacent
-// entry absorbs the new span, then further entries that touch the *new*
-// span (not the grown entry) are absorbed and removed, resuming one past the
-// removed position.
-void add_interval(std::vector<Interval> &ivs, const Interval &nw) {
-  auto find = [&](size_t from) -> long {
-    for (size_t i = from; i < ivs.size(); ++i)
-      if (overlaps(nw, ivs[i]) || adjacent(nw, ivs[i])) return (long)i;
-    return -1;
-  };
-  long const first = find(0);
-  if (first < 0) {
-    ivs.push_back(nw);
-    return;
+// A channel's interval list under the reference's merge rule
+// (src/blend.c:113-151): the first entry, in list order, that overlaps or
+// touches the new span absorbs it; then, scanning on in list order, entries
+// that touch the *new* span (not the grown entry) are absorbed and removed,
+// and the scan resumes one position past the removed entry - so the entry
+// that moves into the freed position is skipped.
+//
+// Entries are numbered in creation order; as new entries are appended and
+// removals keep the order of the others, list order is number order.  A
+// start-sorted index finds the entries touching a span (starts up to the
+// span's end, back to the longest entry's length before its start), and the
+// set of live numbers gives each removed entry's successor, so one merge
+// costs O(k log n) for k candidates instead of a scan of the whole list.
+class IntervalList {
+ public:
+  void add(const Interval &nw) {
+    std::vector<int> touch;
+    auto it = by_start_.upper_bound(std::make_pair(nw.stop, INT_MAX));
+    while (it != by_start_.begin()) {
+      --it;
+      if (it->first + max_len_ < nw.start) break;
+      if (iv_[it->second].stop >= nw.start) touch.push_back(it->second);
+    }
+    if (touch.empty()) {
+      insert(nw);
+      return;
+    }
+    std::sort(touch.begin(), touch.end());
+    const int first = touch[0];
+    Interval g = iv_[first];
+    if (nw.start < g.start) g.start = nw.start;
+    if (nw.stop > g.stop) g.stop = nw.stop;
+    int cursor = first;
+    size_t k = 1;
+    for (;;) {
+      while (k < touch.size() && touch[k] <= cursor) ++k;
+      if (k == touch.size()) break;
+      const int e = touch[k++];
+      if (iv_[e].start < g.start) g.start = iv_[e].start;
+      if (iv_[e].stop > g.stop) g.stop = iv_[e].stop;
+      erase(e);
+      auto s = live_.upper_bound(e);
+      if (s == live_.end()) break;
+      cursor = *s;  // moved into the freed position: not examined
+    }
+    replace(first, g);
   }
-  Interval &f = ivs[first];
-  if (nw.start < f.start) f.start = nw.start;
-  if (nw.stop > f.stop) f.stop = nw.stop;
-  size_t from = (size_t)first + 1;
-  for (;;) {
-    long const i = find(from);
-    if (i < 0) break;
-    Interval &g = ivs[first];
-    if (ivs[i].start < g.start) g.start = ivs[i].start;
-    if (ivs[i].stop > g.stop) g.stop = ivs[i].stop;
-    ivs.erase(ivs.begin() + i);
-    from = (size_t)i + 1;
+
+  std::vector<Interval> list() const {
+    std::vector<Interval> out;
+    out.reserve(live_.size());
+    for (int id : live_) out.push_back(iv_[id]);
+    return out;
   }
-}
+
+ private:
+  void insert(const Interval &v) {
+    const int id = (int)iv_.size();
+    iv_.push_back(v);
+    live_.insert(id);
+    by_start_.insert(std::make_pair(v.start, id));
+    max_len_ = std::max(max_len_, v.stop - v.start);
+  }
+  void erase(int id) {
+    live_.erase(id);
+    by_start_.erase(std::make_pair(iv_[id].start, id));
+  }
+  void replace(int id, const Interval &v) {
+    by_start_.erase(std::make_pair(iv_[id].start, id));
+    iv_[id] = v;
+    by_start_.insert(std::make_pair(v.start, id));
+    max_len_ = std::max(max_len_, v.stop - v.start);
+  }
+
+  std::vector<Interval> iv_;                 // by number
+  std::set<int> live_;                       // numbers in the list
+  std::set<std::pair<long, int>> by_start_;  // (start, number) of live entries
+  long max_len_ = 0;
+};
 
 // Patch neighbour tapers (src/model.c:20-50,149-188).
 std::vector<std::vector<int>> patch_use_taper(const ProblemArgs &a) {
@@ -200,6 +251,10 @@ Schedule lambda_schedule(real initial_factor, int n_its) {
 
 int Plan::channel_index(int value, int trace_type) const {
   if (trace_type == AGDMissing) return -1;
+  if (!channel_lookup.empty() || channel_values.empty()) {
+    auto it = channel_lookup.find(value);
+    return it == channel_lookup.end() ? -1 : it->second;
+  }
   for (size_t i = 0; i < channel_values.size(); ++i)
     if (channel_values[i] == value) return (int)i;
   return -1;
@@ -207,21 +262,34 @@ int Plan::channel_index(int value, int trace_type) const {
 
 BlendCoord Plan::coord_of(long shottime, int n_times, int channel, int trace_type) const {
   // set_blend_coords (src/blend.c:693-726): first interval of the channel
-  // that strictly overlaps the trace span, clipped to it.
+  // (in list order) that strictly overlaps the trace span, clipped to it.
+  // The candidates come from the start-sorted index: intervals starting
+  // before the span ends, back to max_len before the span starts.
   BlendCoord c{-1, 0, 0};
   int const ci = channel_index(channel, trace_type);
   if (trace_type == AGDMissing || ci < 0) return c;
   Interval const span{shottime, shottime + n_times};
   const std::vector<Interval> &ivs = intervals[ci];
-  for (size_t i = 0; i < ivs.size(); ++i) {
-    if (overlaps(span, ivs[i])) {
-      long const s = span.start > ivs[i].start ? span.start : ivs[i].start;
-      long const e = span.stop < ivs[i].stop ? span.stop : ivs[i].stop;
-      c.rec = seg_off[ci][i] + (s - ivs[i].start);
-      c.trace_start = (int)(s - span.start);
-      c.n = (int)(e - s);
-      return c;
+  int best = -1;
+  if (ci < (int)by_start.size()) {
+    const auto &idx = by_start[ci];
+    auto it = std::lower_bound(idx.begin(), idx.end(), std::make_pair(span.stop, -1));
+    while (it != idx.begin()) {
+      --it;
+      if (it->first + max_len[ci] <= span.start) break;
+      if (overlaps(span, ivs[it->second]) && (best < 0 || it->second < best)) best = it->second;
     }
+  } else {
+    for (size_t i = 0; i < ivs.size() && best < 0; ++i)
+      if (overlaps(span, ivs[i])) best = (int)i;
+  }
+  if (best >= 0) {
+    const Interval &iv = ivs[best];
+    long const s = span.start > iv.start ? span.start : iv.start;
+    long const e = span.stop < iv.stop ? span.stop : iv.stop;
+    c.rec = seg_off[ci][best] + (s - iv.start);
+    c.trace_start = (int)(s - span.start);
+    c.n = (int)(e - s);
   }
   return c;
 }
@@ -230,24 +298,19 @@ void build_blend_config(int n_patches, const int *n_traces, const int *n_times,
                         const long *const *shottimes, const int *const *channels,
                         const enum AGDTraceType *const *trace_types, Plan &plan) {
   // Unique channels in first-appearance order, missing traces ignored
-  // (src/blend.c:176-223).
+  // (src/blend.c:176-223); a hash map gives each trace its channel index.
   plan.channel_values.clear();
+  plan.channel_lookup.clear();
   for (int p = 0; p < n_patches; ++p) {
     for (int t = 0; t < n_traces[p]; ++t) {
       if (trace_types[p][t] == AGDMissing) continue;
       int const c = channels[p][t];
-      bool found = false;
-      for (int v : plan.channel_values)
-        if (v == c) {
-          found = true;
-          break;
-        }
-      if (!found) plan.channel_values.push_back(c);
+      if (plan.channel_lookup.emplace(c, (int)plan.channel_values.size()).second)
+        plan.channel_values.push_back(c);
     }
   }
   size_t const nch = plan.channel_values.size();
-  plan.intervals.assign(nch, {});
-  std::vector<std::vector<Interval>> mutes(nch);
+  std::vector<IntervalList> record_lists(nch), mute_lists(nch);
   // Per-channel record intervals and bad-trace mute intervals
   // (src/blend.c:305-342).
   for (int p = 0; p < n_patches; ++p) {
@@ -255,9 +318,23 @@ void build_blend_config(int n_patches, const int *n_traces, const int *n_times,
       int const ci = plan.channel_index(channels[p][t], trace_types[p][t]);
       if (ci < 0) continue;
       Interval const iv{shottimes[p][t], shottimes[p][t] + n_times[p]};
-      add_interval(plan.intervals[ci], iv);
-      if (trace_types[p][t] == AGDBad) add_interval(mutes[ci], iv);
+      record_lists[ci].add(iv);
+      if (trace_types[p][t] == AGDBad) mute_lists[ci].add(iv);
     }
+  }
+  plan.intervals.assign(nch, {});
+  std::vector<std::vector<Interval>> mutes(nch);
+  plan.by_start.assign(nch, {});
+  plan.max_len.assign(nch, 0);
+  for (size_t c = 0; c < nch; ++c) {
+    plan.intervals[c] = record_lists[c].list();
+    mutes[c] = mute_lists[c].list();
+    for (size_t i = 0; i < plan.intervals[c].size(); ++i) {
+      const Interval &iv = plan.intervals[c][i];
+      plan.by_start[c].emplace_back(iv.start, (int)i);
+      plan.max_len[c] = std::max(plan.max_len[c], iv.stop - iv.start);
+    }
+    std::sort(plan.by_start[c].begin(), plan.by_start[c].end());
   }
   plan.seg_off.assign(nch, {});
   long off = 0;
@@ -268,14 +345,22 @@ void build_blend_config(int n_patches, const int *n_traces, const int *n_times,
     }
   }
   plan.record_size = off;
-  // Mute spans clipped to each overlapping record interval
-  // (src/blend.c:585-627).
+  // Mute spans clipped to each overlapping record interval, intervals in
+  // list order (src/blend.c:585-627)
   plan.mute.clear();
   for (size_t c = 0; c < nch; ++c) {
+    const auto &idx = plan.by_start[c];
     for (const Interval &m : mutes[c]) {
-      for (size_t i = 0; i < plan.intervals[c].size(); ++i) {
+      std::vector<int> hit;
+      auto it = std::lower_bound(idx.begin(), idx.end(), std::make_pair(m.stop, -1));
+      while (it != idx.begin()) {
+        --it;
+        if (it->first + plan.max_len[c] <= m.start) break;
+        if (overlaps(m, plan.intervals[c][it->second])) hit.push_back(it->second);
+      }
+      std::sort(hit.begin(), hit.end());
+      for (int i : hit) {
         const Interval &iv = plan.intervals[c][i];
-        if (!overlaps(m, iv)) continue;
         long const s = m.start < iv.start ? iv.start : m.start;
         long const e = m.stop > iv.stop ? iv.stop : m.stop;
         plan.mute.emplace_back(plan.seg_off[c][i] + (s - iv.start), (int)(e - s));

@@ -10,6 +10,8 @@
 
 #include <complex>
 #include <string>
+#include <unordered_map>
+#include <utility>
 #include <vector>
 
 #include "agdeblend.h"
@@ -77,6 +79,13 @@ struct Plan {
   std::vector<std::vector<Interval>> intervals;  // per channel
   std::vector<std::vector<long>> seg_off;        // per channel, per interval
   long record_size = 0;
+  // lookups built with the configuration: channel value -> index; per
+  // channel the intervals sorted by start (start, position in `intervals`)
+  // and the longest interval, which bounds how far back a search by start
+  // must look
+  std::unordered_map<int, int> channel_lookup;
+  std::vector<std::vector<std::pair<long, int>>> by_start;
+  std::vector<long> max_len;
   std::vector<std::pair<long, int>> mute;        // (flat start, n)
 
   std::vector<WindowPlan> windows;

@@ -85,3 +85,48 @@ def test_plan_enlarged_windows():
                                   sv.shapes, sv.shottimes, sv.channels, sv.trace_types)
     assert list(win[:, 10]) == [37, 37, 36]
     _compare(sv)
+
+
+def _merge_survey(seed, n_traces=400, nt=16):
+    """One 2-D patch whose trace spans overlap, touch and arrive out of
+    order on three channels: shot times on a grid of half a trace, so that
+    new spans often touch several list entries at once (the cases where the
+    reference's merge scan skips an entry)."""
+    rng = np.random.default_rng(seed)
+    st = (rng.integers(0, 60, n_traces) * (nt // 2)).astype(np.int64)
+    ch = rng.integers(0, 3, n_traces).astype(np.int32)
+    tt = rng.choice([S.LIVE, S.LIVE, S.LIVE, S.BAD, S.MISSING], n_traces).astype(np.int32)
+    tt[0] = S.LIVE
+    data = np.zeros((n_traces, nt), np.float32)
+    return S.Survey("merge", [0], [2], [[n_traces, nt]], [[0]], [[n_traces, nt]], [st], [ch],
+                    [tt], [data], [data], 1)
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_interval_merge_order_matches_reference(seed):
+    """The sort-based merge (plan.cpp IntervalList) against the oracle's
+    list scan, record layout, mute spans and blend coordinates included."""
+    _compare(_merge_survey(500 + seed))
+
+
+def test_planning_scales_to_a_million_traces():
+    """256 channels x 4096 shots x 64 samples with records that never touch:
+    4096 record intervals per channel (an interval search per trace would
+    scan 8 M entries per channel)."""
+    import time
+
+    n_ch, n_shots, nt = 256, 4096, 64
+    # record spans are C = 128 samples long (the padded time length of the
+    # 64-sample windows): shots 200 samples apart never touch
+    st = np.repeat((np.arange(n_shots) * 200).astype(np.int64)[None, :], n_ch, 0)
+    ch = np.repeat(np.arange(n_ch, dtype=np.int32)[:, None], n_shots, 1)
+    tt = np.zeros((n_ch, n_shots), np.int32)
+    t0 = time.perf_counter()
+    info, win, bl = A.plan_export([0], [3], [[16, 32, 64]], [[0, 0]], [[n_ch, n_shots, nt]],
+                                  [st], [ch], [tt])
+    dt = time.perf_counter() - t0
+    conv = int(win[0, 8])
+    assert conv == 128
+    assert info[4] == n_ch * n_shots  # one record interval per trace
+    assert info[2] == n_ch * n_shots * conv
+    assert dt < 30.0
