@@ -196,7 +196,6 @@ class Engine {
   using SpaceAdjFn = void (*)(PlaneBatches<R>, int, R, R, const R *, const R *, R *);
   using TimeFwdFn = void (*)(const TimeJob<R> *, const int *, const int *);
   using TimeAdjFn = void (*)(const TimeJob<R> *, const int *, const int *, const R *, int);
-  static constexpr int kTimeNB = 32;  // traces per block of the fast time kernels
   struct PlaneLaunch {
     DevArray<PlaneBatch<R>> batch;
     int n_batch = 0;
@@ -228,12 +227,26 @@ class Engine {
     const AdjVariant &av() const { return adj_vars[adj_pick]; }
   };
   // windows of one padded time length on the fast time kernels (whatever
-  // kernels serve their space axes)
+  // kernels serve their space axes), with candidate instantiations (traces
+  // per block, padded line stride, blocks per SM) picked by timing
+  struct TimeFwdVariant {
+    TimeFwdFn fn;
+    int nb;
+    size_t smem;
+  };
+  struct TimeAdjVariant {
+    TimeAdjFn fn;
+    int nb;
+    size_t smem;
+  };
   struct TimeGroup {
     std::vector<int> win;
-    TimeFwdFn tm_fwd = nullptr;
-    TimeAdjFn tm_adj = nullptr;
+    std::vector<TimeFwdVariant> fwd_vars;
+    std::vector<TimeAdjVariant> adj_vars;
+    int fwd_pick = 0, adj_pick = 0;
     TimeLaunch tf, ta;
+    const TimeFwdVariant &fv() const { return fwd_vars[fwd_pick]; }
+    const TimeAdjVariant &av() const { return adj_vars[adj_pick]; }
   };
   std::vector<std::unique_ptr<FastClass>> classes;
   std::vector<std::unique_ptr<TimeGroup>> tgroups;
@@ -552,14 +565,36 @@ class Engine {
     return !c.fwd_vars.empty() && !c.adj_vars.empty();
   }
 
-  // time-axis kernels for the window's padded time length
+  // time-axis kernel candidates for Pt = 2 M1 M2: NB traces per block, line
+  // stride LS (M + 1, or padded to 10 mod 16 complex so that the four-step
+  // passes hit distinct banks), MB blocks per SM
+  template <int M1, int M2, int NB, int LS, int MB>
+  static void add_time(TimeGroup &g) {
+    constexpr int M = M1 * M2;
+    constexpr int H = 4 * M / 5;
+    g.fwd_vars.push_back(TimeFwdVariant{time_fwd_fast<R, M1, M2, NB, LS, MB>, NB,
+                                        2 * (size_t)NB * LS * sizeof(C) +
+                                            (size_t)NB * H * sizeof(R)});
+    g.adj_vars.push_back(TimeAdjVariant{time_adj_fast<R, M1, M2, NB, LS, MB>, NB,
+                                        (size_t)NB * LS * sizeof(C) +
+                                            2 * (size_t)NB * 2 * H * sizeof(R)});
+  }
+
   static bool time_case(const WindowPlan &W, TimeGroup &g) {
+    g.fwd_vars.clear();
+    g.adj_vars.clear();
     if (W.Pt == 320) {
-      g.tm_fwd = time_fwd_fast<R, 16, 10, kTimeNB>;
-      g.tm_adj = time_adj_fast<R, 16, 10, kTimeNB>;
+      add_time<16, 10, 32, 161, 1>(g);
+      if constexpr (sizeof(R) == sizeof(float)) {
+        add_time<16, 10, 32, 170, 2>(g);
+        add_time<16, 10, 16, 170, 4>(g);
+      }
     } else if (W.Pt == 160) {
-      g.tm_fwd = time_fwd_fast<R, 8, 10, kTimeNB>;
-      g.tm_adj = time_adj_fast<R, 8, 10, kTimeNB>;
+      add_time<8, 10, 32, 81, 1>(g);
+      if constexpr (sizeof(R) == sizeof(float)) {
+        add_time<8, 10, 32, 90, 2>(g);
+        add_time<8, 10, 16, 90, 4>(g);
+      }
     } else {
       return false;
     }
@@ -677,7 +712,10 @@ class Engine {
         return;
       }
     }
-    CK(cudaMemsetAsync(X.get(), 0, X.bytes(), stream));
+    // a non-zero model and a small threshold, so that the adjoint's update
+    // takes the arithmetic path of real iterations (every byte 0x3f: about
+    // 0.75 in float, 1.6e-4 in double)
+    CK(cudaMemsetAsync(X.get(), 0x3f, X.bytes(), stream));
     CK(cudaMemsetAsync(S0.get(), 0, S0.bytes(), stream));
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
@@ -720,8 +758,8 @@ class Engine {
         if (L.n_batch == 0) continue;
         const SpaceAdjFn fn = c.adj_vars[v].fn;
         ta[v] = std::min(ta[v], timed([&] {
-          fn<<<L.grid, L.nt, L.smem, stream>>>(L.batches(), kUpdateThreshold, (R)0, (R)0,
-                                               nullptr, nullptr, scalar.get());
+          fn<<<L.grid, L.nt, L.smem, stream>>>(L.batches(), kUpdateThreshold, (R)0.5,
+                                               (R)1e-6, nullptr, nullptr, scalar.get());
           CK(cudaGetLastError());
         }));
       }
@@ -763,8 +801,10 @@ class Engine {
   void opt_in_classes() {
     const int limit = optin_smem();
     int dyn = smem_max;
-    for (const auto &gp : tgroups)
-      dyn = std::min({dyn, opt_in(gp->tm_fwd, limit), opt_in(gp->tm_adj, limit)});
+    for (const auto &gp : tgroups) {
+      for (const TimeFwdVariant &v : gp->fwd_vars) dyn = std::min(dyn, opt_in(v.fn, limit));
+      for (const TimeAdjVariant &v : gp->adj_vars) dyn = std::min(dyn, opt_in(v.fn, limit));
+    }
     for (const auto &cp : classes) {
       for (const FwdVariant &v : cp->fwd_vars) dyn = std::min(dyn, opt_in(v.fn, limit));
       for (const AdjVariant &v : cp->adj_vars) dyn = std::min(dyn, opt_in(v.fn, limit));
@@ -804,27 +844,115 @@ class Engine {
   }
 
   void build_time_group(TimeGroup &g) {
-    const WindowPlan &W0 = plan.windows[g.win[0]];
-    const int h = W0.h;
-    const int LS = W0.Pt / 2 + 1;
-    const size_t per_fwd = 2 * (size_t)LS * sizeof(C) + (size_t)h * sizeof(R);
-    const size_t per_adj = (size_t)LS * sizeof(C) + 2 * (size_t)(2 * h) * sizeof(R);
-    make_fixed_time_launch(g.tf, per_fwd * kTimeNB, g.win);
-    make_fixed_time_launch(g.ta, per_adj * kTimeNB, g.win);
+    autotune_time(g);
+    make_fixed_time_launch(g.tf, g.fv().smem, g.win, g.fv().nb);
+    make_fixed_time_launch(g.ta, g.av().smem, g.win, g.av().nb);
   }
 
-  void make_fixed_time_launch(TimeLaunch &L, size_t smem, const std::vector<int> &wins) {
+  // As autotune_space, for the candidates of a time group: forward
+  // S0/S1 -> Y, adjoint record (or Y after the wavelet stage) -> S0/S1.
+  // AGD_GPU_TIME_VARIANT="f,a" forces the candidates (tests).
+  void autotune_time(TimeGroup &g) {
+    g.fwd_pick = g.adj_pick = 0;
+    const char *env = std::getenv("AGD_GPU_TIME_VARIANT");
+    if (env != nullptr && env[0] != '\0') {
+      int f = 0, a = 0;
+      if (std::sscanf(env, "%d,%d", &f, &a) == 2) {
+        g.fwd_pick = std::max(0, std::min(f, (int)g.fwd_vars.size() - 1));
+        g.adj_pick = std::max(0, std::min(a, (int)g.adj_vars.size() - 1));
+        return;
+      }
+    }
+    if (g.fwd_vars.size() == 1 && g.adj_vars.size() == 1) return;
+    long traces = 0;
+    for (int w : g.win) traces += plan.windows[w].n_traces;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    char key[96];
+    std::snprintf(key, sizeof key, "time:%d:%d:%d:%d:%d", dev, (int)sizeof(R),
+                  plan.windows[g.win[0]].Pt, wavelets ? 1 : 0,
+                  (int)std::log2((double)std::max(1L, traces)));
+    static std::mutex mu;
+    static std::map<std::string, std::pair<int, int>> cache;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      auto it = cache.find(key);
+      if (it != cache.end()) {
+        g.fwd_pick = it->second.first;
+        g.adj_pick = it->second.second;
+        return;
+      }
+    }
+    if (Y.get() != nullptr) CK(cudaMemsetAsync(Y.get(), 0, Y.bytes(), stream));
+    if (rec_d.get() != nullptr) CK(cudaMemsetAsync(rec_d.get(), 0, rec_d.bytes(), stream));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto timed = [&](auto launch) {
+      launch();
+      CK(cudaEventRecord(e0, stream));
+      launch();
+      launch();
+      CK(cudaEventRecord(e1, stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      return ms;
+    };
+    const size_t nf = g.fwd_vars.size(), na = g.adj_vars.size();
+    std::vector<TimeLaunch> lf(nf), la(na);
+    std::vector<float> tf(nf, 1e30f), ta(na, 1e30f);
+    for (size_t v = 0; v < nf; ++v)
+      if (g.fwd_vars[v].smem <= (size_t)smem_max)
+        make_fixed_time_launch(lf[v], g.fwd_vars[v].smem, g.win, g.fwd_vars[v].nb);
+    for (size_t v = 0; v < na; ++v)
+      if (g.adj_vars[v].smem <= (size_t)smem_max)
+        make_fixed_time_launch(la[v], g.adj_vars[v].smem, g.win, g.adj_vars[v].nb);
+    const int from_record = wavelets ? 0 : 1;
+    for (int round = 0; round < 3; ++round) {
+      for (size_t v = 0; v < nf; ++v) {
+        const TimeLaunch &L = lf[v];
+        if (L.n_cta == 0) continue;
+        const TimeFwdFn fn = g.fwd_vars[v].fn;
+        tf[v] = std::min(tf[v], timed([&] {
+          fn<<<L.n_cta, kThreads, L.smem, stream>>>(time_jobs.get(), L.cta_job.get(),
+                                                    L.cta_trace0.get());
+          CK(cudaGetLastError());
+        }));
+      }
+      for (size_t v = 0; v < na; ++v) {
+        const TimeLaunch &L = la[v];
+        if (L.n_cta == 0) continue;
+        const TimeAdjFn fn = g.adj_vars[v].fn;
+        ta[v] = std::min(ta[v], timed([&] {
+          fn<<<L.n_cta, kThreads, L.smem, stream>>>(time_jobs.get(), L.cta_job.get(),
+                                                    L.cta_trace0.get(), rec_d.get(),
+                                                    from_record);
+          CK(cudaGetLastError());
+        }));
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    g.fwd_pick = (int)(std::min_element(tf.begin(), tf.end()) - tf.begin());
+    g.adj_pick = (int)(std::min_element(ta.begin(), ta.end()) - ta.begin());
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = {g.fwd_pick, g.adj_pick};
+  }
+
+  void make_fixed_time_launch(TimeLaunch &L, size_t smem, const std::vector<int> &wins,
+                              int nb) {
     if (smem > (size_t)smem_max) throw DeviceError("time window too long for shared memory");
     std::vector<int> cj, ct;
     for (int w : wins)
-      for (int t = 0; t < plan.windows[w].n_traces; t += kTimeNB) {
+      for (int t = 0; t < plan.windows[w].n_traces; t += nb) {
         cj.push_back(w);
         ct.push_back(t);
       }
     L.cta_job.upload(cj, stream);
     L.cta_trace0.upload(ct, stream);
     L.n_cta = (int)cj.size();
-    L.nb = kTimeNB;
+    L.nb = nb;
     L.smem = smem;
   }
 
@@ -1183,8 +1311,8 @@ class Engine {
     for (const auto &gp : tgroups) {
       const TimeGroup &g = *gp;
       if (!g.tf.n_cta) continue;
-      g.tm_fwd<<<g.tf.n_cta, kThreads, g.tf.smem, stream>>>(time_jobs.get(), g.tf.cta_job.get(),
-                                                            g.tf.cta_trace0.get());
+      g.fv().fn<<<g.tf.n_cta, kThreads, g.tf.smem, stream>>>(time_jobs.get(), g.tf.cta_job.get(),
+                                                             g.tf.cta_trace0.get());
       CK(cudaGetLastError());
     }
     if (time_fwd.n_cta) {
@@ -1201,7 +1329,7 @@ class Engine {
     for (const auto &gp : tgroups) {
       const TimeGroup &g = *gp;
       if (!g.ta.n_cta) continue;
-      g.tm_adj<<<g.ta.n_cta, kThreads, g.ta.smem, stream>>>(
+      g.av().fn<<<g.ta.n_cta, kThreads, g.ta.smem, stream>>>(
           time_jobs.get(), g.ta.cta_job.get(), g.ta.cta_trace0.get(), record, from_record);
       CK(cudaGetLastError());
     }
@@ -1746,6 +1874,9 @@ int agd_gpu_problem_info(agd_gpu_problem const *pb, long int *info) {
   info[14] = e.kernels_per_iteration();
   info[15] = (long)e.classes.size();
   info[16] = n_fast;
+  info[17] = e.tgroups.empty() ? -1 : e.tgroups[0]->fwd_pick;
+  info[18] = e.tgroups.empty() ? -1 : e.tgroups[0]->adj_pick;
+  info[19] = e.tgroups.empty() ? 0 : (long)e.tgroups[0]->fwd_vars.size();
   return 0;
 }
 

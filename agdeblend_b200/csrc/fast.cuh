@@ -640,14 +640,17 @@ __device__ __forceinline__ int fourstep_pos(int k) {
 // overlap-add; segment [t h, (t+1) h) of a trace is final once window t is
 // added, so only a one-hop carry stays in shared memory.  Blocks own NB
 // traces; the bins of window t + 1 are copied in (cp.async) while window t is
-// processed.
-template <typename R, int M1, int M2, int NB>
-__global__ void __launch_bounds__(kThreads)
+// processed.  Lines of the F = M + 1 bins are LS >= F apart in shared memory
+// (a padded stride spreads the four-step accesses over the banks); MINB
+// blocks share an SM.
+template <typename R, int M1, int M2, int NB, int LS, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
     time_fwd_fast(const TimeJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
                   const int *__restrict__ cta_trace0) {
   using C = Cx<R>;
   constexpr int M = M1 * M2;
-  constexpr int LS = M + 1;  // F bins per line
+  constexpr int F = M + 1;  // bins per line
+  static_assert(LS >= F, "line stride");
   constexpr int H = 4 * M / 5;
   constexpr int HALF = M / 2 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -666,8 +669,8 @@ __global__ void __launch_bounds__(kThreads)
   C *stage[2] = {reinterpret_cast<C *>(smem_raw), reinterpret_cast<C *>(smem_raw) + NB * LS};
   R *carry = reinterpret_cast<R *>(stage[1] + NB * LS);  // [NB][H]
   auto issue = [&](int t, C *buf) {
-    const C *zt = job.z + (long)t * LS * ntr + t0;
-    for (int idx = threadIdx.x; idx < NB * LS; idx += kThreads) {
+    const C *zt = job.z + (long)t * F * ntr + t0;
+    for (int idx = threadIdx.x; idx < NB * F; idx += kThreads) {
       const int f = idx / NB;
       const int i = idx - f * NB;
       if (i < nb) cp_async<sizeof(C)>(buf + i * LS + f, zt + f * ntr + i);
@@ -744,15 +747,17 @@ __global__ void __launch_bounds__(kThreads)
 // trace buffer), taper, pack pairs into M complex values, forward FFT, split
 // into the M + 1 bins and double bins 1..M-1.  The raw samples of window
 // t + 1 are copied in (cp.async, zero-filled outside the blended span) while
-// window t is transformed.
-template <typename R, int M1, int M2, int NB>
-__global__ void __launch_bounds__(kThreads)
+// window t is transformed.  Line stride LS >= M + 1 and MINB as in
+// time_fwd_fast.
+template <typename R, int M1, int M2, int NB, int LS, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
     time_adj_fast(const TimeJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
                   const int *__restrict__ cta_trace0, const R *__restrict__ record,
                   int from_record) {
   using C = Cx<R>;
   constexpr int M = M1 * M2;
-  constexpr int LS = M + 1;
+  constexpr int F = M + 1;  // bins per line
+  static_assert(LS >= F, "line stride");
   constexpr int H = 4 * M / 5;
   constexpr int LT = 2 * H;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -830,8 +835,8 @@ __global__ void __launch_bounds__(kThreads)
     __syncthreads();
     lines_fourstep<R, M1, M2, false>(line, NB, LS, twM);
     // split: X_k = (Z_k + conj Z_{M-k}) / 2 - i e^{-2 pi i k / Pt} (Z_k - conj Z_{M-k}) / 2
-    C *zt = job.z + (long)t * LS * ntr + t0;
-    for (int idx = threadIdx.x; idx < NB * LS; idx += kThreads) {
+    C *zt = job.z + (long)t * F * ntr + t0;
+    for (int idx = threadIdx.x; idx < NB * F; idx += kThreads) {
       const int f = idx / NB;
       const int i = idx - f * NB;
       if (i < nb) {

@@ -39,9 +39,11 @@ def _interleave(x):
     return np.stack([x.real, x.imag], -1).reshape(-1)
 
 
-def _problem(sv, generic=False, dtype=np.float32, variant=None):
+def _problem(sv, generic=False, dtype=np.float32, variant=None, time_variant=None):
     env = {"AGD_GPU_GENERIC": "1" if generic else "0",
-           "AGD_GPU_SPACE_VARIANT": "" if variant is None else f"{variant[0]},{variant[1]}"}
+           "AGD_GPU_SPACE_VARIANT": "" if variant is None else f"{variant[0]},{variant[1]}",
+           "AGD_GPU_TIME_VARIANT": "" if time_variant is None else
+           f"{time_variant[0]},{time_variant[1]}"}
     old = {k: os.environ.get(k) for k in env}
     os.environ.update(env)
     try:
@@ -98,6 +100,22 @@ def test_every_space_candidate_vs_oracle(name, make):
         pick = (min(v, n_f - 1), min(v, n_a - 1))
         prob = _problem(sv, variant=pick)
         assert (prob.info[10], prob.info[11]) == pick
+        _check_operators(sv, prob, 1e-5)
+        prob.close()
+
+
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+def test_every_time_candidate_vs_oracle(name, make):
+    """Each time-kernel candidate (traces per block, line stride) the set-up
+    timing may pick."""
+    sv = make()
+    probe = _problem(sv)
+    n = int(probe.info[19])
+    probe.close()
+    assert n >= 1
+    for v in range(n):
+        prob = _problem(sv, time_variant=(v, v))
+        assert (prob.info[17], prob.info[18]) == (v, v)
         _check_operators(sv, prob, 1e-5)
         prob.close()
 
