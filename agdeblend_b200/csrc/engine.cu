@@ -38,23 +38,142 @@ static void check(cudaError_t e, const char *what) {
 }
 #define CK(x) check((x), #x)
 
+// Device blocks of finished problems kept for the next problem on the same
+// device: a deblending call allocates its large arrays (model, intermediates,
+// traces, records) once per call, and a fresh cudaMalloc of gigabytes costs
+// page mapping that can exceed the solve itself.  Blocks enter the cache
+// only from the destructor of an engine whose stream has been synchronised,
+// so no kernel can still use them.  Best fit within a factor of two; at most
+// half the device memory is held (AGD_GPU_CACHE=0 disables the cache;
+// agd_gpu_release_cache frees it).
+class DevicePool {
+ public:
+  static void *take(size_t bytes) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (enabled()) {
+      std::lock_guard<std::mutex> g(mu());
+      auto &m = free_blocks()[dev];
+      auto it = m.lower_bound(bytes);
+      if (it != m.end() && it->first <= 2 * bytes + (size_t(1) << 20)) {
+        void *p = it->second;
+        held() -= it->first;
+        m.erase(it);
+        return p;
+      }
+    }
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaErrorMemoryAllocation) {
+      cudaGetLastError();
+      release_device(dev);
+      e = cudaMalloc(&p, bytes);
+    }
+    CK(e);
+    std::lock_guard<std::mutex> g(mu());
+    sizes()[p] = bytes;
+    return p;
+  }
+
+  static void put(void *p) {
+    if (p == nullptr) return;
+    int dev = 0;
+    size_t freeb = 0, total = 0;
+    if (!enabled() || cudaGetDevice(&dev) != cudaSuccess ||
+        cudaMemGetInfo(&freeb, &total) != cudaSuccess) {
+      drop(p);
+      return;
+    }
+    std::lock_guard<std::mutex> g(mu());
+    const size_t bytes = sizes()[p];
+    if (held() + bytes > total / 2) {
+      sizes().erase(p);
+      cudaFree(p);
+      return;
+    }
+    free_blocks()[dev].emplace(bytes, p);
+    held() += bytes;
+  }
+
+  static void release_device(int dev) {
+    std::lock_guard<std::mutex> g(mu());
+    auto &m = free_blocks()[dev];
+    for (auto &kv : m) {
+      held() -= kv.first;
+      sizes().erase(kv.second);
+      cudaFree(kv.second);
+    }
+    m.clear();
+  }
+
+  static void release_all() {
+    std::vector<int> devs;
+    {
+      std::lock_guard<std::mutex> g(mu());
+      for (auto &kv : free_blocks()) devs.push_back(kv.first);
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (int d : devs) {
+      cudaSetDevice(d);
+      release_device(d);
+    }
+    cudaSetDevice(cur);
+  }
+
+ private:
+  static bool enabled() {
+    static const bool on = [] {
+      const char *env = std::getenv("AGD_GPU_CACHE");
+      return !(env != nullptr && env[0] == '0');
+    }();
+    return on;
+  }
+  static void drop(void *p) {
+    {
+      std::lock_guard<std::mutex> g(mu());
+      sizes().erase(p);
+    }
+    cudaFree(p);
+  }
+  static std::mutex &mu() {
+    static std::mutex m;
+    return m;
+  }
+  static std::map<int, std::multimap<size_t, void *>> &free_blocks() {
+    static std::map<int, std::multimap<size_t, void *>> m;
+    return m;
+  }
+  static std::map<void *, size_t> &sizes() {
+    static std::map<void *, size_t> m;
+    return m;
+  }
+  static size_t &held() {
+    static size_t h = 0;
+    return h;
+  }
+};
+
 template <typename T>
 class DevArray {
  public:
   DevArray() = default;
   DevArray(const DevArray &) = delete;
   DevArray &operator=(const DevArray &) = delete;
-  DevArray(DevArray &&o) noexcept : p_(o.p_), n_(o.n_) {
+  DevArray(DevArray &&o) noexcept : p_(o.p_), n_(o.n_), pooled_(o.pooled_) {
     o.p_ = nullptr;
     o.n_ = 0;
+    o.pooled_ = false;
   }
   DevArray &operator=(DevArray &&o) noexcept {
     if (this != &o) {
       release();
       p_ = o.p_;
       n_ = o.n_;
+      pooled_ = o.pooled_;
       o.p_ = nullptr;
       o.n_ = 0;
+      o.pooled_ = false;
     }
     return *this;
   }
@@ -62,6 +181,16 @@ class DevArray {
   void alloc(size_t n) {
     release();
     if (n) CK(cudaMalloc(reinterpret_cast<void **>(&p_), n * sizeof(T)));
+    n_ = n;
+  }
+  // From the device cache; the array must live until its engine's stream
+  // is idle (engine members: the engine synchronises before destruction).
+  void alloc_pooled(size_t n) {
+    release();
+    if (n) {
+      p_ = static_cast<T *>(DevicePool::take(n * sizeof(T)));
+      pooled_ = true;
+    }
     n_ = n;
   }
   void upload(const std::vector<T> &v, cudaStream_t s) {
@@ -72,14 +201,21 @@ class DevArray {
   size_t size() const { return n_; }
   size_t bytes() const { return n_ * sizeof(T); }
   void release() {
-    if (p_) cudaFree(p_);
+    if (p_) {
+      if (pooled_)
+        DevicePool::put(p_);
+      else
+        cudaFree(p_);
+    }
     p_ = nullptr;
     n_ = 0;
+    pooled_ = false;
   }
 
  private:
   T *p_ = nullptr;
   size_t n_ = 0;
+  bool pooled_ = false;
 };
 
 // Distinct FFT lengths with their radix lists and twiddle tables.
@@ -284,7 +420,16 @@ class Engine {
       CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
     }
     set_smem_limits();
-    build();
+    try {
+      build();
+    } catch (...) {
+      // nothing of this engine may still run when its arrays are released
+      cudaStreamSynchronize(stream);
+      release_graph();
+      cudaStreamDestroy(stream);
+      stream = nullptr;
+      throw;
+    }
   }
 
   ~Engine() {
@@ -476,9 +621,10 @@ class Engine {
 
   // Candidate instantiations of the fast space kernels for one padded shape
   // P0..P2 (window lengths 4P/5): threads, planes per batch, stages and
-  // blocks per SM.  The two-stage kernels fill most of the shared memory with
-  // one block per SM; the one-stage kernels run two or three blocks per SM
-  // (two for 40-point lines, whose registers do not fit three).  The
+  // blocks per SM.  Two-stage kernels either fill most of the shared memory
+  // with one block per SM or take a third of it per block with two blocks
+  // per SM; the one-stage kernels run two or three blocks per SM (two for
+  // 40-point lines, whose registers do not fit three).  The
   // fastest of each list is picked by timing on the problem (autotune_space).
   template <int D, int P0, int P1, int P2, int NT, int NP, int ST, int MB>
   static void add_fwd(FastClass &c) {
@@ -511,28 +657,38 @@ class Engine {
       if (shape_is<1, 40, 1, 1>(W)) {
         add_fwd<1, 40, 1, 1, 256, 256, 2, 1>(c);
         add_fwd<1, 40, 1, 1, 256, 96, 1, 2>(c);
+        add_fwd<1, 40, 1, 1, 256, 96, 2, 2>(c);
         add_adj<1, 40, 1, 1, 192, 192, 2, 1>(c);
         add_adj<1, 40, 1, 1, 256, 96, 1, 2>(c);
+        add_adj<1, 40, 1, 1, 256, 96, 2, 2>(c);
       } else if (shape_is<1, 20, 1, 1>(W)) {
         add_fwd<1, 20, 1, 1, 256, 256, 2, 1>(c);
         add_fwd<1, 20, 1, 1, 256, 128, 1, 3>(c);
+        add_fwd<1, 20, 1, 1, 256, 128, 2, 2>(c);
         add_adj<1, 20, 1, 1, 256, 256, 2, 1>(c);
         add_adj<1, 20, 1, 1, 256, 128, 1, 3>(c);
+        add_adj<1, 20, 1, 1, 256, 128, 2, 2>(c);
       } else if (shape_is<2, 20, 40, 1>(W)) {
         add_fwd<2, 20, 40, 1, 384, 16, 2, 1>(c);
         add_fwd<2, 20, 40, 1, 256, 12, 1, 2>(c);
+        add_fwd<2, 20, 40, 1, 256, 6, 2, 2>(c);
         add_adj<2, 20, 40, 1, 384, 11, 2, 1>(c);
         add_adj<2, 20, 40, 1, 256, 12, 1, 2>(c);
+        add_adj<2, 20, 40, 1, 256, 5, 2, 2>(c);
       } else if (shape_is<2, 20, 20, 1>(W)) {
         add_fwd<2, 20, 20, 1, 384, 24, 2, 1>(c);
         add_fwd<2, 20, 20, 1, 256, 12, 1, 3>(c);
+        add_fwd<2, 20, 20, 1, 256, 12, 2, 2>(c);
         add_adj<2, 20, 20, 1, 384, 20, 2, 1>(c);
         add_adj<2, 20, 20, 1, 256, 12, 1, 3>(c);
+        add_adj<2, 20, 20, 1, 256, 10, 2, 2>(c);
       } else if (shape_is<2, 40, 40, 1>(W)) {
         add_fwd<2, 40, 40, 1, 320, 8, 2, 1>(c);
         add_fwd<2, 40, 40, 1, 256, 6, 1, 2>(c);
+        add_fwd<2, 40, 40, 1, 256, 3, 2, 2>(c);
         add_adj<2, 40, 40, 1, 256, 5, 2, 1>(c);
         add_adj<2, 40, 40, 1, 256, 6, 1, 2>(c);
+        add_adj<2, 40, 40, 1, 256, 2, 2, 2>(c);
       } else if (shape_is<3, 20, 20, 20>(W)) {
         add_fwd<3, 20, 20, 20, 512, 1, 2, 1>(c);
         add_fwd<3, 20, 20, 20, 256, 1, 1, 3>(c);
@@ -1041,12 +1197,12 @@ class Engine {
     wt_C.upload(wC, stream);
 
     pick_classes();
-    X.alloc(M);
-    S0.alloc(M);
-    if (n_generic) S1.alloc(M);
-    Y.alloc(toff);
-    rec_d.alloc(plan.record_size);
-    rec_r.alloc(plan.record_size);
+    X.alloc_pooled(M);
+    S0.alloc_pooled(M);
+    if (n_generic) S1.alloc_pooled(M);
+    Y.alloc_pooled(toff);
+    rec_d.alloc_pooled(plan.record_size);
+    rec_r.alloc_pooled(plan.record_size);
     scalar.alloc(1);
     dscalar.alloc(1);
     multi = plan.n_problems > 1;
@@ -1198,7 +1354,7 @@ class Engine {
       poff += (long)plan.n_traces[p] * plan.n_times[p];
     }
     data_size = poff;
-    data_dev.alloc(data_size);
+    data_dev.alloc_pooled(data_size);
     {
       std::vector<std::vector<long>> cover;  // per global patch trace
       std::vector<long> tr_base(plan.n_patches);
@@ -1242,7 +1398,7 @@ class Engine {
 
   void ensure_plain_adjoint() {
     if (G.get() != nullptr || plan.model_size == 0) return;
-    G.alloc(plan.model_size);
+    G.alloc_pooled(plan.model_size);
     for (auto &cp : classes) {
       FastClass &c = *cp;
       std::vector<PlaneJob<R>> jobs = c.plain_jobs;
@@ -2167,6 +2323,8 @@ int agd_gpu_batch_create(int n_problems, int const *n_patches, int const *const 
   }
   return create_batch(args, problem);
 }
+
+void agd_gpu_release_cache(void) { agd::DevicePool::release_all(); }
 
 int agd_gpu_problem_steps(agd_gpu_problem const *pb, AGD_TYPE *steps) {
   if (pb == nullptr || steps == nullptr) return 1;

@@ -146,6 +146,12 @@ int agd_gpu_batch_create(int n_problems, int const *n_patches, int const *const 
  * problem). */
 int agd_gpu_problem_steps(agd_gpu_problem const *problem, AGD_TYPE *steps);
 
+/* The library keeps the large device arrays of finished problems (at most
+ * half the device memory) for the next problem on the same device, since a
+ * fresh allocation of gigabytes costs more than a solve; this returns them
+ * to the device.  AGD_GPU_CACHE=0 in the environment disables the cache. */
+void agd_gpu_release_cache(void);
+
 /* agd_blend for callers that cannot allocate device memory (code running
  * inside a CUDA stream capture, hosts whose pool owns all device memory,
  * latency-critical callers).  No counterpart in the reference: it is an
