@@ -641,6 +641,21 @@ class Engine {
                                     ST, ((size_t)ST * NP * Sh::size + x) * sizeof(C)});
   }
 
+  // row-fused candidates (fast.cuh space_fwd_rows / space_adj_rows)
+  template <int D, int P0, int P1, int P2, int NT, int NP, int MB>
+  static void add_fwd_rows(FastClass &c) {
+    using Sh = PlaneShape<D, P0, P1, P2>;
+    c.fwd_vars.push_back(FwdVariant{space_fwd_rows<R, D, P0, P1, P2, NT, NP, MB>, NT, NP, 1,
+                                    (size_t)NP * Sh::size * sizeof(C)});
+  }
+
+  template <int D, int P0, int P1, int P2, int NT, int NP, int ST, int MB>
+  static void add_adj_rows(FastClass &c) {
+    using Sh = PlaneShape<D, P0, P1, P2>;
+    c.adj_vars.push_back(AdjVariant{space_adj_rows<R, D, P0, P1, P2, NT, NP, ST, MB>, NT, NP,
+                                    ST, (size_t)ST * NP * Sh::size * sizeof(C)});
+  }
+
   template <int D, int P0, int P1, int P2>
   static bool shape_is(const WindowPlan &W) {
     const int P[3] = {P0, P1, P2};
@@ -661,6 +676,8 @@ class Engine {
         add_adj<1, 40, 1, 1, 192, 192, 2, 1>(c);
         add_adj<1, 40, 1, 1, 256, 96, 1, 2>(c);
         add_adj<1, 40, 1, 1, 256, 96, 2, 2>(c);
+        add_fwd_rows<1, 40, 1, 1, 256, 64, 2>(c);
+        add_adj_rows<1, 40, 1, 1, 256, 64, 2, 2>(c);
       } else if (shape_is<1, 20, 1, 1>(W)) {
         add_fwd<1, 20, 1, 1, 256, 256, 2, 1>(c);
         add_fwd<1, 20, 1, 1, 256, 128, 1, 3>(c);
@@ -668,6 +685,8 @@ class Engine {
         add_adj<1, 20, 1, 1, 256, 256, 2, 1>(c);
         add_adj<1, 20, 1, 1, 256, 128, 1, 3>(c);
         add_adj<1, 20, 1, 1, 256, 128, 2, 2>(c);
+        add_fwd_rows<1, 20, 1, 1, 256, 128, 3>(c);
+        add_adj_rows<1, 20, 1, 1, 256, 128, 2, 2>(c);
       } else if (shape_is<2, 20, 40, 1>(W)) {
         add_fwd<2, 20, 40, 1, 384, 16, 2, 1>(c);
         add_fwd<2, 20, 40, 1, 256, 12, 1, 2>(c);
@@ -675,6 +694,8 @@ class Engine {
         add_adj<2, 20, 40, 1, 384, 11, 2, 1>(c);
         add_adj<2, 20, 40, 1, 256, 12, 1, 2>(c);
         add_adj<2, 20, 40, 1, 256, 5, 2, 2>(c);
+        add_fwd_rows<2, 20, 40, 1, 256, 8, 2>(c);
+        add_adj_rows<2, 20, 40, 1, 256, 6, 2, 2>(c);
       } else if (shape_is<2, 20, 20, 1>(W)) {
         add_fwd<2, 20, 20, 1, 384, 24, 2, 1>(c);
         add_fwd<2, 20, 20, 1, 256, 12, 1, 3>(c);
@@ -682,6 +703,8 @@ class Engine {
         add_adj<2, 20, 20, 1, 384, 20, 2, 1>(c);
         add_adj<2, 20, 20, 1, 256, 12, 1, 3>(c);
         add_adj<2, 20, 20, 1, 256, 10, 2, 2>(c);
+        add_fwd_rows<2, 20, 20, 1, 256, 12, 3>(c);
+        add_adj_rows<2, 20, 20, 1, 256, 10, 2, 2>(c);
       } else if (shape_is<2, 40, 40, 1>(W)) {
         add_fwd<2, 40, 40, 1, 320, 8, 2, 1>(c);
         add_fwd<2, 40, 40, 1, 256, 6, 1, 2>(c);
@@ -689,11 +712,16 @@ class Engine {
         add_adj<2, 40, 40, 1, 256, 5, 2, 1>(c);
         add_adj<2, 40, 40, 1, 256, 6, 1, 2>(c);
         add_adj<2, 40, 40, 1, 256, 2, 2, 2>(c);
+        add_fwd_rows<2, 40, 40, 1, 256, 4, 2>(c);
+        add_adj_rows<2, 40, 40, 1, 256, 3, 2, 2>(c);
       } else if (shape_is<3, 20, 20, 20>(W)) {
         add_fwd<3, 20, 20, 20, 512, 1, 2, 1>(c);
         add_fwd<3, 20, 20, 20, 256, 1, 1, 3>(c);
+        add_fwd_rows<3, 20, 20, 20, 256, 1, 3>(c);
         add_adj<3, 20, 20, 20, 512, 1, 2, 1>(c);
         add_adj<3, 20, 20, 20, 256, 1, 1, 3>(c);
+        add_adj_rows<3, 20, 20, 20, 512, 1, 2, 1>(c);
+        add_adj_rows<3, 20, 20, 20, 256, 1, 1, 3>(c);
       }
     } else {
       // double: the two-stage kernels only (one-stage kernels with several

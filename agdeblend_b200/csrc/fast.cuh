@@ -579,6 +579,209 @@ __global__ void __launch_bounds__(NT, MINB)
   }
 }
 
+// ------------------------------------------------------------ row-fused space kernels
+
+// One row of N complex values from global memory, in 16-byte vectors when
+// `vec` (float, even N, a 16-byte aligned row; windows of odd model size
+// leave the next windows' rows at odd complex offsets).
+template <typename R, int N>
+__device__ __forceinline__ void load_row(Cx<R> (&v)[N], const Cx<R> *src, bool vec) {
+  if (sizeof(R) == sizeof(float) && N % 2 == 0 && vec) {
+    const float4 *s4 = reinterpret_cast<const float4 *>(src);
+#pragma unroll
+    for (int k = 0; k < N / 2; ++k) {
+      const float4 q = s4[k];
+      v[2 * k] = cmake<Cx<R>>(q.x, q.y);
+      v[2 * k + 1] = cmake<Cx<R>>(q.z, q.w);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = src[k];
+  }
+}
+
+// Forward operator, all space axes, with the first pass (last axis) reading
+// each model row straight from global memory into registers: no staging of
+// the model planes in shared memory.  The remaining axes and the store of
+// the cropped planes are those of space_fwd_fast.  MINB blocks per SM
+// overlap one another's loads.
+template <typename R, int D, int P0, int P1, int P2, int NT, int NP, int MINB>
+__global__ void __launch_bounds__(NT, MINB) space_fwd_rows(PlaneBatches<R> batches) {
+  using C = Cx<R>;
+  using S = PlaneShape<D, P0, P1, P2>;
+  constexpr int Z = S::size;
+  constexpr int PL = S::PL;                      // last-axis padded length
+  constexpr int LL = PL * 4 / 5;                 // its window length
+  constexpr int ROWS = S::dense_P / PL;          // rows per model plane
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *buf = reinterpret_cast<C *>(smem_raw);
+  for (int b = blockIdx.x; b < batches.n; b += gridDim.x) {
+    const PlaneBatch<R> bt = batches.b[b];
+    const int np = bt.count;
+    // rows are PL (even) apart within a window: one alignment test per batch
+    const bool vec = (reinterpret_cast<uintptr_t>(bt.src) & 15) == 0;
+    for (int r = threadIdx.x; r < np * ROWS; r += NT) {
+      const int p = r / ROWS;
+      const int q = r - p * ROWS;
+      C v[PL];
+      load_row<R, PL>(v, bt.src + (long)p * S::dense_P + (long)q * PL, vec);
+      dft<R, PL, true>(v);
+      C *row = buf + p * Z + q * S::PLS;
+#pragma unroll
+      for (int e = 0; e < LL; ++e) row[e] = v[e];
+    }
+    __syncthreads();
+    if constexpr (D == 2) {
+      lines_fft<R, P0, true, NT, NP, Z, 1, S::L1, 0, S::S0, 1, P0, S::L0>(buf, np);
+      __syncthreads();
+    } else if constexpr (D == 3) {
+      lines_fft<R, P1, true, NT, NP, Z, P0, S::L2, S::S0, S::S1, 1, P1, S::L1>(buf, np);
+      __syncthreads();
+      lines_fft<R, P0, true, NT, NP, Z, S::L1, S::L2, S::S1, S::S0, 1, P0, S::L0>(buf, np);
+      __syncthreads();
+    }
+    C *dst = bt.dst;
+    const int n_store = np * S::dense_L;
+    for (int e = threadIdx.x; e < n_store; e += NT) {
+      const int p = e / S::dense_L;
+      dst[e] = buf[p * Z + plane_pos<D, P0, P1, P2, S::L1, S::L2>(e - p * S::dense_L)];
+    }
+    __syncthreads();
+  }
+}
+
+// Adjoint, all space axes, with the update fused into the last pass: that
+// pass runs along the contiguous axis, so each thread's P outputs are one
+// row of the model plane, which it reads, updates (epilogues as
+// space_adj_fast) and writes back in 16-byte vectors.  The padded planes of
+// the intermediate are staged as in space_adj_fast (STAGES 1 or 2); no model
+// staging buffer.
+template <typename R, int D, int P0, int P1, int P2, int NT, int NP, int STAGES, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+    space_adj_rows(PlaneBatches<R> batches, int epilogue, R step_arg, R lamb_arg,
+                   const R *step_dev, const R *lamb_dev, R *max_out) {
+  static_assert(STAGES == 1 || STAGES == 2, "one or two stages");
+  using C = Cx<R>;
+  using S = PlaneShape<D, P0, P1, P2>;
+  constexpr int Z = S::size;
+  constexpr int PL = S::PL;
+  constexpr int LL = PL * 4 / 5;
+  constexpr int ROWS = S::dense_P / PL;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *base = reinterpret_cast<C *>(smem_raw);
+  C *stage[2] = {base, base + (STAGES == 2 ? NP * Z : 0)};
+  auto issue = [&](const PlaneBatch<R> &bt, C *buf) {
+    const int n = bt.count * S::dense_L;
+    for (int e = threadIdx.x; e < n; e += NT) {
+      const int p = e / S::dense_L;
+      cp_async<sizeof(C)>(buf + p * Z + plane_pos<D, P0, P1, P2, S::L1, S::L2>(
+                                            e - p * S::dense_L),
+                          bt.src + e);
+    }
+  };
+  const bool multi = step_dev != nullptr;
+  R local_max = (R)0;
+  const PlaneBatch<R> none{nullptr, nullptr, 0, 0};
+  int b = blockIdx.x;
+  PlaneBatch<R> cur = b < batches.n ? batches.b[b] : none;
+  PlaneBatch<R> nxt = b + gridDim.x < batches.n ? batches.b[b + gridDim.x] : none;
+  if (b < batches.n) issue(cur, stage[0]);
+  cp_async_commit();
+  for (int k = 0; b < batches.n; ++k, b += gridDim.x) {
+    const int b2 = b + 2 * gridDim.x;
+    const PlaneBatch<R> after = b2 < batches.n ? batches.b[b2] : none;
+    if constexpr (STAGES == 2) {
+      if (nxt.count > 0) issue(nxt, stage[(k + 1) & 1]);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const int np = cur.count;
+    C *buf = stage[STAGES == 2 ? (k & 1) : 0];
+    if constexpr (D == 2) {
+      lines_fft<R, P0, false, NT, NP, Z, 1, S::L1, 0, S::S0, 1, S::L0, P0>(buf, np);
+      __syncthreads();
+    } else if constexpr (D == 3) {
+      lines_fft<R, P0, false, NT, NP, Z, S::L1, S::L2, S::S1, S::S0, 1, S::L0, P0>(buf, np);
+      __syncthreads();
+      lines_fft<R, P1, false, NT, NP, Z, P0, S::L2, S::S0, S::S1, 1, S::L1, P1>(buf, np);
+      __syncthreads();
+    }
+    const R step = multi ? step_dev[cur.pid] : step_arg;
+    const R lamb = lamb_dev != nullptr ? lamb_dev[multi ? cur.pid : 0] : lamb_arg;
+    const R lamb_sq = lamb * lamb;
+    // rows are PL (even) apart within a window: one alignment test per batch
+    const bool vec = sizeof(R) == sizeof(float) && (reinterpret_cast<uintptr_t>(cur.dst) & 15) == 0;
+    for (int r = threadIdx.x; r < np * ROWS; r += NT) {
+      const int p = r / ROWS;
+      const int q = r - p * ROWS;
+      const C *row = buf + p * Z + q * S::PLS;
+      C v[PL];
+#pragma unroll
+      for (int e = 0; e < PL; ++e) v[e] = e < LL ? row[e] : cmake<C>((R)0, (R)0);
+      dft<R, PL, false>(v);
+      C *xr = cur.dst + (long)p * S::dense_P + (long)q * PL;
+      if (epilogue == kStore) {
+#pragma unroll
+        for (int e = 0; e < PL; ++e) xr[e] = v[e];
+        continue;
+      }
+#pragma unroll
+      for (int e = 0; e < PL; e += 2) {
+        C x0, x1;
+        if (vec) {
+          const float4 q4 = *reinterpret_cast<const float4 *>(xr + e);
+          x0 = cmake<C>((R)q4.x, (R)q4.y);
+          x1 = cmake<C>((R)q4.z, (R)q4.w);
+        } else {
+          x0 = xr[e];
+          x1 = xr[e + 1];
+        }
+        C n0 = cmake<C>(sub_rn<R>(x0.x, mul_rn<R>(step, v[e].x)),
+                        sub_rn<R>(x0.y, mul_rn<R>(step, v[e].y)));
+        C n1 = cmake<C>(sub_rn<R>(x1.x, mul_rn<R>(step, v[e + 1].x)),
+                        sub_rn<R>(x1.y, mul_rn<R>(step, v[e + 1].y)));
+        if (epilogue == kUpdateThreshold) {
+          n0 = soft_threshold<R>(n0, lamb, lamb_sq);
+          n1 = soft_threshold<R>(n1, lamb, lamb_sq);
+        } else {
+          const R a0 = abs_sq<R>(n0);
+          const R a1 = abs_sq<R>(n1);
+          local_max = a0 > local_max ? a0 : local_max;
+          local_max = a1 > local_max ? a1 : local_max;
+        }
+        if (vec) {
+          *reinterpret_cast<float4 *>(xr + e) =
+              make_float4((float)n0.x, (float)n0.y, (float)n1.x, (float)n1.y);
+        } else {
+          xr[e] = n0;
+          xr[e + 1] = n1;
+        }
+      }
+    }
+    __syncthreads();
+    if (multi && epilogue == kUpdateMax) {  // one maximum per problem
+      __shared__ R red_b[32];
+      const R m = block_max<R>(local_max, red_b);
+      if (threadIdx.x == 0) atomic_max_nonneg(max_out + cur.pid, m);
+      local_max = (R)0;
+    }
+    if constexpr (STAGES == 1) {
+      if (nxt.count > 0) issue(nxt, stage[0]);
+      cp_async_commit();
+    }
+    cur = nxt;
+    nxt = after;
+  }
+  if (!multi && epilogue == kUpdateMax) {
+    __shared__ R red[32];
+    const R m = block_max<R>(local_max, red);
+    if (threadIdx.x == 0) atomic_max_nonneg(max_out, m);
+  }
+}
+
 // ------------------------------------------------------------ time axis
 
 // Twiddles W_N^k, k < N, copied to shared memory for lookups whose index

@@ -135,3 +135,43 @@ def test_mixed_window_classes_vs_oracle_and_generic():
     for a, b in zip(out, out_g):
         assert rel_l2(a, b) <= 1e-5
     gen.close()
+
+
+def _odd_offset_batch():
+    """A gather whose enlarged windows (37, 37 and 36 samples: padded 47,
+    47, 45; 5 time windows of 161 bins) have odd model sizes, then a gather
+    of 32-sample windows on the shape-specialised kernels, whose models then
+    start at odd complex offsets (8-byte but not 16-byte aligned)."""
+    a = S.gather_2d(seed=3110, n_shots=78, nt=500, window=(32, 256))
+    b = S.gather_2d(seed=3111, n_shots=64, nt=500, window=(32, 256))
+    off, odd_fast = 0, 0
+    for g in (a, b):
+        info, win, bl = A.plan_export(g.volumes, g.n_dims, g.window_shapes, g.coords, g.shapes,
+                                      g.shottimes, g.channels, g.trace_types)
+        for row in win:
+            if row[10] * 5 == row[14] * 4 and off % 2:
+                odd_fast += 1
+            off += int(row[2]) * int(row[3]) * int(row[14])
+    assert odd_fast > 0
+    return [a, b]
+
+
+def test_every_space_candidate_at_odd_model_offsets():
+    gathers = _odd_offset_batch()
+    refs = [_single(g, 10) for g in gathers]
+    probe = A.Problem.from_batch(gathers)
+    n = int(max(probe.info[12], probe.info[13]))
+    probe.close()
+    old = os.environ.get("AGD_GPU_SPACE_VARIANT")
+    try:
+        for v in range(n):
+            os.environ["AGD_GPU_SPACE_VARIANT"] = f"{v},{v}"
+            outs = A.deblend_batch([_kw(g) for g in gathers], 1.0, 10)
+            for out, ref in zip(outs, refs):
+                for o, r in zip(out, ref):
+                    assert rel_l2(o, r) <= 1e-5
+    finally:
+        if old is None:
+            os.environ.pop("AGD_GPU_SPACE_VARIANT", None)
+        else:
+            os.environ["AGD_GPU_SPACE_VARIANT"] = old
