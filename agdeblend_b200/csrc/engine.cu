@@ -409,6 +409,9 @@ class Engine {
   DevArray<WaveletFastJob<R>> wavf_jobs;
   DevArray<int> kperm;
   TimeLaunch wavf;
+  using WaveletFn = void (*)(const WaveletFastJob<R> *, const int *, const int *, int,
+                             const C *, const long *, int, const R *);
+  WaveletFn wav_fn = nullptr;
   R stepsize = 0;
 
   explicit Engine(Plan &&p) : plan(std::move(p)) {
@@ -460,8 +463,12 @@ class Engine {
   void set_smem_limits() {
     const int limit = smem_max;
     smem_max = std::min({opt_in(axis_pass<R>, limit), opt_in(time_c2r_ola<R>, limit),
-                         opt_in(time_r2c<R>, limit), opt_in(wavelet_apply<R>, limit),
-                         opt_in(wavelet_fast<R>, limit)});
+                         opt_in(time_r2c<R>, limit), opt_in(wavelet_apply<R>, limit)});
+    if constexpr (sizeof(R) == sizeof(float))
+      smem_max = std::min({smem_max, opt_in(wavelet_fast<R, 2>, limit),
+                           opt_in(wavelet_fast<R, 3>, limit)});
+    else
+      smem_max = std::min(smem_max, opt_in(wavelet_fast<R, 1>, limit));
   }
 
   // twiddle tables of the register DFTs in constant memory of the current
@@ -540,10 +547,8 @@ class Engine {
       n_max = std::max(n_max, N);
     }
     const size_t per_pair = (size_t)n_max * sizeof(C);
-    const int np = (int)std::max<size_t>(1, std::min<size_t>(4, 60000 / per_pair));
-    if (per_pair * np > (size_t)smem_max) return;
+    if (per_pair > (size_t)smem_max) return;
     kperm.upload(perm, stream);
-    std::vector<int> cj, cp;
     for (int w = 0; w < nw; ++w) {
       const WindowPlan &W = plan.windows[w];
       WaveletFastJob<R> &j = jobs[w];
@@ -554,19 +559,117 @@ class Engine {
       j.blend_ts = blend_ts.get() + wt_base[w];
       j.blend_n = blend_n.get() + wt_base[w];
       j.n_traces = W.n_traces;
-      for (int p = 0; p < (W.n_traces + 1) / 2; p += np) {
-        cj.push_back(w);
-        cp.push_back(p);
-      }
     }
     wavf_jobs.upload(jobs, stream);
-    wavf.cta_job.upload(cj, stream);
-    wavf.cta_trace0.upload(cp, stream);
-    wavf.n_cta = (int)cj.size();
-    wavf.nb = np;
-    wavf.smem = per_pair * np;
     upload_twiddles();
+    // candidates: blocks per SM and pairs per block (about a third of the
+    // SM's shared memory per block at three blocks)
+    struct Cand {
+      WaveletFn fn;
+      int np;
+    };
+    std::vector<Cand> cands;
+    auto pairs = [&](size_t budget) {
+      return (int)std::max<size_t>(1, std::min<size_t>(4, budget / per_pair));
+    };
+    if constexpr (sizeof(R) == sizeof(float)) {
+      cands.push_back(Cand{wavelet_fast<R, 2>, pairs(60000)});
+      cands.push_back(Cand{wavelet_fast<R, 3>, pairs(60000)});
+      cands.push_back(Cand{wavelet_fast<R, 3>, pairs(40000)});
+    } else {
+      cands.push_back(Cand{wavelet_fast<R, 1>, pairs(60000)});
+    }
+    auto launch_for = [&](TimeLaunch &L, int np) {
+      std::vector<int> cj, cp;
+      for (int w = 0; w < nw; ++w)
+        for (int p = 0; p < (plan.windows[w].n_traces + 1) / 2; p += np) {
+          cj.push_back(w);
+          cp.push_back(p);
+        }
+      L.cta_job.upload(cj, stream);
+      L.cta_trace0.upload(cp, stream);
+      L.n_cta = (int)cj.size();
+      L.nb = np;
+      L.smem = per_pair * np;
+    };
+    int pick = 0;
+    const char *force = std::getenv("AGD_GPU_WAVELET_VARIANT");
+    if (force != nullptr && force[0] != '\0') {
+      pick = std::max(0, std::min(std::atoi(force), (int)cands.size() - 1));
+    } else if (cands.size() > 1) {
+      pick = autotune_wavelet(cands.size(), [&](size_t v, TimeLaunch &L) {
+        launch_for(L, cands[v].np);
+        return cands[v].fn;
+      });
+    }
+    wav_candidates = (int)cands.size();
+    wav_pick = pick;
+    wav_fn = cands[pick].fn;
+    launch_for(wavf, cands[pick].np);
     wav_fast = true;
+  }
+
+  int wav_candidates = 0, wav_pick = -1;
+
+  // Times the wavelet candidates (both directions, three rounds, CUDA
+  // events), cached per device, precision, trace length and size class.
+  template <typename Make>
+  int autotune_wavelet(size_t n, Make make) {
+    long traces = 0;
+    int c_max = 0;
+    for (const WindowPlan &W : plan.windows) {
+      traces += W.n_traces;
+      c_max = std::max(c_max, W.C);
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    char key[96];
+    std::snprintf(key, sizeof key, "wav:%d:%d:%d:%d", dev, (int)sizeof(R), c_max,
+                  (int)std::log2((double)std::max(1L, traces)));
+    static std::mutex mu;
+    static std::map<std::string, int> cache;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      auto it = cache.find(key);
+      if (it != cache.end()) return it->second;
+    }
+    CK(cudaMemsetAsync(Y.get(), 0, Y.bytes(), stream));
+    CK(cudaMemsetAsync(rec_d.get(), 0, rec_d.bytes(), stream));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    std::vector<TimeLaunch> ls(n);
+    std::vector<WaveletFn> fns(n);
+    std::vector<float> best(n, 1e30f);
+    for (size_t v = 0; v < n; ++v) fns[v] = make(v, ls[v]);
+    for (int round = 0; round < 3; ++round)
+      for (size_t v = 0; v < n; ++v) {
+        const TimeLaunch &L = ls[v];
+        if (L.smem > (size_t)smem_max || L.n_cta == 0) continue;
+        auto run = [&] {
+          fns[v]<<<L.n_cta, kWavThreads, L.smem, stream>>>(
+              wavf_jobs.get(), L.cta_job.get(), L.cta_trace0.get(), L.nb, spectra.get(),
+              spec_off.get(), +1, nullptr);
+          fns[v]<<<L.n_cta, kWavThreads, L.smem, stream>>>(
+              wavf_jobs.get(), L.cta_job.get(), L.cta_trace0.get(), L.nb, spectra.get(),
+              spec_off.get(), -1, rec_d.get());
+          CK(cudaGetLastError());
+        };
+        run();
+        CK(cudaEventRecord(e0, stream));
+        run();
+        CK(cudaEventRecord(e1, stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        best[v] = std::min(best[v], ms);
+      }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const int pick = (int)(std::min_element(best.begin(), best.end()) - best.begin());
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = pick;
+    return pick;
   }
 
   // ---------------------------------------------------------------- set-up
@@ -1547,7 +1650,7 @@ class Engine {
   // the window traces (direction -1, prime-factor kernel only)
   void launch_wavelet_fast(int direction, const R *record) {
     if (!wavf.n_cta) return;
-    wavelet_fast<R><<<wavf.n_cta, kWavThreads, wavf.smem, stream>>>(
+    wav_fn<<<wavf.n_cta, kWavThreads, wavf.smem, stream>>>(
         wavf_jobs.get(), wavf.cta_job.get(), wavf.cta_trace0.get(), wavf.nb, spectra.get(),
         spec_off.get(), direction, record);
     CK(cudaGetLastError());
@@ -2061,6 +2164,8 @@ int agd_gpu_problem_info(agd_gpu_problem const *pb, long int *info) {
   info[17] = e.tgroups.empty() ? -1 : e.tgroups[0]->fwd_pick;
   info[18] = e.tgroups.empty() ? -1 : e.tgroups[0]->adj_pick;
   info[19] = e.tgroups.empty() ? 0 : (long)e.tgroups[0]->fwd_vars.size();
+  info[20] = e.wav_fast ? e.wav_pick : -1;
+  info[21] = e.wav_candidates;
   return 0;
 }
 

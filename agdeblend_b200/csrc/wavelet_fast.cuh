@@ -128,8 +128,10 @@ __device__ __forceinline__ Cx<R> spectrum_at(const Cx<R> *sp, int k, int N, bool
 // Each CTA transforms np_max pairs of traces of one window (fewer in the
 // window's last CTA).  direction +1: convolution in place on the traces;
 // -1: correlation of the traces gathered from `record`, written to y.
-template <typename R>
-__global__ void __launch_bounds__(kWavThreads, sizeof(R) == 4 ? 2 : 1)
+// MINB blocks per SM (the register budget of the 17-point DFTs decides
+// which is faster; the engine times the candidates).
+template <typename R, int MINB>
+__global__ void __launch_bounds__(kWavThreads, MINB)
     wavelet_fast(const WaveletFastJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
                  const int *__restrict__ cta_pair0, int np_max,
                  const Cx<R> *__restrict__ spectra, const long *__restrict__ spec_off,

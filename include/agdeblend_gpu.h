@@ -40,7 +40,7 @@ int agd_gpu_problem_create(int n_patches, int const *volumes, int const *n_dims,
 
 void agd_gpu_problem_destroy(agd_gpu_problem *problem);
 
-/* info (20 values): [0] windows, [1] model complex elements, [2] record
+/* info (22 values): [0] windows, [1] model complex elements, [2] record
  * samples, [3] window traces (all windows), [4] record segments, [5] mute
  * spans, [6] device bytes held, [7] blend contributions per forward,
  * [8] 1 if the shape-specialised kernels serve every window, 2 if they
@@ -51,7 +51,8 @@ void agd_gpu_problem_destroy(agd_gpu_problem *problem);
  * candidates, [14] kernels launched per iteration, [15] window classes on
  * the shape-specialised kernels, [16] windows on them, [17] and [18] the
  * time-kernel candidates picked for the first time group (-1 without
- * one), [19] its number of candidates. */
+ * one), [19] its number of candidates, [20] the wavelet-kernel candidate
+ * picked (-1 without the prime-factor kernel), [21] their number. */
 int agd_gpu_problem_info(agd_gpu_problem const *problem, long int *info);
 
 /* Step size 0.5 / max blend fold (reference get_stepsize, src/model.c:1230-1312). */

@@ -143,6 +143,35 @@ def test_wavelet_fast_vibroseis_length_2431():
     assert _check(sv, np.float32, 5)
 
 
+def test_every_wavelet_candidate_vs_oracle():
+    """Each wavelet-kernel candidate (blocks per SM, pairs per block) the
+    set-up timing may pick, on the 2431-sample traces."""
+    sv = _vibroseis_small(63)
+    probe = _problem(sv, np.float32)
+    n = int(probe.info[21])
+    probe.close()
+    assert n >= 1
+    old = os.environ.get("AGD_GPU_WAVELET_VARIANT")
+    try:
+        for v in range(n):
+            os.environ["AGD_GPU_WAVELET_VARIANT"] = str(v)
+            prob = _problem(sv, np.float32)
+            assert prob.info[20] == v
+            plan = _plan(sv)
+            rec = np.random.default_rng(v).standard_normal(prob.record_size)
+            O.apply_mute(plan.cfg, rec)
+            x_ref = _interleave(O.model_to_flat(O.adjoint(plan, rec)))
+            assert rel_l2(prob.adjoint(rec), x_ref) <= 1e-5
+            y_ref = O.forward(plan, O.flat_to_model(plan, x_ref[0::2] + 1j * x_ref[1::2]))
+            assert rel_l2(prob.forward(x_ref), y_ref) <= 1e-5
+            prob.close()
+    finally:
+        if old is None:
+            os.environ.pop("AGD_GPU_WAVELET_VARIANT", None)
+        else:
+            os.environ["AGD_GPU_WAVELET_VARIANT"] = old
+
+
 def test_wavelet_fast_solve_matches_oracle():
     sv = _vibroseis_small(62)
     prob = _problem(sv, np.float32)
