@@ -867,6 +867,20 @@ class Engine {
                                             2 * (size_t)NB * 2 * H * sizeof(R)});
   }
 
+  // fused candidates (fast.cuh time_fwd_fused / time_adj_fused), 256 / M1
+  // traces per block
+  template <int M1, int M2, int LSB, int LSW, int MB>
+  static void add_time_fused(TimeGroup &g) {
+    constexpr int M = M1 * M2;
+    constexpr int H = 4 * M / 5;
+    constexpr int NB = kThreads / M1;
+    g.fwd_vars.push_back(TimeFwdVariant{time_fwd_fused<R, M1, M2, LSB, LSW, MB>, NB,
+                                        ((size_t)2 * NB * LSB + (size_t)NB * LSW) * sizeof(C)});
+    g.adj_vars.push_back(TimeAdjVariant{time_adj_fused<R, M1, M2, LSW, MB>, NB,
+                                        (size_t)NB * LSW * sizeof(C) +
+                                            2 * (size_t)NB * 2 * H * sizeof(R)});
+  }
+
   static bool time_case(const WindowPlan &W, TimeGroup &g) {
     g.fwd_vars.clear();
     g.adj_vars.clear();
@@ -875,12 +889,16 @@ class Engine {
       if constexpr (sizeof(R) == sizeof(float)) {
         add_time<16, 10, 32, 170, 2>(g);
         add_time<16, 10, 16, 170, 4>(g);
+        add_time_fused<16, 10, 170, 186, 3>(g);
+        add_time_fused<16, 10, 170, 186, 2>(g);
       }
     } else if (W.Pt == 160) {
       add_time<8, 10, 32, 81, 1>(g);
       if constexpr (sizeof(R) == sizeof(float)) {
         add_time<8, 10, 32, 90, 2>(g);
         add_time<8, 10, 16, 90, 4>(g);
+        add_time_fused<8, 10, 90, 90, 3>(g);
+        add_time_fused<8, 10, 90, 90, 2>(g);
       }
     } else {
       return false;

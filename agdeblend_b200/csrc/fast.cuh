@@ -1058,4 +1058,282 @@ __global__ void __launch_bounds__(kThreads, MINB)
   }
 }
 
+// ------------------------------------------------------------ fused time kernels
+
+// Hermitian combine of the c2r input (bins X of one trace, F = M + 1):
+// Z_k = (X_k + conj X_{M-k}) + i e^{+2 pi i k / Pt} (X_k - conj X_{M-k}),
+// the imaginary parts of X_0 and X_M dropped (c2r ignores them).
+template <typename R, int M>
+__device__ __forceinline__ Cx<R> combine_bin(const Cx<R> *x, int k, const Cx<R> *tw2M) {
+  using C = Cx<R>;
+  C a = x[k];
+  C b = x[M - k];
+  if (k == 0) {
+    a.y = (R)0;
+    b.y = (R)0;
+  }
+  const C bc = cmake<C>(b.x, -b.y);
+  const C e = cadd(a, bc);
+  const C d = csub(a, bc);
+  const C o = cmul(d, tw_at<true>(tw2M, k));
+  return cmake<C>(e.x - o.y, e.y + o.x);
+}
+
+// Forward time axis, fused: as time_fwd_fast, but the Hermitian combine is
+// done while loading the first four-step pass, and the second pass keeps
+// its outputs in registers: thread (trace i, k1) holds the samples
+// j = 2 (k1 + M1 k2) + c, and as H / 2 = 2 M / 5 = 4 M1 (M2 = 10), the
+// samples j < H (k2 < 4) and their successors j + H (k2 + 4) belong to the
+// same thread, so taper, overlap-add and the one-hop carry stay in
+// registers.  Two barriers per time window.  NB = 256 / M1 traces per block;
+// M2 = 10.  Bins lines LSB apart, work groups M2 + 1 apart within lines LSW
+// apart (both 10 mod 16, so the passes hit distinct banks).
+template <typename R, int M1, int M2, int LSB, int LSW, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
+    time_fwd_fused(const TimeJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
+                   const int *__restrict__ cta_trace0) {
+  using C = Cx<R>;
+  constexpr int M = M1 * M2;
+  constexpr int F = M + 1;
+  constexpr int H = 4 * M / 5;
+  constexpr int NB = kThreads / M1;
+  constexpr int G = M2 + 1;  // work group stride
+  static_assert(M2 == 10 && NB * M1 == kThreads, "fused time kernel shape");
+  static_assert(LSB >= F && LSW >= M1 * G, "line strides");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ C twM[M];
+  __shared__ C tw2M[2 * M];
+  load_twiddles<R, M>(twM);
+  load_twiddles<R, 2 * M>(tw2M);
+  const TimeJob<R> job = jobs[cta_job[blockIdx.x]];
+  const int t0 = cta_trace0[blockIdx.x];
+  const int nb = min(NB, job.n_traces - t0);
+  const long ntr = job.n_traces;
+  C *stage[2] = {reinterpret_cast<C *>(smem_raw), reinterpret_cast<C *>(smem_raw) + NB * LSB};
+  C *work = stage[1] + NB * LSB;
+  // this thread's trace and second-pass line, fixed over the time windows
+  const int ti = threadIdx.x / M1;
+  const int k1 = threadIdx.x - ti * M1;
+  const bool live = ti < nb;
+  const R sc = live ? job.space_scale[t0 + ti] : (R)0;
+  R tap[8][2];  // tapers of the samples j = 2 (k1 + M1 k2) + c, k2 < 8
+#pragma unroll
+  for (int k2 = 0; k2 < 8; ++k2)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) tap[k2][c] = job.time_taper[2 * (k1 + M1 * k2) + c];
+  R carry[4][2];
+#pragma unroll
+  for (int k2 = 0; k2 < 4; ++k2) carry[k2][0] = carry[k2][1] = (R)0;
+  R *yrow = job.y + (long)(t0 + (live ? ti : 0)) * job.C;
+  auto issue = [&](int t, C *buf) {
+    const C *zt = job.z + (long)t * F * ntr + t0;
+    for (int idx = threadIdx.x; idx < NB * F; idx += kThreads) {
+      const int f = idx / NB;
+      const int i = idx - f * NB;
+      if (i < nb) cp_async<sizeof(C)>(buf + i * LSB + f, zt + f * ntr + i);
+    }
+  };
+  issue(0, stage[0]);
+  cp_async_commit();
+  for (int t = 0; t < job.T; ++t) {
+    if (t + 1 < job.T) issue(t + 1, stage[(t + 1) & 1]);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const C *bins = stage[t & 1];
+    // first pass: lines (trace i, n2) over n1, combined bins as input
+    for (int it = threadIdx.x; it < NB * M2; it += kThreads) {
+      const int i = it / M2;
+      const int n2 = it - i * M2;
+      C v[M1];
+      if (i < nb) {
+#pragma unroll
+        for (int n1 = 0; n1 < M1; ++n1) v[n1] = combine_bin<R, M>(bins + i * LSB, M2 * n1 + n2, tw2M);
+      } else {
+#pragma unroll
+        for (int n1 = 0; n1 < M1; ++n1) v[n1] = cmake<C>((R)0, (R)0);
+      }
+      dft<R, M1, true>(v);
+      C *w = work + i * LSW + n2;
+#pragma unroll
+      for (int q = 0; q < M1; ++q)
+        w[G * q] = (q == 0) ? v[0] : cmul(v[q], tw_at<true>(twM, (n2 * q) % M));
+    }
+    __syncthreads();
+    // second pass: line k1 of trace ti; outputs X[k1 + M1 k2] = samples
+    // 2 (k1 + M1 k2) + {0, 1}
+    C v[M2];
+    const C *w = work + ti * LSW + G * k1;
+#pragma unroll
+    for (int n2 = 0; n2 < M2; ++n2) v[n2] = w[n2];
+    dft<R, M2, true>(v);
+    if (live) {
+      R *yt = yrow + t * H;
+#pragma unroll
+      for (int k2 = 0; k2 < 4; ++k2) {
+        const int j = 2 * (k1 + M1 * k2);
+        yt[j] = carry[k2][0] + (v[k2].x * sc) * tap[k2][0];
+        yt[j + 1] = carry[k2][1] + (v[k2].y * sc) * tap[k2][1];
+      }
+#pragma unroll
+      for (int k2 = 0; k2 < 4; ++k2) {
+        carry[k2][0] = (v[k2 + 4].x * sc) * tap[k2 + 4][0];
+        carry[k2][1] = (v[k2 + 4].y * sc) * tap[k2 + 4][1];
+      }
+    }
+  }
+  // last half window, then zeros up to C
+  if (live) {
+    R *yt = yrow + job.T * H;
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) {
+      const int j = 2 * (k1 + M1 * k2);
+      yt[j] = carry[k2][0];
+      yt[j + 1] = carry[k2][1];
+    }
+  }
+  const int tail = job.C - (job.T + 1) * H;
+  for (int idx = threadIdx.x; idx < nb * tail; idx += kThreads) {
+    const int i = idx / tail;
+    const int j = idx - i * tail;
+    job.y[(long)(t0 + i) * job.C + (job.T + 1) * H + j] = (R)0;
+  }
+}
+
+// Adjoint time axis, fused: as time_adj_fast, but the scaling, tapering and
+// packing of the raw samples is done while loading the first four-step
+// pass, and the second pass writes its outputs back into its own group of
+// the work buffer (no second buffer).  Three barriers per time window.
+template <typename R, int M1, int M2, int LSW, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
+    time_adj_fused(const TimeJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
+                   const int *__restrict__ cta_trace0, const R *__restrict__ record,
+                   int from_record) {
+  using C = Cx<R>;
+  constexpr int M = M1 * M2;
+  constexpr int F = M + 1;
+  constexpr int H = 4 * M / 5;
+  constexpr int LT = 2 * H;
+  constexpr int NB = kThreads / M1;
+  constexpr int G = M2 + 1;
+  static_assert(M2 == 10 && NB * M1 == kThreads, "fused time kernel shape");
+  static_assert(LSW >= M1 * G, "line stride");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ C twM[M];
+  __shared__ C tw2M[2 * M];
+  __shared__ long span_base[NB];
+  __shared__ int span_lo[NB], span_hi[NB];
+  __shared__ R scale[NB];
+  __shared__ R taper[LT];
+  load_twiddles<R, M>(twM);
+  load_twiddles<R, 2 * M>(tw2M);
+  const TimeJob<R> job = jobs[cta_job[blockIdx.x]];
+  const int t0 = cta_trace0[blockIdx.x];
+  const int nb = min(NB, job.n_traces - t0);
+  const long ntr = job.n_traces;
+  for (int j = threadIdx.x; j < LT; j += kThreads) taper[j] = job.time_taper[j];
+  for (int i = threadIdx.x; i < NB; i += kThreads) {
+    const int tr = t0 + i;
+    span_lo[i] = 0;
+    span_hi[i] = 0;
+    span_base[i] = 0;
+    scale[i] = (R)0;
+    if (i >= nb) continue;
+    scale[i] = job.space_scale[tr];
+    if (from_record) {
+      const long rec = job.blend_rec[tr];
+      const int ts = job.blend_ts[tr];
+      span_base[i] = rec - ts;
+      span_lo[i] = rec >= 0 ? ts : 0;
+      span_hi[i] = rec >= 0 ? ts + job.blend_n[tr] : 0;
+    } else {
+      span_base[i] = (long)tr * job.C;
+      span_hi[i] = job.C;
+    }
+  }
+  __syncthreads();
+  const R *src_base = from_record ? record : job.y;
+  C *work = reinterpret_cast<C *>(smem_raw);
+  R *raw[2] = {reinterpret_cast<R *>(work + NB * LSW),
+               reinterpret_cast<R *>(work + NB * LSW) + NB * LT};
+  auto issue = [&](int t, R *rb) {
+    for (int g = threadIdx.x; g < NB * (LT / 4); g += kThreads) {
+      const int i = g / (LT / 4);
+      const int j0 = 4 * (g - i * (LT / 4));
+      const int s0 = t * H + j0;
+      const int lo = span_lo[i];
+      const int hi = span_hi[i];
+      const R *src = src_base + span_base[i] + s0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const bool valid = s0 + q >= lo && s0 + q < hi;
+        cp_async<sizeof(R)>(rb + i * LT + j0 + q, valid ? src + q : src_base, valid);
+      }
+    }
+  };
+  const int ti = threadIdx.x / M1;
+  const int k1 = threadIdx.x - ti * M1;
+  issue(0, raw[0]);
+  cp_async_commit();
+  for (int t = 0; t < job.T; ++t) {
+    if (t + 1 < job.T) issue(t + 1, raw[(t + 1) & 1]);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const R *rb = raw[t & 1];
+    // first pass: packed, tapered samples (2 m, 2 m + 1) as input
+    for (int it = threadIdx.x; it < NB * M2; it += kThreads) {
+      const int i = it / M2;
+      const int n2 = it - i * M2;
+      const R sc = scale[i];
+      C v[M1];
+#pragma unroll
+      for (int n1 = 0; n1 < M1; ++n1) {
+        const int j = 2 * (M2 * n1 + n2);
+        R v0 = (R)0, v1 = (R)0;
+        if (j < LT) {
+          v0 = (rb[i * LT + j] * sc) * taper[j];
+          v1 = (rb[i * LT + j + 1] * sc) * taper[j + 1];
+        }
+        v[n1] = cmake<C>(v0, v1);
+      }
+      dft<R, M1, false>(v);
+      C *w = work + i * LSW + n2;
+#pragma unroll
+      for (int q = 0; q < M1; ++q)
+        w[G * q] = (q == 0) ? v[0] : cmul(v[q], tw_at<false>(twM, (n2 * q) % M));
+    }
+    __syncthreads();
+    {  // second pass, in place in this thread's group: Z[k1 + M1 k2]
+      C v[M2];
+      C *w = work + ti * LSW + G * k1;
+#pragma unroll
+      for (int n2 = 0; n2 < M2; ++n2) v[n2] = w[n2];
+      dft<R, M2, false>(v);
+#pragma unroll
+      for (int k2 = 0; k2 < M2; ++k2) w[k2] = v[k2];
+    }
+    __syncthreads();
+    // split: X_k = (Z_k + conj Z_{M-k}) / 2 - i e^{-2 pi i k / Pt} (Z_k - conj Z_{M-k}) / 2
+    C *zt = job.z + (long)t * F * ntr + t0;
+    for (int idx = threadIdx.x; idx < NB * F; idx += kThreads) {
+      const int f = idx / NB;
+      const int i = idx - f * NB;
+      if (i < nb) {
+        const C *b = work + i * LSW;
+        const int fa = f % M;
+        const int fb = (M - f) % M;
+        const C zk = b[G * (fa % M1) + fa / M1];
+        const C zm = b[G * (fb % M1) + fb / M1];
+        const C zc = cmake<C>(zm.x, -zm.y);
+        const C e = cmake<C>((R)0.5 * (zk.x + zc.x), (R)0.5 * (zk.y + zc.y));
+        const C o = cmake<C>((R)0.5 * (zk.y - zc.y), (R)-0.5 * (zk.x - zc.x));
+        C x = cadd(e, cmul(tw_at<false>(tw2M, f), o));
+        if (f >= 1 && f <= M - 1) x = cmake<C>(x.x * (R)2, x.y * (R)2);
+        zt[f * ntr + i] = x;
+      }
+    }
+  }
+}
+
 }  // namespace agd
