@@ -439,50 +439,76 @@ __global__ void __launch_bounds__(kThreads)
 // ------------------------------------------------------------ blending
 
 // Ordered gather into the blended record.  Block b owns record samples
-// [b*chunk, (b+1)*chunk) and visits the contributions overlapping its chunk
-// in the reference's order (window, then trace), so sums are formed in the
-// same order as its serial blend loops (src/blend.c:936-1027,1155-1260).
+// [b*chunk, (b+1)*chunk) (chunk <= 4 * blockDim) and visits the
+// contributions overlapping its chunk in the reference's order (window, then
+// trace), so sums are formed in the same order as its serial blend loops
+// (src/blend.c:936-1027,1155-1260).  The contribution list is staged in
+// shared memory in tiles of kGatherTile; each thread keeps the sums of its
+// samples in registers across the tiles.
+constexpr int kGatherTile = 256;
+constexpr int kGatherSpt = 4;  // samples per thread at most
+
 template <typename R>
 __global__ void __launch_bounds__(kThreads)
     blend_gather(const Contrib *__restrict__ contrib, const long *__restrict__ chunk_ptr,
                  int chunk, long record_size, const R *__restrict__ src, R *out,
                  int mode, const uint8_t *__restrict__ mute, const R *__restrict__ d,
                  const R *__restrict__ taper, int taper_len, double *sumsq) {
+  __shared__ Contrib tile[kGatherTile];
   const long c0 = (long)blockIdx.x * chunk;
   const long b0 = chunk_ptr[blockIdx.x];
   const long b1 = chunk_ptr[blockIdx.x + 1];
-  double local = 0.0;
-  for (int k = threadIdx.x; k < chunk; k += blockDim.x) {
-    const long s = c0 + k;
-    if (s >= record_size) break;
-    R acc = (R)0;
-    R cnt = (R)0;
-    for (long c = b0; c < b1; ++c) {
-      const Contrib cb = contrib[c];
-      const long off = s - cb.rec;
-      if (off < 0 || off >= cb.n) continue;
-      const R v = src[cb.src + off];
-      if (mode == kGatherOverwrite) {
-        acc = v;
-      } else if (mode == kGatherMean) {
-        R w = (R)1;
-        if (taper_len > 1) {
-          const int t = (int)off;
-          const int to_end = cb.n - 1 - t;
-          const int edge = t < to_end ? t : to_end;
-          if (edge < taper_len) w = taper[edge];
+  R acc[kGatherSpt], cnt[kGatherSpt];
+#pragma unroll
+  for (int q = 0; q < kGatherSpt; ++q) acc[q] = cnt[q] = (R)0;
+  for (long base = b0; base < b1; base += kGatherTile) {
+    const int nt = (int)min((long)kGatherTile, b1 - base);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nt; i += blockDim.x) tile[i] = contrib[base + i];
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kGatherSpt; ++q) {
+      const int k = threadIdx.x + q * blockDim.x;
+      const long s = c0 + k;
+      if (k >= chunk || s >= record_size) continue;
+      R a = acc[q], w_sum = cnt[q];
+      for (int c = 0; c < nt; ++c) {
+        const Contrib cb = tile[c];
+        const long off = s - cb.rec;
+        if (off < 0 || off >= cb.n) continue;
+        const R v = src[cb.src + off];
+        if (mode == kGatherOverwrite) {
+          a = v;
+        } else if (mode == kGatherMean) {
+          R w = (R)1;
+          if (taper_len > 1) {
+            const int t = (int)off;
+            const int to_end = cb.n - 1 - t;
+            const int edge = t < to_end ? t : to_end;
+            if (edge < taper_len) w = taper[edge];
+          }
+          a += v * w;
+          w_sum += w;
+        } else {
+          a += v;
         }
-        acc += v * w;
-        cnt += w;
-      } else {
-        acc += v;
       }
+      acc[q] = a;
+      cnt[q] = w_sum;
     }
-    if (mode == kGatherMean && cnt > (R)0) acc /= cnt;
-    if (mode == kGatherResidual) acc = acc - d[s];
-    if (mute != nullptr && mute[s]) acc = (R)0;
-    out[s] = acc;
-    local += (double)acc * (double)acc;
+  }
+  double local = 0.0;
+#pragma unroll
+  for (int q = 0; q < kGatherSpt; ++q) {
+    const int k = threadIdx.x + q * blockDim.x;
+    const long s = c0 + k;
+    if (k >= chunk || s >= record_size) continue;
+    R a = acc[q];
+    if (mode == kGatherMean && cnt[q] > (R)0) a /= cnt[q];
+    if (mode == kGatherResidual) a = a - d[s];
+    if (mute != nullptr && mute[s]) a = (R)0;
+    out[s] = a;
+    local += (double)a * (double)a;
   }
   if (sumsq != nullptr) {
     __shared__ double red[32];
