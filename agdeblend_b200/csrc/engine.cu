@@ -876,9 +876,11 @@ class Engine {
     constexpr int NB = kThreads / M1;
     g.fwd_vars.push_back(TimeFwdVariant{time_fwd_fused<R, M1, M2, LSB, LSW, MB>, NB,
                                         ((size_t)2 * NB * LSB + (size_t)NB * LSW) * sizeof(C)});
+    constexpr int LT = 2 * H;
+    constexpr int LTP = LT + ((20 - LT % 32) + 32) % 32;  // as time_adj_fused
     g.adj_vars.push_back(TimeAdjVariant{time_adj_fused<R, M1, M2, LSW, MB>, NB,
                                         (size_t)NB * LSW * sizeof(C) +
-                                            2 * (size_t)NB * 2 * H * sizeof(R)});
+                                            2 * (size_t)NB * LTP * sizeof(R)});
   }
 
   static bool time_case(const WindowPlan &W, TimeGroup &g) {

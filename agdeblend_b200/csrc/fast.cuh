@@ -1216,6 +1216,10 @@ __global__ void __launch_bounds__(kThreads, MINB)
   constexpr int LT = 2 * H;
   constexpr int NB = kThreads / M1;
   constexpr int G = M2 + 1;
+  // raw sample rows padded to 20 mod 32 floats: the first pass reads sample
+  // pairs as 8-byte loads, and a half-warp's pairs then fall in distinct
+  // banks
+  constexpr int LTP = LT + ((20 - LT % 32) + 32) % 32;
   static_assert(M2 == 10 && NB * M1 == kThreads, "fused time kernel shape");
   static_assert(LSW >= M1 * G, "line stride");
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1255,7 +1259,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
   const R *src_base = from_record ? record : job.y;
   C *work = reinterpret_cast<C *>(smem_raw);
   R *raw[2] = {reinterpret_cast<R *>(work + NB * LSW),
-               reinterpret_cast<R *>(work + NB * LSW) + NB * LT};
+               reinterpret_cast<R *>(work + NB * LSW) + NB * LTP};
   auto issue = [&](int t, R *rb) {
     for (int g = threadIdx.x; g < NB * (LT / 4); g += kThreads) {
       const int i = g / (LT / 4);
@@ -1267,7 +1271,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const bool valid = s0 + q >= lo && s0 + q < hi;
-        cp_async<sizeof(R)>(rb + i * LT + j0 + q, valid ? src + q : src_base, valid);
+        cp_async<sizeof(R)>(rb + i * LTP + j0 + q, valid ? src + q : src_base, valid);
       }
     }
   };
@@ -1292,8 +1296,9 @@ __global__ void __launch_bounds__(kThreads, MINB)
         const int j = 2 * (M2 * n1 + n2);
         R v0 = (R)0, v1 = (R)0;
         if (j < LT) {
-          v0 = (rb[i * LT + j] * sc) * taper[j];
-          v1 = (rb[i * LT + j + 1] * sc) * taper[j + 1];
+          const Cx<R> pr = *reinterpret_cast<const Cx<R> *>(rb + i * LTP + j);
+          v0 = (pr.x * sc) * taper[j];
+          v1 = (pr.y * sc) * taper[j + 1];
         }
         v[n1] = cmake<C>(v0, v1);
       }
