@@ -66,6 +66,8 @@ def _bind_extension(lib, dtype):
     lib.agd_gpu_blend_input.argtypes = [c_void_p, POINTER(rp), rp]
     lib.agd_gpu_set_output.argtypes = [c_void_p, rp, POINTER(rp)]
     lib.agd_gpu_solve.argtypes = [c_void_p, rc, c_int, c_int, POINTER(rp)]
+    lib.agd_gpu_solve_range.argtypes = [c_void_p, rc, c_int, c_int, c_int, c_int, rp, rp,
+                                        POINTER(rp)]
     lib.agd_gpu_time_iterations.argtypes = [c_void_p, POINTER(rp), rc, c_int, c_int, c_int,
                                             POINTER(c_double)]
     lib.agd_gpu_profile_iteration.argtypes = [c_void_p, rc, POINTER(c_double)]
@@ -82,6 +84,7 @@ def _bind_extension(lib, dtype):
     for name in ("agd_gpu_problem_info", "agd_gpu_stepsize", "agd_gpu_forward",
                  "agd_gpu_adjoint", "agd_gpu_blend_input", "agd_gpu_set_output",
                  "agd_gpu_solve", "agd_gpu_time_iterations", "agd_plan_export",
+                 "agd_gpu_solve_range",
                  "agd_gpu_batch_create", "agd_gpu_problem_steps"):
         getattr(lib, name).restype = c_int
 
@@ -323,6 +326,20 @@ class Problem:
         self._check(self.lib.agd_gpu_solve(self.h, initial_factor, n_its, print_freq, ptrs),
                     "solve")
         return [k.reshape(s) for k, s in zip(keep, self.shapes)]
+
+    def solve_range(self, data, initial_factor: float, n_its: int, it_begin: int, it_end: int,
+                    model_in=None, print_freq: int = 0):
+        """Iterations [it_begin, it_end) of the n_its schedule (checkpoint /
+        resume).  Returns (output patches, model after iteration it_end - 1)."""
+        ptrs, keep = self._data_ptrs(data, writable=True)
+        m_in = None
+        if model_in is not None:
+            m_in = np.ascontiguousarray(model_in, self.dtype)
+        m_out = np.zeros(2 * self.model_size, self.dtype)
+        self._check(self.lib.agd_gpu_solve_range(
+            self.h, initial_factor, n_its, it_begin, it_end, print_freq,
+            self._p(m_in) if m_in is not None else None, self._p(m_out), ptrs), "solve_range")
+        return [k.reshape(s) for k, s in zip(keep, self.shapes)], m_out
 
     def time_iterations(self, data, initial_factor: float, n_its: int, warmup: int,
                         steps: int) -> np.ndarray:

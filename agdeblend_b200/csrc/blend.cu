@@ -79,6 +79,12 @@ struct Dev {
   }
 };
 
+// cudaMalloc, or a reported failure under the test hook AGD_GPU_FAIL_ALLOC
+cudaError_t dev_alloc(void **p, size_t bytes) {
+  if (agd::injected_alloc_failure()) return cudaErrorMemoryAllocation;
+  return cudaMalloc(p, bytes);
+}
+
 #define BCK(x)                                                                \
   do {                                                                        \
     cudaError_t e_ = (x);                                                     \
@@ -173,18 +179,18 @@ extern "C" int agd_blend(int n_patches, int const *n_traces, int const *n_times,
   cudaStream_t s = nullptr;
   Dev d_in, d_rec, d_flat, d_ptr, d_mute, d_taper, d_out, d_orec, d_ots, d_on, d_odst, d_ont;
   BCK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  BCK(cudaMalloc(&d_in.p, std::max<long>(in_size, 1) * sizeof(real)));
-  BCK(cudaMalloc(&d_rec.p, std::max<long>(R, 1) * sizeof(real)));
-  BCK(cudaMalloc(&d_flat.p, std::max<size_t>(flat.size(), 1) * sizeof(agd::Contrib)));
-  BCK(cudaMalloc(&d_ptr.p, ptr.size() * sizeof(long)));
-  BCK(cudaMalloc(&d_mute.p, std::max<long>(R, 1)));
-  BCK(cudaMalloc(&d_taper.p, std::max<size_t>(taper.size(), 1) * sizeof(real)));
-  BCK(cudaMalloc(&d_out.p, std::max<long>(out_size, 1) * sizeof(real)));
-  BCK(cudaMalloc(&d_orec.p, std::max<long>(n_out_tr, 1) * sizeof(long)));
-  BCK(cudaMalloc(&d_ots.p, std::max<long>(n_out_tr, 1) * sizeof(int)));
-  BCK(cudaMalloc(&d_on.p, std::max<long>(n_out_tr, 1) * sizeof(int)));
-  BCK(cudaMalloc(&d_odst.p, std::max<long>(n_out_tr, 1) * sizeof(long)));
-  BCK(cudaMalloc(&d_ont.p, std::max<long>(n_out_tr, 1) * sizeof(int)));
+  BCK(dev_alloc(&d_in.p, std::max<long>(in_size, 1) * sizeof(real)));
+  BCK(dev_alloc(&d_rec.p, std::max<long>(R, 1) * sizeof(real)));
+  BCK(dev_alloc(&d_flat.p, std::max<size_t>(flat.size(), 1) * sizeof(agd::Contrib)));
+  BCK(dev_alloc(&d_ptr.p, ptr.size() * sizeof(long)));
+  BCK(dev_alloc(&d_mute.p, std::max<long>(R, 1)));
+  BCK(dev_alloc(&d_taper.p, std::max<size_t>(taper.size(), 1) * sizeof(real)));
+  BCK(dev_alloc(&d_out.p, std::max<long>(out_size, 1) * sizeof(real)));
+  BCK(dev_alloc(&d_orec.p, std::max<long>(n_out_tr, 1) * sizeof(long)));
+  BCK(dev_alloc(&d_ots.p, std::max<long>(n_out_tr, 1) * sizeof(int)));
+  BCK(dev_alloc(&d_on.p, std::max<long>(n_out_tr, 1) * sizeof(int)));
+  BCK(dev_alloc(&d_odst.p, std::max<long>(n_out_tr, 1) * sizeof(long)));
+  BCK(dev_alloc(&d_ont.p, std::max<long>(n_out_tr, 1) * sizeof(int)));
   for (int p = 0; p < n_patches; ++p)
     BCK(cudaMemcpyAsync((real *)d_in.p + in_off[p], data[p],
                         (size_t)n_traces[p] * n_times[p] * sizeof(real), cudaMemcpyHostToDevice,

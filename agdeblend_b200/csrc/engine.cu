@@ -49,6 +49,7 @@ static void check(cudaError_t e, const char *what) {
 class DevicePool {
  public:
   static void *take(size_t bytes) {
+    if (injected_alloc_failure()) throw DeviceError("injected device allocation failure");
     int dev = 0;
     CK(cudaGetDevice(&dev));
     if (enabled()) {
@@ -180,6 +181,8 @@ class DevArray {
   ~DevArray() { release(); }
   void alloc(size_t n) {
     release();
+    if (n && injected_alloc_failure())
+      throw DeviceError("injected device allocation failure");
     if (n) CK(cudaMalloc(reinterpret_cast<void **>(&p_), n * sizeof(T)));
     n_ = n;
   }
@@ -1983,20 +1986,45 @@ class Engine {
   // the solver of agd_deblend (src/agdeblend.c:584-633); iterations replay a
   // captured CUDA graph unless residuals are printed
   void solve(R initial_factor, int n_its, int print_freq) {
+    solve_range(initial_factor, n_its, 0, n_its, print_freq, nullptr, nullptr);
+  }
+
+  // Iterations [begin, end) of the n_its schedule, for checkpoint / resume
+  // and warm starts.  The whole solver state is the model and the iteration
+  // number: the thresholds follow from lambda_0 of the initial step, which
+  // is recomputed (it depends on the data only).  begin = 0 starts from the
+  // initial step like solve(); begin > 0 starts from model_in, the model
+  // after iteration begin - 1 (reference layout).  model_out, if given,
+  // receives the model after iteration end - 1, and the patch data receive
+  // that model's output.
+  void solve_range(R initial_factor, int n_its, int begin, int end, int print_freq,
+                   const R *model_in, R *model_out) {
     start_schedule(initial_factor, n_its, std::max(1, n_its - 1));
+    int first = 1;
+    if (begin > 0) {
+      model_from_ref(model_in);
+      const int counter = begin - 1;  // iteration `begin` uses table row begin - 1
+      CK(cudaMemcpyAsync(lamb_counter.get(), &counter, sizeof(int), cudaMemcpyHostToDevice,
+                         stream));
+      CK(cudaStreamSynchronize(stream));
+      first = begin;
+    }
     if (print_freq > 0) {
-      const double r = record_norm(rec_d.get());
-      std::printf("Iteration 0 Residual %f\n", r);
-      for (int it = 1; it < n_its; ++it) {
+      if (begin == 0) {
+        const double r = record_norm(rec_d.get());
+        std::printf("Iteration 0 Residual %f\n", r);
+      }
+      for (int it = first; it < end; ++it) {
         const bool print_residual = it % print_freq == 0;
         iteration_body(print_residual);
         if (print_residual)
           std::printf("Iteration %d Residual %f\n", it, std::sqrt(read_dscalar()));
       }
-    } else if (n_its > 1) {
+    } else if (end > first) {
       capture_iteration();
-      for (int it = 1; it < n_its; ++it) replay_iteration();
+      for (int it = first; it < end; ++it) replay_iteration();
     }
+    if (model_out != nullptr) model_to_ref(X.get(), model_out);
     output();
   }
 
@@ -2265,6 +2293,27 @@ int agd_gpu_solve(agd_gpu_problem *pb, AGD_TYPE initial_factor, int n_its, int p
     e.upload_data(data);
     pb->input_blend();
     e.solve(initial_factor, n_its, print_freq);
+    e.download_data(data);
+    return 0;
+  });
+}
+
+int agd_gpu_solve_range(agd_gpu_problem *pb, AGD_TYPE initial_factor, int n_its, int it_begin,
+                        int it_end, int print_freq, AGD_TYPE const *model_in,
+                        AGD_TYPE *model_out, AGD_TYPE *const *data) {
+  if (pb == nullptr || data == nullptr) return 1;
+  if (n_its <= 0 || it_begin < 0 || it_end < it_begin || it_end > n_its ||
+      (it_begin > 0 && model_in == nullptr)) {
+    std::fprintf(stderr,
+                 "ERROR: need 0 <= it_begin <= it_end <= n_its, n_its > 0, and a model to "
+                 "resume from when it_begin > 0\nERROR in agd_gpu_solve_range\n");
+    return 1;
+  }
+  return guarded("agd_gpu_solve_range", [&] {
+    agd::EngineR &e = *pb->eng;
+    e.upload_data(data);
+    pb->input_blend();
+    e.solve_range(initial_factor, n_its, it_begin, it_end, print_freq, model_in, model_out);
     e.download_data(data);
     return 0;
   });

@@ -6,7 +6,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
+#include <mutex>
 #include <set>
+#include <string>
 
 namespace agd {
 
@@ -733,6 +736,24 @@ int build_batch_plan(const std::vector<ProblemArgs> &args, Plan &out) {
     out.model_size += sub.model_size;
   }
   return 0;
+}
+
+}  // namespace agd
+
+namespace agd {
+
+bool injected_alloc_failure() {
+  const char *env = std::getenv("AGD_GPU_FAIL_ALLOC");
+  if (env == nullptr || env[0] == '\0') return false;
+  static std::mutex mu;
+  static std::string last;
+  static long count = 0;
+  std::lock_guard<std::mutex> g(mu);
+  if (last != env) {
+    last = env;
+    count = 0;
+  }
+  return ++count == std::atol(env);
 }
 
 }  // namespace agd

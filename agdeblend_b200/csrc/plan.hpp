@@ -151,6 +151,13 @@ std::vector<std::complex<double>> wavelet_spectrum(const real *w, int len, int n
 // Hann taper (set_taper_window, src/fk.c:28-73).
 std::vector<real> taper_window(int length, int left, int right);
 
+// Test hook for the error paths: with AGD_GPU_FAIL_ALLOC=n in the
+// environment, the n-th device allocation counted from when the variable was
+// set (or last changed) reports failure, so tests can walk every allocation
+// of a call and check that the call returns 1 and releases what it held,
+// without any fault on the GPU.
+bool injected_alloc_failure();
+
 // lambda schedule constants (src/agdeblend.c:526-533) in AGD_TYPE.
 struct Schedule {
   real decay;

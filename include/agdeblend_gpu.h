@@ -79,6 +79,19 @@ int agd_gpu_set_output(agd_gpu_problem *problem, AGD_TYPE const *model,
 int agd_gpu_solve(agd_gpu_problem *problem, AGD_TYPE initial_factor, int n_its,
                   int print_freq, AGD_TYPE *const *data);
 
+/* Checkpoint / resume (no counterpart in the reference, which keeps the
+ * solver state inside agd_deblend): runs iterations [it_begin, it_end) of
+ * the n_its-iteration schedule of agd_gpu_solve.  it_begin = 0 starts from
+ * the initial step; it_begin > 0 starts from model_in, the model after
+ * iteration it_begin - 1 (layout as agd_gpu_forward).  model_out (may be
+ * NULL) receives the model after iteration it_end - 1, and `data` the
+ * output of that model.  The thresholds are recomputed from the data, so
+ * stopping after iteration k and resuming from model_out with it_begin = k
+ * + 1 gives agd_gpu_solve's result. */
+int agd_gpu_solve_range(agd_gpu_problem *problem, AGD_TYPE initial_factor, int n_its,
+                        int it_begin, int it_end, int print_freq, AGD_TYPE const *model_in,
+                        AGD_TYPE *model_out, AGD_TYPE *const *data);
+
 /* Benchmark hook: loads `data`, runs the set-up step, then `warmup` untimed
  * and `steps` timed ISTA iterations with every input resident on the device,
  * each iteration a replay of one captured CUDA graph (as agd_gpu_solve runs
