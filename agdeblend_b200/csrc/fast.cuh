@@ -540,7 +540,40 @@ __global__ void __launch_bounds__(NT, MINB)
     space_axes<R, D, P0, P1, P2, NT, NP, false>(buf, np);
     if constexpr (STAGES == 2) cp_async_wait<0>();
     __syncthreads();
-    for (int e = threadIdx.x; e < n_store; e += NT) {
+    // two consecutive elements per thread in 16-byte vectors when the model
+    // is 16-byte aligned (float; rows have even length, so elements 2q and
+    // 2q + 1 share a row of the padded plane)
+    const bool vec = sizeof(R) == sizeof(float) && (reinterpret_cast<uintptr_t>(dst) & 15) == 0;
+    const int n_vec = vec ? n_store / 2 : 0;
+#pragma unroll 2
+    for (int q = threadIdx.x; q < n_vec; q += NT) {
+      const int e = 2 * q;
+      const int p = e / S::dense_P;
+      const int pos = p * S::size + plane_pos<D, P0, P1, P2, S::Q1, S::Q2>(e - p * S::dense_P);
+      const C g0 = buf[pos];
+      const C g1 = buf[pos + 1];
+      float4 *d4 = reinterpret_cast<float4 *>(dst) + q;
+      if (epilogue == kStore) {
+        *d4 = make_float4((float)g0.x, (float)g0.y, (float)g1.x, (float)g1.y);
+        continue;
+      }
+      const float4 xv = STAGES == 2 ? reinterpret_cast<const float4 *>(xbuf)[q] : *d4;
+      C n0 = cmake<C>(sub_rn<R>((R)xv.x, mul_rn<R>(step, g0.x)),
+                      sub_rn<R>((R)xv.y, mul_rn<R>(step, g0.y)));
+      C n1 = cmake<C>(sub_rn<R>((R)xv.z, mul_rn<R>(step, g1.x)),
+                      sub_rn<R>((R)xv.w, mul_rn<R>(step, g1.y)));
+      if (epilogue == kUpdateThreshold) {
+        n0 = soft_threshold<R>(n0, lamb, lamb_sq);
+        n1 = soft_threshold<R>(n1, lamb, lamb_sq);
+      } else {
+        const R a0 = abs_sq<R>(n0);
+        const R a1 = abs_sq<R>(n1);
+        local_max = a0 > local_max ? a0 : local_max;
+        local_max = a1 > local_max ? a1 : local_max;
+      }
+      *d4 = make_float4((float)n0.x, (float)n0.y, (float)n1.x, (float)n1.y);
+    }
+    for (int e = vec ? n_store : threadIdx.x; e < n_store; e += NT) {
       const int p = e / S::dense_P;
       const C g = buf[p * S::size + plane_pos<D, P0, P1, P2, S::Q1, S::Q2>(e - p * S::dense_P)];
       if (epilogue == kStore) {
