@@ -410,7 +410,7 @@ class Engine {
   // trace length factors into supported coprime prime powers
   bool wav_fast = false;
   DevArray<WaveletFastJob<R>> wavf_jobs;
-  DevArray<int> kperm;
+  DevArray<unsigned short> pfa_map;  // per trace length: qmap [C], kpos [C]
   TimeLaunch wavf;
   using WaveletFn = void (*)(const WaveletFastJob<R> *, const int *, const int *, int,
                              const C *, const long *, int, const R *);
@@ -468,10 +468,15 @@ class Engine {
     smem_max = std::min({opt_in(axis_pass<R>, limit), opt_in(time_c2r_ola<R>, limit),
                          opt_in(time_r2c<R>, limit), opt_in(wavelet_apply<R>, limit)});
     if constexpr (sizeof(R) == sizeof(float))
-      smem_max = std::min({smem_max, opt_in(wavelet_fast<R, 2>, limit),
-                           opt_in(wavelet_fast<R, 3>, limit)});
+      smem_max = std::min({smem_max, opt_in(wavelet_fast<R, 2, 17>, limit),
+                           opt_in(wavelet_fast<R, 3, 17>, limit),
+                           opt_in(wavelet_fast<R, 4, 17>, limit),
+                           opt_in(wavelet_fast<R, 2, 32>, limit),
+                           opt_in(wavelet_fast<R, 3, 32>, limit)});
     else
-      smem_max = std::min(smem_max, opt_in(wavelet_fast<R, 1>, limit));
+      smem_max = std::min({smem_max, opt_in(wavelet_fast<R, 1, 17>, limit),
+                           opt_in(wavelet_fast<R, 2, 17>, limit),
+                           opt_in(wavelet_fast<R, 1, 32>, limit)});
   }
 
   // twiddle tables of the register DFTs in constant memory of the current
@@ -490,9 +495,12 @@ class Engine {
       CK(cudaMemcpyToSymbol(c_tw_d, tw.data(), tw.size() * sizeof(C)));
   }
 
-  // C = product of pairwise coprime prime powers with a register DFT
+  // C = product of pairwise coprime prime powers with a register DFT; the
+  // even factor (if any) is the outermost axis, so the innermost axis, whose
+  // lines start f apart, has an odd extent (no shared-memory bank conflicts)
   static bool pfa_shape(int N, PfaShape &sh) {
     static const int kOk[] = {2, 3, 4, 5, 7, 8, 9, 11, 13, 16, 17, 19, 23, 25, 27, 32};
+    if (N < 2 || N > 65535) return false;
     sh = PfaShape{};
     sh.N = N;
     int n = N;
@@ -508,25 +516,36 @@ class Engine {
         return false;
       sh.f[sh.nf++] = q;
     }
-    for (int i = 0; i < sh.nf; ++i) {
-      sh.s[i] = N / sh.f[i];
-      sh.inv[i] = 1;
-      while ((long)sh.s[i] * sh.inv[i] % sh.f[i] != 1 % sh.f[i]) ++sh.inv[i];
+    int g = 1;
+    for (int i = sh.nf - 1; i >= 0; --i) {
+      sh.g[i] = g;
+      sh.inv_g[i] = 1.0f / (float)g;
+      sh.inv_lines[i] = (float)sh.f[i] / (float)N;
+      g *= sh.f[i];
     }
     return true;
   }
 
-  // position -> frequency after the forward passes (Chinese remainder map)
-  static void pfa_kperm(const PfaShape &sh, std::vector<int> &out) {
+  // qmap[t]: dense position of sample t (coordinates t s_i^-1 mod f_i);
+  // kpos[k]: dense position of frequency k after the forward passes
+  // (coordinates k mod f_i)
+  static void pfa_tables(const PfaShape &sh, std::vector<unsigned short> &out) {
     const long N = sh.N;
-    for (long p = 0; p < N; ++p) {
-      long k = 0;
-      for (int i = 0; i < sh.nf; ++i) {
-        const long ki = p * sh.inv[i] % sh.f[i];
-        const long ei = (long)sh.s[i] * sh.inv[i] % N;
-        k = (k + ki * ei) % N;
-      }
-      out.push_back((int)k);
+    long inv[kPfaMaxFactors];
+    for (int i = 0; i < sh.nf; ++i) {
+      const long s = N / sh.f[i];
+      inv[i] = 1;
+      while (s * inv[i] % sh.f[i] != 1 % sh.f[i]) ++inv[i];
+    }
+    for (long t = 0; t < N; ++t) {
+      long q = 0;
+      for (int i = 0; i < sh.nf; ++i) q += t * inv[i] % sh.f[i] * sh.g[i];
+      out.push_back((unsigned short)q);
+    }
+    for (long k = 0; k < N; ++k) {
+      long q = 0;
+      for (int i = 0; i < sh.nf; ++i) q += k % sh.f[i] * sh.g[i];
+      out.push_back((unsigned short)q);
     }
   }
 
@@ -536,28 +555,31 @@ class Engine {
     if (env != nullptr && env[0] == '1') return;
     const int nw = (int)plan.windows.size();
     std::vector<WaveletFastJob<R>> jobs(nw);
-    std::vector<int> perm;
+    std::vector<unsigned short> perm;
     std::map<int, long> perm_off;
+    int fmax = 1;  // largest factor of any trace length
     int n_max = 1;
     for (int w = 0; w < nw; ++w) {
       WaveletFastJob<R> &j = jobs[w];
       const int N = plan.windows[w].C;
       if (!pfa_shape(N, j.sh)) return;
+      for (int i = 0; i < j.sh.nf; ++i) fmax = std::max(fmax, j.sh.f[i]);
       if (!perm_off.count(N)) {
         perm_off[N] = (long)perm.size();
-        pfa_kperm(j.sh, perm);
+        pfa_tables(j.sh, perm);
       }
       n_max = std::max(n_max, N);
     }
     const size_t per_pair = (size_t)n_max * sizeof(C);
     if (per_pair > (size_t)smem_max) return;
-    kperm.upload(perm, stream);
+    pfa_map.upload(perm, stream);
     for (int w = 0; w < nw; ++w) {
       const WindowPlan &W = plan.windows[w];
       WaveletFastJob<R> &j = jobs[w];
       j.y = wj[w].y;
       j.src = wj[w].src;
-      j.kperm = kperm.get() + perm_off[W.C];
+      j.qmap = pfa_map.get() + perm_off[W.C];
+      j.kpos = j.qmap + W.C;
       j.blend_rec = blend_rec.get() + wt_base[w];
       j.blend_ts = blend_ts.get() + wt_base[w];
       j.blend_n = blend_n.get() + wt_base[w];
@@ -575,12 +597,24 @@ class Engine {
     auto pairs = [&](size_t budget) {
       return (int)std::max<size_t>(1, std::min<size_t>(4, budget / per_pair));
     };
-    if constexpr (sizeof(R) == sizeof(float)) {
-      cands.push_back(Cand{wavelet_fast<R, 2>, pairs(60000)});
-      cands.push_back(Cand{wavelet_fast<R, 3>, pairs(60000)});
-      cands.push_back(Cand{wavelet_fast<R, 3>, pairs(40000)});
+    if (fmax <= 17) {
+      if constexpr (sizeof(R) == sizeof(float)) {
+        cands.push_back(Cand{wavelet_fast<R, 2, 17>, pairs(80000)});
+        cands.push_back(Cand{wavelet_fast<R, 3, 17>, pairs(60000)});
+        cands.push_back(Cand{wavelet_fast<R, 3, 17>, pairs(40000)});
+        cands.push_back(Cand{wavelet_fast<R, 4, 17>, pairs(40000)});
+      } else {
+        cands.push_back(Cand{wavelet_fast<R, 1, 17>, pairs(80000)});
+        cands.push_back(Cand{wavelet_fast<R, 2, 17>, pairs(80000)});
+      }
     } else {
-      cands.push_back(Cand{wavelet_fast<R, 1>, pairs(60000)});
+      if constexpr (sizeof(R) == sizeof(float)) {
+        cands.push_back(Cand{wavelet_fast<R, 2, 32>, pairs(60000)});
+        cands.push_back(Cand{wavelet_fast<R, 3, 32>, pairs(60000)});
+        cands.push_back(Cand{wavelet_fast<R, 3, 32>, pairs(40000)});
+      } else {
+        cands.push_back(Cand{wavelet_fast<R, 1, 32>, pairs(60000)});
+      }
     }
     auto launch_for = [&](TimeLaunch &L, int np) {
       std::vector<int> cj, cp;
