@@ -526,9 +526,9 @@ class Engine {
     return true;
   }
 
-  // qmap[t]: dense position of sample t (coordinates t s_i^-1 mod f_i);
+  // qmap[t]: dense position of sample t (coordinates t mod f_i);
   // kpos[k]: dense position of frequency k after the forward passes
-  // (coordinates k mod f_i)
+  // (coordinates k s_i^-1 mod f_i, s_i = C / f_i)
   static void pfa_tables(const PfaShape &sh, std::vector<unsigned short> &out) {
     const long N = sh.N;
     long inv[kPfaMaxFactors];
@@ -539,12 +539,12 @@ class Engine {
     }
     for (long t = 0; t < N; ++t) {
       long q = 0;
-      for (int i = 0; i < sh.nf; ++i) q += t * inv[i] % sh.f[i] * sh.g[i];
+      for (int i = 0; i < sh.nf; ++i) q += t % sh.f[i] * sh.g[i];
       out.push_back((unsigned short)q);
     }
     for (long k = 0; k < N; ++k) {
       long q = 0;
-      for (int i = 0; i < sh.nf; ++i) q += k % sh.f[i] * sh.g[i];
+      for (int i = 0; i < sh.nf; ++i) q += k * inv[i] % sh.f[i] * sh.g[i];
       out.push_back((unsigned short)q);
     }
   }
@@ -796,6 +796,19 @@ class Engine {
                                     ST, (size_t)ST * NP * Sh::size * sizeof(C)});
   }
 
+  // pipelined adjoint candidates (fast.cuh space_adj_pipe): NP dense
+  // cropped staging planes and NP padded work planes
+  template <int D, int P0, int P1, int P2, int NT, int NP, int MB, bool XS = false>
+  static void add_adj_pipe(FastClass &c) {
+    using Sh = PlaneShape<D, P0, P1, P2>;
+    const size_t stg = (size_t)NP * Sh::dense_L;
+    const size_t work = (size_t)NP * Sh::size;
+    const size_t x = XS ? (size_t)NP * Sh::dense_P : 0;
+    c.adj_vars.push_back(AdjVariant{space_adj_pipe<R, D, P0, P1, P2, NT, NP, MB, XS>, NT, NP,
+                                    XS ? 4 : 3,
+                                    (stg + stg % 2 + work + work % 2 + x) * sizeof(C)});
+  }
+
   template <int D, int P0, int P1, int P2>
   static bool shape_is(const WindowPlan &W) {
     const int P[3] = {P0, P1, P2};
@@ -818,6 +831,7 @@ class Engine {
         add_adj<1, 40, 1, 1, 256, 96, 2, 2>(c);
         add_fwd_rows<1, 40, 1, 1, 256, 64, 2>(c);
         add_adj_rows<1, 40, 1, 1, 256, 64, 2, 2>(c);
+        add_adj_pipe<1, 40, 1, 1, 256, 128, 2>(c);
       } else if (shape_is<1, 20, 1, 1>(W)) {
         add_fwd<1, 20, 1, 1, 256, 256, 2, 1>(c);
         add_fwd<1, 20, 1, 1, 256, 128, 1, 3>(c);
@@ -827,6 +841,8 @@ class Engine {
         add_adj<1, 20, 1, 1, 256, 128, 2, 2>(c);
         add_fwd_rows<1, 20, 1, 1, 256, 128, 3>(c);
         add_adj_rows<1, 20, 1, 1, 256, 128, 2, 2>(c);
+        add_adj_pipe<1, 20, 1, 1, 256, 160, 3>(c);
+        add_adj_pipe<1, 20, 1, 1, 256, 256, 2>(c);
       } else if (shape_is<2, 20, 40, 1>(W)) {
         add_fwd<2, 20, 40, 1, 384, 16, 2, 1>(c);
         add_fwd<2, 20, 40, 1, 256, 12, 1, 2>(c);
@@ -836,6 +852,9 @@ class Engine {
         add_adj<2, 20, 40, 1, 256, 5, 2, 2>(c);
         add_fwd_rows<2, 20, 40, 1, 256, 8, 2>(c);
         add_adj_rows<2, 20, 40, 1, 256, 6, 2, 2>(c);
+        add_adj_pipe<2, 20, 40, 1, 256, 6, 2>(c);
+        add_adj_pipe<2, 20, 40, 1, 256, 5, 2, true>(c);
+        add_adj_pipe<2, 20, 40, 1, 256, 8, 2>(c);
       } else if (shape_is<2, 20, 20, 1>(W)) {
         add_fwd<2, 20, 20, 1, 384, 24, 2, 1>(c);
         add_fwd<2, 20, 20, 1, 256, 12, 1, 3>(c);
@@ -845,6 +864,9 @@ class Engine {
         add_adj<2, 20, 20, 1, 256, 10, 2, 2>(c);
         add_fwd_rows<2, 20, 20, 1, 256, 12, 3>(c);
         add_adj_rows<2, 20, 20, 1, 256, 10, 2, 2>(c);
+        add_adj_pipe<2, 20, 20, 1, 256, 12, 3>(c);
+        add_adj_pipe<2, 20, 20, 1, 256, 16, 2>(c);
+        add_adj_pipe<2, 20, 20, 1, 256, 8, 2, true>(c);
       } else if (shape_is<2, 40, 40, 1>(W)) {
         add_fwd<2, 40, 40, 1, 320, 8, 2, 1>(c);
         add_fwd<2, 40, 40, 1, 256, 6, 1, 2>(c);
@@ -854,6 +876,7 @@ class Engine {
         add_adj<2, 40, 40, 1, 256, 2, 2, 2>(c);
         add_fwd_rows<2, 40, 40, 1, 256, 4, 2>(c);
         add_adj_rows<2, 40, 40, 1, 256, 3, 2, 2>(c);
+        add_adj_pipe<2, 40, 40, 1, 256, 4, 2>(c);
       } else if (shape_is<3, 20, 20, 20>(W)) {
         add_fwd<3, 20, 20, 20, 512, 1, 2, 1>(c);
         add_fwd<3, 20, 20, 20, 256, 1, 1, 3>(c);
@@ -862,6 +885,9 @@ class Engine {
         add_adj<3, 20, 20, 20, 256, 1, 1, 3>(c);
         add_adj_rows<3, 20, 20, 20, 512, 1, 2, 1>(c);
         add_adj_rows<3, 20, 20, 20, 256, 1, 1, 3>(c);
+        add_adj_pipe<3, 20, 20, 20, 256, 1, 2>(c);
+        add_adj_pipe<3, 20, 20, 20, 384, 1, 2>(c);
+        add_adj_pipe<3, 20, 20, 20, 448, 1, 1, true>(c);
       }
     } else {
       // double: the two-stage kernels only (one-stage kernels with several

@@ -117,6 +117,28 @@ __host__ __device__ constexpr int small_split(int n) {
 template <typename R, int N, bool INV>
 __device__ __forceinline__ void dft(Cx<R> (&v)[N]);
 
+// Coprime split N = N1 * (N / N1) for the prime-factor DFT: N1 the largest
+// power of two dividing N, or for odd N the power of its smallest prime
+// (0 when N is a prime power).
+__host__ __device__ constexpr int coprime_split(int n) {
+  int p2 = 1;
+  while (n % (2 * p2) == 0) p2 *= 2;
+  if (p2 > 1) return p2 < n ? p2 : 0;
+  int p = 3;
+  while (p * p <= n && n % p) p += 2;
+  if (n % p) return 0;  // n prime
+  int q = 1;
+  while (n % (q * p) == 0) q *= p;
+  return q < n ? q : 0;
+}
+
+// k in [0, N1 N2) with k = k1 (mod N1), k = k2 (mod N2)
+__host__ __device__ constexpr int crt_index(int k1, int k2, int N1, int N2) {
+  int k = k2;
+  while (k % N1 != k1) k += N2;
+  return k;
+}
+
 // Odd length N with a twiddle table: the outputs k and N-k share the sums
 // x_j + x_{N-j} (times cos) and x_j - x_{N-j} (times sin), so
 //   X_k = A_k -/+ i B_k,  X_{N-k} = A_k +/- i B_k   (forward / inverse),
@@ -158,6 +180,36 @@ __device__ __forceinline__ void dft_odd(Cx<R> (&v)[N]) {
     }
   }
   v[0] = tot;
+}
+
+// Prime-factor (Good-Thomas) DFT in registers for coprime N1, N2: input
+// n = (n1 N2 + n2 N1) mod N, output k with k = k1 (mod N1), k = k2
+// (mod N2); as exp(-2 pi i n k / N) = W_N1^(n1 k1) W_N2^(n2 k2) the two
+// stages need no twiddle factors, and every index is a compile-time
+// register name.
+template <typename R, int N1, int N2, bool INV>
+__device__ __forceinline__ void dft_pfa(Cx<R> (&v)[N1 * N2]) {
+  using C = Cx<R>;
+  constexpr int N = N1 * N2;
+  C a[N];
+#pragma unroll
+  for (int n2 = 0; n2 < N2; ++n2) {
+    C t[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) t[n1] = v[(n1 * N2 + n2 * N1) % N];
+    dft<R, N1, INV>(t);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) a[k1 * N2 + n2] = t[k1];
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < N1; ++k1) {
+    C t[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) t[n2] = a[k1 * N2 + n2];
+    dft<R, N2, INV>(t);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) v[crt_index(k1, k2, N1, N2)] = t[k2];
+  }
 }
 
 // Four-step in registers: N = N1 * N2, natural order in and out.
@@ -250,6 +302,9 @@ __device__ __forceinline__ void dft(Cx<R> (&v)[N]) {
     v[6] = csub(e[2], o2);
     v[3] = cadd(e[3], o3);
     v[7] = csub(e[3], o3);
+  } else if constexpr (coprime_split(N) != 0) {
+    constexpr int N1 = coprime_split(N);
+    dft_pfa<R, N1, N / N1, INV>(v);
   } else if constexpr (small_split(N) != 0) {
     constexpr int N1 = small_split(N);
     dft_fourstep<R, N1, N / N1, INV>(v);
@@ -808,6 +863,215 @@ __global__ void __launch_bounds__(NT, MINB)
     cur = nxt;
     nxt = after;
   }
+  if (!multi && epilogue == kUpdateMax) {
+    __shared__ R red[32];
+    const R m = block_max<R>(local_max, red);
+    if (threadIdx.x == 0) atomic_max_nonneg(max_out, m);
+  }
+}
+
+// Line FFTs from one buffer into another: lines over EO x EI positions of
+// np planes, source strides (plane SPL, outer SSO, line SSL, inner SSI),
+// destination strides (DPL, DSO, DSL, DSI); NIN elements read (zero beyond),
+// NOUT written.
+template <typename R, int N, bool INV, int NT, int EO, int EI, int SPL, int SSO, int SSL,
+          int SSI, int DPL, int DSO, int DSL, int DSI, int NIN, int NOUT>
+__device__ __forceinline__ void lines_fft_copy(const Cx<R> *src, Cx<R> *dst, int np) {
+  using C = Cx<R>;
+  constexpr int PER = EO * EI;
+  const int total = np * PER;
+  for (int l = threadIdx.x; l < total; l += NT) {
+    const int p = l / PER;
+    const int r = l - p * PER;
+    const int o = r / EI;
+    const int i = r - o * EI;
+    const C *s = src + p * SPL + o * SSO + i * SSI;
+    C *d = dst + p * DPL + o * DSO + i * DSI;
+    C v[N];
+#pragma unroll
+    for (int e = 0; e < N; ++e) v[e] = e < NIN ? s[e * SSL] : cmake<C>((R)0, (R)0);
+    dft<R, N, INV>(v);
+#pragma unroll
+    for (int e = 0; e < NOUT; ++e) d[e * DSL] = v[e];
+  }
+}
+
+// Adjoint, all space axes, with the ISTA update fused (epilogues as
+// space_adj_fast), pipelined: the cropped input planes of a batch are copied
+// densely (16-byte cp.async where aligned) into a staging buffer; the first
+// pass (axis 0, zero-padding L0 -> P0) reads them from there into the padded
+// work buffer, after which the staging buffer takes the next batch's copies
+// while the remaining passes and the update run.  The update walks the model
+// rows (the contiguous axis, PL elements) with a fixed thread -> (row,
+// 16-byte column) map: padded rows sit PLS apart in the work buffer and PL
+// apart in the model, so no index division is needed.  The model planes
+// come either from registers (XS false: each thread keeps U loads in
+// flight, the first U issued before the last pass) or from a third shared
+// buffer filled by cp.async at the start of the batch, behind all three
+// passes (XS true).  Shared memory: NP dense cropped planes, NP padded
+// planes (and NP dense model planes).
+template <typename R, int D, int P0, int P1, int P2, int NT, int NP, int MINB, bool XS>
+__global__ void __launch_bounds__(NT, MINB)
+    space_adj_pipe(PlaneBatches<R> batches, int epilogue, R step_arg, R lamb_arg,
+                   const R *step_dev, const R *lamb_dev, R *max_out) {
+  using C = Cx<R>;
+  using S = PlaneShape<D, P0, P1, P2>;
+  constexpr int Z = S::size;
+  constexpr int PL = S::PL;
+  constexpr int PLS = S::PLS;
+  constexpr int ROWS = S::dense_P / PL;
+  static_assert(Z == ROWS * PLS, "padded rows evenly spaced");
+  constexpr int CW = PL / 2;               // 16-byte columns of a row (float)
+  constexpr int TR = NT / CW;              // rows per sweep
+  // model loads in flight per thread (XS false), and whether the first ones
+  // are issued before the last pass, from the register budget
+  constexpr int kRegs = 65536 / (NT * MINB);
+  constexpr int U = XS ? 1 : (kRegs >= 120 && PL <= 20 ? 8 : 4);
+  constexpr bool kEarly = !XS && D > 1 && 2 * PL + 4 * U + 24 <= kRegs;
+  constexpr bool kVec = sizeof(R) == sizeof(float) && PL % 2 == 0;
+  constexpr int kStg = NP * S::dense_L + (NP * S::dense_L) % 2;  // 16-byte aligned
+  constexpr int kWork = NP * Z + (NP * Z) % 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *stg = reinterpret_cast<C *>(smem_raw);
+  C *work = stg + kStg;
+  C *xbuf = work + kWork;  // XS only
+  auto copy_in = [&](C *to, const C *from, int n) {
+    if (sizeof(C) == 8 && n % 2 == 0 && (reinterpret_cast<uintptr_t>(from) & 15) == 0) {
+      for (int e = threadIdx.x; e < n / 2; e += NT) cp_async<16>(to + 2 * e, from + 2 * e);
+    } else {
+      for (int e = threadIdx.x; e < n; e += NT) cp_async<sizeof(C)>(to + e, from + e);
+    }
+  };
+  const bool multi = step_dev != nullptr;
+  const bool need_x = epilogue != kStore;
+  R local_max = (R)0;
+  const int col = threadIdx.x % CW;
+  const int rr = threadIdx.x / CW;
+  const bool lane_on = rr < TR;
+  const PlaneBatch<R> none{nullptr, nullptr, 0, 0};
+  int b = blockIdx.x;
+  PlaneBatch<R> cur = b < batches.n ? batches.b[b] : none;
+  PlaneBatch<R> nxt = b + gridDim.x < batches.n ? batches.b[b + gridDim.x] : none;
+  if (b < batches.n) copy_in(stg, cur.src, cur.count * S::dense_L);
+  cp_async_commit();
+  for (; b < batches.n; b += gridDim.x) {
+    const int b2 = b + 2 * gridDim.x;
+    const PlaneBatch<R> after = b2 < batches.n ? batches.b[b2] : none;
+    const int np = cur.count;
+    C *dst = cur.dst;
+    if constexpr (XS) {
+      // model planes of this batch, behind the three passes (group order:
+      // staging of this batch, model of this batch, staging of the next)
+      if (need_x) copy_in(xbuf, dst, np * S::dense_P);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    // first pass: staging (dense L planes) -> work (padded P planes)
+    if constexpr (D == 1) {
+      lines_fft_copy<R, P0, false, NT, 1, 1, S::dense_L, 0, 1, 0, Z, 0, 1, 0, S::L0, P0>(
+          stg, work, np);
+    } else if constexpr (D == 2) {
+      lines_fft_copy<R, P0, false, NT, 1, S::L1, S::dense_L, 0, S::L1, 1, Z, 0, S::S0, 1, S::L0,
+                     P0>(stg, work, np);
+    } else {
+      lines_fft_copy<R, P0, false, NT, S::L1, S::L2, S::dense_L, S::L2, S::L1 * S::L2, 1, Z,
+                     S::S1, S::S0, 1, S::L0, P0>(stg, work, np);
+    }
+    __syncthreads();
+    if (nxt.count > 0) copy_in(stg, nxt.src, nxt.count * S::dense_L);
+    cp_async_commit();
+    const R step = multi ? step_dev[cur.pid] : step_arg;
+    const R lamb = lamb_dev != nullptr ? lamb_dev[multi ? cur.pid : 0] : lamb_arg;
+    const R lamb_sq = lamb * lamb;
+    if constexpr (D == 3) {
+      lines_fft<R, P1, false, NT, NP, Z, P0, S::L2, S::S0, S::S1, 1, S::L1, P1>(work, np);
+      __syncthreads();
+    }
+    const int nrows = np * ROWS;
+    const bool vec = kVec && (reinterpret_cast<uintptr_t>(dst) & 15) == 0;
+    float4 xv[U];
+    auto load_x = [&](int r0) {
+#pragma unroll
+      for (int j = 0; j < U; ++j) {
+        const int r = r0 + rr + TR * j;
+        if (lane_on && r < nrows)
+          xv[j] = reinterpret_cast<const float4 *>(XS ? xbuf : dst)[r * CW + col];
+      }
+    };
+    if (kEarly && vec && need_x) load_x(0);
+    // last pass (contiguous axis) in the work buffer
+    if constexpr (D == 2) {
+      lines_fft<R, P1, false, NT, NP, Z, P0, 1, S::S0, 1, 0, S::L1, P1>(work, np);
+    } else if constexpr (D == 3) {
+      lines_fft<R, P2, false, NT, NP, Z, P0 * P1, 1, S::S1, 1, 0, S::L2, P2>(work, np);
+    }
+    if constexpr (XS) cp_async_wait<1>();  // this batch's model planes
+    __syncthreads();
+    if (vec) {
+      for (int r0 = 0; r0 < nrows; r0 += TR * U) {
+        if ((r0 > 0 || !kEarly) && need_x) load_x(r0);
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+          const int r = r0 + rr + TR * j;
+          if (!lane_on || r >= nrows) continue;
+          const C g0 = work[r * PLS + 2 * col];
+          const C g1 = work[r * PLS + 2 * col + 1];
+          float4 *d4 = reinterpret_cast<float4 *>(dst) + r * CW + col;
+          if (!need_x) {
+            *d4 = make_float4((float)g0.x, (float)g0.y, (float)g1.x, (float)g1.y);
+            continue;
+          }
+          C n0 = cmake<C>(sub_rn<R>((R)xv[j].x, mul_rn<R>(step, g0.x)),
+                          sub_rn<R>((R)xv[j].y, mul_rn<R>(step, g0.y)));
+          C n1 = cmake<C>(sub_rn<R>((R)xv[j].z, mul_rn<R>(step, g1.x)),
+                          sub_rn<R>((R)xv[j].w, mul_rn<R>(step, g1.y)));
+          if (epilogue == kUpdateThreshold) {
+            n0 = soft_threshold<R>(n0, lamb, lamb_sq);
+            n1 = soft_threshold<R>(n1, lamb, lamb_sq);
+          } else {
+            const R a0 = abs_sq<R>(n0);
+            const R a1 = abs_sq<R>(n1);
+            local_max = a0 > local_max ? a0 : local_max;
+            local_max = a1 > local_max ? a1 : local_max;
+          }
+          *d4 = make_float4((float)n0.x, (float)n0.y, (float)n1.x, (float)n1.y);
+        }
+      }
+    } else {
+      const int n_store = nrows * PL;
+      for (int e = threadIdx.x; e < n_store; e += NT) {
+        const int r = e / PL;
+        const C g = work[r * PLS + (e - r * PL)];
+        if (!need_x) {
+          dst[e] = g;
+          continue;
+        }
+        const C x = XS ? xbuf[e] : dst[e];
+        C xn = cmake<C>(sub_rn<R>(x.x, mul_rn<R>(step, g.x)),
+                        sub_rn<R>(x.y, mul_rn<R>(step, g.y)));
+        if (epilogue == kUpdateThreshold) {
+          xn = soft_threshold<R>(xn, lamb, lamb_sq);
+        } else {
+          const R a2 = abs_sq<R>(xn);
+          local_max = a2 > local_max ? a2 : local_max;
+        }
+        dst[e] = xn;
+      }
+    }
+    __syncthreads();
+    if (multi && epilogue == kUpdateMax) {  // one maximum per problem
+      __shared__ R red_b[32];
+      const R m = block_max<R>(local_max, red_b);
+      if (threadIdx.x == 0) atomic_max_nonneg(max_out + cur.pid, m);
+      local_max = (R)0;
+    }
+    cur = nxt;
+    nxt = after;
+  }
+  cp_async_wait<0>();
   if (!multi && epilogue == kUpdateMax) {
     __shared__ R red[32];
     const R m = block_max<R>(local_max, red);

@@ -8,14 +8,16 @@
 // window travel as one complex sequence z = a + i b:
 //
 //  * prime-factor (Good-Thomas) FFT in shared memory: with C = f_0 f_1 ...
-//    and s_i = C / f_i, sample t has the coordinates n_i = t s_i^-1 mod f_i
-//    (t = sum_i n_i s_i mod C), and the load copies it to position
-//    sum_i n_i g_i of a dense array with extents (f_0, f_1, ...) and strides
-//    g_i (qmap, built on the host).  A pass along axis i is then a plain
-//    f_i-point DFT over lines of stride g_i, with no twiddles and no index
-//    wrap; after the forward passes frequency k sits at
-//    sum_i (k mod f_i) g_i (kpos), and the inverse passes return the dense
-//    array to the sample layout, which the store reads back through qmap.
+//    and s_i = C / f_i, sample t has the coordinates n_i = t mod f_i, and
+//    the load copies it to position sum_i n_i g_i of a dense array with
+//    extents (f_0, f_1, ...) and strides g_i (qmap, built on the host).  As
+//    exp(-2 pi i t k / C) factors over the axes for k = sum_i k_i s_i mod C,
+//    a pass along axis i is a plain f_i-point DFT over lines of stride g_i,
+//    with no twiddles and no index wrap; after the forward passes frequency
+//    k sits at sum_i (k s_i^-1 mod f_i) g_i (kpos), and the inverse passes
+//    return the dense array to the sample layout, which the store reads
+//    back through qmap.  Consecutive samples lie sum_i g_i apart, an odd
+//    stride, so the copies in and out are free of bank conflicts.
 //  * between them, with Z' the product spectrum,
 //      Z'_k = ((Z_k + conj Z_{C-k}) S_a + (Z_k - conj Z_{C-k}) S_b) / 2,
 //    which is Z_k S when both traces use the same spectrum.  The real and
@@ -159,37 +161,27 @@ __global__ void __launch_bounds__(kWavThreads, MINB)
   const unsigned short *__restrict__ kpos = job.kpos;
 
   // ---- load: trace a -> real part, trace b -> imaginary part, each sample
-  // to its dense position; every copy of the block in flight together
+  // to its dense position; thread u copies half u & 1 of sample u >> 1, so a
+  // warp fills 16 whole complex slots; every copy of the block in flight
+  // together
   for (int pr = 0; pr < np; ++pr) {
     const int ta = 2 * (pair0 + pr);
-    const bool has_b = ta + 1 < n_tr;
-    C *b = buf + pr * N;
+    const int tb = ta + 1 < n_tr ? ta + 1 : -1;
+    const int mine = tb >= 0 ? ta + (threadIdx.x & 1) : ta;  // this thread's trace
+    R *b = reinterpret_cast<R *>(buf + pr * N) + (threadIdx.x & 1);
+    const bool live = tb >= 0 || (threadIdx.x & 1) == 0;
     if (record != nullptr) {
-      const long ra = job.blend_rec[ta];
-      const int sa = job.blend_ts[ta];
-      const int na = ra >= 0 ? job.blend_n[ta] : 0;
-      long rb = 0;
-      int sb = 0, nb = 0;
-      if (has_b && job.blend_rec[ta + 1] >= 0) {
-        rb = job.blend_rec[ta + 1];
-        sb = job.blend_ts[ta + 1];
-        nb = job.blend_n[ta + 1];
-      }
-      for (int t = threadIdx.x; t < N; t += kWavThreads) {
-        C *d = b + __ldg(qmap + t);
-        const bool va = t >= sa && t < sa + na;
-        const bool vb = t >= sb && t < sb + nb;
-        cp_async<sizeof(R)>(&d->x, va ? record + ra + (t - sa) : record, va);
-        cp_async<sizeof(R)>(&d->y, vb ? record + rb + (t - sb) : record, vb);
+      const long r0 = job.blend_rec[mine];
+      const int s0 = job.blend_ts[mine];
+      const int n0 = live && r0 >= 0 ? job.blend_n[mine] : 0;
+      for (int t = threadIdx.x >> 1; t < N; t += kWavThreads / 2) {
+        const bool v = t >= s0 && t < s0 + n0;
+        cp_async<sizeof(R)>(b + 2 * __ldg(qmap + t), v ? record + r0 + (t - s0) : record, v);
       }
     } else {
-      const R *ya = job.y + (long)ta * N;
-      const R *yb = has_b ? ya + N : ya;
-      for (int t = threadIdx.x; t < N; t += kWavThreads) {
-        C *d = b + __ldg(qmap + t);
-        cp_async<sizeof(R)>(&d->x, ya + t);
-        cp_async<sizeof(R)>(&d->y, yb + t, has_b);
-      }
+      const R *y0 = job.y + (long)mine * N;
+      for (int t = threadIdx.x >> 1; t < N; t += kWavThreads / 2)
+        cp_async<sizeof(R)>(b + 2 * __ldg(qmap + t), y0 + t, live);
     }
   }
   cp_async_commit();
