@@ -60,6 +60,7 @@ def _bind_extension(lib, dtype):
     lib.agd_gpu_problem_destroy.argtypes = [c_void_p]
     lib.agd_gpu_problem_destroy.restype = None
     lib.agd_gpu_problem_info.argtypes = [c_void_p, POINTER(c_long)]
+    lib.agd_gpu_problem_kernels.argtypes = [c_void_p, ctypes.c_char_p, c_int]
     lib.agd_gpu_stepsize.argtypes = [c_void_p, rp]
     lib.agd_gpu_forward.argtypes = [c_void_p, rp, rp]
     lib.agd_gpu_adjoint.argtypes = [c_void_p, rp, rp]
@@ -81,7 +82,7 @@ def _bind_extension(lib, dtype):
         POINTER(POINTER(ip)), POINTER(POINTER(lip)), POINTER(POINTER(ip)), POINTER(POINTER(ip)),
         POINTER(ip), POINTER(POINTER(ip)), POINTER(POINTER(rp)), POINTER(c_void_p)]
     lib.agd_gpu_problem_steps.argtypes = [c_void_p, rp]
-    for name in ("agd_gpu_problem_info", "agd_gpu_stepsize", "agd_gpu_forward",
+    for name in ("agd_gpu_problem_info", "agd_gpu_problem_kernels", "agd_gpu_stepsize", "agd_gpu_forward",
                  "agd_gpu_adjoint", "agd_gpu_blend_input", "agd_gpu_set_output",
                  "agd_gpu_solve", "agd_gpu_time_iterations", "agd_plan_export",
                  "agd_gpu_solve_range",
@@ -261,6 +262,15 @@ class Problem:
         self.lib.agd_gpu_stepsize(self.h, ctypes.byref(s))
         self.stepsize = float(s.value)
         self._rp = POINTER(rc)
+
+    def kernels(self) -> dict:
+        """Kernel family of each phase for the first window class and time
+        group ({"space_fwd": ..., "space_adj": ..., "time_fwd": ...,
+        "time_adj": ..., "wavelet": ...}), as profilers list the kernels."""
+        buf = ctypes.create_string_buffer(512)
+        self._check(self.lib.agd_gpu_problem_kernels(self.h, buf, len(buf)),
+                    "agd_gpu_problem_kernels")
+        return dict(kv.split("=", 1) for kv in buf.value.decode().split())
 
     def steps(self) -> np.ndarray:
         """Step size of every problem of the handle."""

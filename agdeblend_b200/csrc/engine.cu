@@ -347,11 +347,13 @@ class Engine {
     SpaceFwdFn fn;
     int nt, np, stages;
     size_t smem;
+    const char *name;  // kernel family (as profilers list it)
   };
   struct AdjVariant {
     SpaceAdjFn fn;
     int nt, np, stages;
     size_t smem;
+    const char *name;  // kernel family (as profilers list it)
   };
   // windows of one padded space shape on the fast space kernels
   struct FastClass {
@@ -372,11 +374,13 @@ class Engine {
     TimeFwdFn fn;
     int nb;
     size_t smem;
+    const char *name;  // kernel family (as profilers list it)
   };
   struct TimeAdjVariant {
     TimeAdjFn fn;
     int nb;
     size_t smem;
+    const char *name;  // kernel family (as profilers list it)
   };
   struct TimeGroup {
     std::vector<int> win;
@@ -770,7 +774,7 @@ class Engine {
   static void add_fwd(FastClass &c) {
     using Sh = PlaneShape<D, P0, P1, P2>;
     c.fwd_vars.push_back(FwdVariant{space_fwd_fast<R, D, P0, P1, P2, NT, NP, ST, MB>, NT, NP,
-                                    ST, (size_t)ST * NP * Sh::size * sizeof(C)});
+                                    ST, (size_t)ST * NP * Sh::size * sizeof(C), "space_fwd_fast"});
   }
 
   template <int D, int P0, int P1, int P2, int NT, int NP, int ST, int MB>
@@ -778,7 +782,7 @@ class Engine {
     using Sh = PlaneShape<D, P0, P1, P2>;
     const size_t x = ST == 2 ? (size_t)NP * Sh::dense_P : 0;
     c.adj_vars.push_back(AdjVariant{space_adj_fast<R, D, P0, P1, P2, NT, NP, ST, MB>, NT, NP,
-                                    ST, ((size_t)ST * NP * Sh::size + x) * sizeof(C)});
+                                    ST, ((size_t)ST * NP * Sh::size + x) * sizeof(C), "space_adj_fast"});
   }
 
   // row-fused candidates (fast.cuh space_fwd_rows / space_adj_rows)
@@ -786,14 +790,14 @@ class Engine {
   static void add_fwd_rows(FastClass &c) {
     using Sh = PlaneShape<D, P0, P1, P2>;
     c.fwd_vars.push_back(FwdVariant{space_fwd_rows<R, D, P0, P1, P2, NT, NP, MB>, NT, NP, 1,
-                                    (size_t)NP * Sh::size * sizeof(C)});
+                                    (size_t)NP * Sh::size * sizeof(C), "space_fwd_rows"});
   }
 
   template <int D, int P0, int P1, int P2, int NT, int NP, int ST, int MB>
   static void add_adj_rows(FastClass &c) {
     using Sh = PlaneShape<D, P0, P1, P2>;
     c.adj_vars.push_back(AdjVariant{space_adj_rows<R, D, P0, P1, P2, NT, NP, ST, MB>, NT, NP,
-                                    ST, (size_t)ST * NP * Sh::size * sizeof(C)});
+                                    ST, (size_t)ST * NP * Sh::size * sizeof(C), "space_adj_rows"});
   }
 
   // pipelined adjoint candidates (fast.cuh space_adj_pipe): NP dense
@@ -806,7 +810,7 @@ class Engine {
     const size_t x = XS ? (size_t)NP * Sh::dense_P : 0;
     c.adj_vars.push_back(AdjVariant{space_adj_pipe<R, D, P0, P1, P2, NT, NP, MB, XS>, NT, NP,
                                     XS ? 4 : 3,
-                                    (stg + stg % 2 + work + work % 2 + x) * sizeof(C)});
+                                    (stg + stg % 2 + work + work % 2 + x) * sizeof(C), "space_adj_pipe"});
   }
 
   template <int D, int P0, int P1, int P2>
@@ -880,6 +884,7 @@ class Engine {
       } else if (shape_is<3, 20, 20, 20>(W)) {
         add_fwd<3, 20, 20, 20, 512, 1, 2, 1>(c);
         add_fwd<3, 20, 20, 20, 256, 1, 1, 3>(c);
+        add_fwd<3, 20, 20, 20, 416, 1, 1, 2>(c);
         add_fwd_rows<3, 20, 20, 20, 256, 1, 3>(c);
         add_adj<3, 20, 20, 20, 512, 1, 2, 1>(c);
         add_adj<3, 20, 20, 20, 256, 1, 1, 3>(c);
@@ -888,6 +893,7 @@ class Engine {
         add_adj_pipe<3, 20, 20, 20, 256, 1, 2>(c);
         add_adj_pipe<3, 20, 20, 20, 384, 1, 2>(c);
         add_adj_pipe<3, 20, 20, 20, 448, 1, 1, true>(c);
+        add_adj_pipe<3, 20, 20, 20, 416, 1, 2>(c);
       }
     } else {
       // double: the two-stage kernels only (one-stage kernels with several
@@ -924,10 +930,10 @@ class Engine {
     constexpr int H = 4 * M / 5;
     g.fwd_vars.push_back(TimeFwdVariant{time_fwd_fast<R, M1, M2, NB, LS, MB>, NB,
                                         2 * (size_t)NB * LS * sizeof(C) +
-                                            (size_t)NB * H * sizeof(R)});
+                                            (size_t)NB * H * sizeof(R), "time_fwd_fast"});
     g.adj_vars.push_back(TimeAdjVariant{time_adj_fast<R, M1, M2, NB, LS, MB>, NB,
                                         (size_t)NB * LS * sizeof(C) +
-                                            2 * (size_t)NB * 2 * H * sizeof(R)});
+                                            2 * (size_t)NB * 2 * H * sizeof(R), "time_adj_fast"});
   }
 
   // fused candidates (fast.cuh time_fwd_fused / time_adj_fused), 256 / M1
@@ -938,12 +944,12 @@ class Engine {
     constexpr int H = 4 * M / 5;
     constexpr int NB = kThreads / M1;
     g.fwd_vars.push_back(TimeFwdVariant{time_fwd_fused<R, M1, M2, LSB, LSW, MB>, NB,
-                                        ((size_t)2 * NB * LSB + (size_t)NB * LSW) * sizeof(C)});
+                                        ((size_t)2 * NB * LSB + (size_t)NB * LSW) * sizeof(C), "time_fwd_fused"});
     constexpr int LT = 2 * H;
     constexpr int LTP = LT + ((20 - LT % 32) + 32) % 32;  // as time_adj_fused
     g.adj_vars.push_back(TimeAdjVariant{time_adj_fused<R, M1, M2, LSW, MB>, NB,
                                         (size_t)NB * LSW * sizeof(C) +
-                                            2 * (size_t)NB * LTP * sizeof(R)});
+                                            2 * (size_t)NB * LTP * sizeof(R), "time_adj_fused"});
   }
 
   static bool time_case(const WindowPlan &W, TimeGroup &g) {
@@ -2275,6 +2281,18 @@ int agd_gpu_problem_info(agd_gpu_problem const *pb, long int *info) {
   info[20] = e.wav_fast ? e.wav_pick : -1;
   info[21] = e.wav_candidates;
   return 0;
+}
+
+int agd_gpu_problem_kernels(agd_gpu_problem const *pb, char *buf, int len) {
+  if (pb == nullptr || buf == nullptr || len <= 0) return 1;
+  const agd::EngineR &e = *pb->eng;
+  const bool sc = !e.classes.empty(), tg = !e.tgroups.empty();
+  const int n = std::snprintf(
+      buf, (size_t)len, "space_fwd=%s space_adj=%s time_fwd=%s time_adj=%s wavelet=%s",
+      sc ? e.classes[0]->fv().name : "axis_pass", sc ? e.classes[0]->av().name : "axis_pass",
+      tg ? e.tgroups[0]->fv().name : "time_c2r_ola", tg ? e.tgroups[0]->av().name : "time_r2c",
+      !e.wavelets ? "none" : (e.wav_fast ? "wavelet_fast" : "wavelet_apply"));
+  return n < 0 || n >= len ? 1 : 0;
 }
 
 int agd_gpu_stepsize(agd_gpu_problem *pb, AGD_TYPE *stepsize) {

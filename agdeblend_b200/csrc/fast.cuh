@@ -477,18 +477,34 @@ __global__ void __launch_bounds__(NT, MINB) space_fwd_fast(PlaneBatches<R> batch
   static_assert(STAGES == 1 || STAGES == 2, "one or two stages");
   using C = Cx<R>;
   using S = PlaneShape<D, P0, P1, P2>;
+  constexpr int PL = S::PL;
+  constexpr int PLS = S::PLS;
+  constexpr int ROWS = S::dense_P / PL;  // model rows per plane
+  static_assert(S::size == ROWS * PLS, "padded rows evenly spaced");
+  constexpr int LL = PL * 4 / 5;         // cropped row
+  constexpr int ORW = S::dense_L / LL;   // cropped rows per plane
+  static_assert(LL % 2 == 0, "cropped rows of column pairs");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *stage[2] = {reinterpret_cast<C *>(smem_raw),
                  reinterpret_cast<C *>(smem_raw) + (STAGES == 2 ? NP * S::size : 0)};
+  // copies in: thread -> (row, column) fixed, rows TR apart per sweep (the
+  // model rows are dense, the padded rows PLS apart: no index division)
+  constexpr int TR = NT / PL;
+  const int lc = threadIdx.x % PL;
+  const int lr = threadIdx.x / PL;
   auto issue = [&](const PlaneBatch<R> &bt, C *buf) {
-    const int n = bt.count * S::dense_P;
-    for (int e = threadIdx.x; e < n; e += NT) {
-      const int p = e / S::dense_P;
-      cp_async<sizeof(C)>(buf + p * S::size + plane_pos<D, P0, P1, P2, S::Q1, S::Q2>(
-                                                  e - p * S::dense_P),
-                          bt.src + e);
-    }
+    if (lr >= TR) return;
+    const int nrows = bt.count * ROWS;
+    const C *s = bt.src + lr * PL + lc;
+    C *d = buf + lr * PLS + lc;
+    for (int r = lr; r < nrows; r += TR, s += TR * PL, d += TR * PLS) cp_async<sizeof(C)>(d, s);
   };
+  // copies out: column pairs of the cropped rows, 16-byte stores when the
+  // batch's output is 16-byte aligned (float)
+  constexpr int CW = LL / 2;
+  constexpr int TS = NT / CW;
+  const int sc = threadIdx.x % CW;
+  const int sr = threadIdx.x / CW;
   const PlaneBatch<R> none{nullptr, nullptr, 0, 0};
   int b = blockIdx.x;
   PlaneBatch<R> cur = b < batches.n ? batches.b[b] : none;
@@ -512,10 +528,28 @@ __global__ void __launch_bounds__(NT, MINB) space_fwd_fast(PlaneBatches<R> batch
     space_axes<R, D, P0, P1, P2, NT, NP, true>(buf, np);
     __syncthreads();
     C *dst = cur.dst;
-    const int n_store = np * S::dense_L;
-    for (int e = threadIdx.x; e < n_store; e += NT) {
-      const int p = e / S::dense_L;
-      dst[e] = buf[p * S::size + plane_pos<D, P0, P1, P2, S::L1, S::L2>(e - p * S::dense_L)];
+    if (sr < TS) {
+      const int nrows = np * ORW;
+      const bool vec = sizeof(R) == sizeof(float) && (reinterpret_cast<uintptr_t>(dst) & 15) == 0;
+      for (int r = sr; r < nrows; r += TS) {
+        const int p = r / ORW;
+        const int rem = r - p * ORW;
+        int srow = p * ROWS + rem;  // padded row holding cropped row r
+        if constexpr (D == 3) {
+          const int i0 = rem / S::L1;
+          srow = p * ROWS + i0 * P1 + (rem - i0 * S::L1);
+        }
+        const C g0 = buf[srow * PLS + 2 * sc];
+        const C g1 = buf[srow * PLS + 2 * sc + 1];
+        C *o = dst + (long)r * LL + 2 * sc;
+        if (vec) {
+          *reinterpret_cast<float4 *>(o) = make_float4((float)g0.x, (float)g0.y, (float)g1.x,
+                                                       (float)g1.y);
+        } else {
+          o[0] = g0;
+          o[1] = g1;
+        }
+      }
     }
     __syncthreads();
     if constexpr (STAGES == 1) {

@@ -362,8 +362,10 @@ def run_gpu(args, rank, world, local):
     fast = int(info[8]) == 1
     wav = sv.wavelets is not None
     wav_fast = int(info[9]) == 1
-    names = (("space_fwd_fast", "time_fwd_fast", "blend_gather", "time_adj_fast",
-              "space_adj_fast") if fast else
+    # phases named by the kernel family the set-up picked for them
+    kn = prob.kernels()
+    names = ((kn["space_fwd"], kn["time_fwd"], "blend_gather", kn["time_adj"], kn["space_adj"])
+             if fast else
              ("axis_pass_fwd0", "time_c2r_ola", "blend_gather", "time_r2c", "axis_pass_adj_last"))
     if wav:
         # the adjoint time phase then also holds the wavelet correlation

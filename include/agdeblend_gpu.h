@@ -55,6 +55,12 @@ void agd_gpu_problem_destroy(agd_gpu_problem *problem);
  * picked (-1 without the prime-factor kernel), [21] their number. */
 int agd_gpu_problem_info(agd_gpu_problem const *problem, long int *info);
 
+/* Kernel families serving the first window class and time group, as a
+ * profiler lists them: "space_fwd=... space_adj=... time_fwd=... time_adj=...
+ * wavelet=..." (no reference counterpart: it names this library's
+ * kernels).  Returns 1 if buf (len bytes) is too short. */
+int agd_gpu_problem_kernels(agd_gpu_problem const *problem, char *buf, int len);
+
 /* Step size 0.5 / max blend fold (reference get_stepsize, src/model.c:1230-1312). */
 int agd_gpu_stepsize(agd_gpu_problem *problem, AGD_TYPE *stepsize);
 
