@@ -251,7 +251,7 @@ class Problem:
         return self
 
     def _finish_init(self):
-        info = np.zeros(22, np.int64)
+        info = np.zeros(23, np.int64)
         self.lib.agd_gpu_problem_info(self.h, info.ctypes.data_as(POINTER(c_long)))
         self.info = info
         self.n_windows = int(info[0])

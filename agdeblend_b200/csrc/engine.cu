@@ -22,6 +22,7 @@
 #include "kernels.cuh"
 #include "plan.hpp"
 #include "wavelet_fast.cuh"
+#include "line_dft.cuh"
 
 namespace agd {
 
@@ -325,6 +326,21 @@ class Engine {
   DevArray<double> dscalar;
 
   std::vector<AxisLaunch> fwd, adj_update, adj_plain;
+  // windows with one space axis of a length without a shape-specialised
+  // kernel, on the line kernels (line_dft.cuh)
+  struct LineLaunch {
+    DevArray<LineJob<R>> jobs;
+    DevArray<int> cta_job;
+    DevArray<long> cta_line0;
+    int n_cta = 0;
+    size_t smem = 0;
+  };
+  LineLaunch line_fwd, line_adj, line_adj_plain;
+  DevArray<R> line_tab;        // per (P, L): forward and adjoint cos / sin tables
+  std::vector<char> win_line;  // 1: window on the line kernels
+  std::vector<LineJob<R>> line_adj_host;  // adjoint jobs (the plain adjoint's, re-aimed)
+  std::vector<int> line_cj;
+  std::vector<long> line_cl;
   TimeLaunch time_fwd, time_adj, wav;
 
   // Shape-specialised kernels (fast.cuh).  Windows are grouped into classes
@@ -470,7 +486,8 @@ class Engine {
   void set_smem_limits() {
     const int limit = smem_max;
     smem_max = std::min({opt_in(axis_pass<R>, limit), opt_in(time_c2r_ola<R>, limit),
-                         opt_in(time_r2c<R>, limit), opt_in(wavelet_apply<R>, limit)});
+                         opt_in(time_r2c<R>, limit), opt_in(wavelet_apply<R>, limit),
+                         opt_in(line_dft_fwd<R>, limit), opt_in(line_dft_adj<R>, limit)});
     if constexpr (sizeof(R) == sizeof(float))
       smem_max = std::min({smem_max, opt_in(wavelet_fast<R, 2, 17>, limit),
                            opt_in(wavelet_fast<R, 3, 17>, limit),
@@ -1039,13 +1056,111 @@ class Engine {
       win_class[w] = k;
       classes[k]->win.push_back(w);
     }
+    // one space axis of any other length up to kLineMaxP: line kernels,
+    // when their blocks fit in shared memory
+    win_line.assign(nw, 0);
+    for (int w = 0; w < nw && !generic_only; ++w) {
+      const WindowPlan &W = plan.windows[w];
+      if (win_class[w] >= 0 || W.D != 1 || W.P[0] > kLineMaxP || W.P[0] < 3) continue;
+      const int P = W.P[0], L = W.L[0];
+      const int H = (P - 1) / 2;
+      const size_t sf = line_fwd_smem<R>(P, H, (L + 3) / 4 * 4);
+      const size_t sa = line_adj_smem<R>(P, L, (P / 2 + 1 + 3) / 4 * 4);
+      if (std::max(sf, sa) <= (size_t)smem_max) win_line[w] = 1;
+    }
     n_generic = 0;
     max_d_generic = 0;
     for (int w = 0; w < nw; ++w)
-      if (win_class[w] < 0) {
+      if (win_class[w] < 0 && !win_line[w]) {
         ++n_generic;
         max_d_generic = std::max(max_d_generic, plan.windows[w].D);
       }
+  }
+
+  // Line-kernel jobs, tables and block lists (windows marked in win_line).
+  // Tables per (P, L) in double precision, rounded once: forward rows
+  // j = 1 .. (P-1)/2 over outputs k < L, adjoint rows j < L over k <= P/2,
+  // cos / sin of 2 pi (j k mod P) / P, rows padded to a multiple of 4.
+  void build_line_kernels() {
+    const int nw = (int)plan.windows.size();
+    std::vector<R> tab;
+    std::map<std::pair<int, int>, std::pair<long, long>> off;  // (P, L) -> fwd, adj
+    auto add_table = [&](int P, int rows, int j0, int kout, int kpad) {
+      const long o = (long)tab.size();
+      tab.resize(tab.size() + 2 * (size_t)rows * kpad, (R)0);
+      for (int r = 0; r < rows; ++r)
+        for (int k = 0; k < kout; ++k) {
+          const long m = (long)(r + j0) * k % P;
+          const double a = 2.0 * 3.14159265358979323846 * (double)m / (double)P;
+          tab[o + (long)r * kpad + k] = (R)std::cos(a);
+          tab[o + (long)rows * kpad + (long)r * kpad + k] = (R)std::sin(a);
+        }
+      return o;
+    };
+    std::vector<LineJob<R>> jf, ja;
+    std::vector<long> tf, ta;  // table offsets of each job
+    line_cj.clear();
+    line_cl.clear();
+    size_t sf_max = 0, sa_max = 0;
+    for (int w = 0; w < nw; ++w) {
+      if (!win_line[w]) continue;
+      const WindowPlan &W = plan.windows[w];
+      const int P = W.P[0], L = W.L[0];
+      const int H = (P - 1) / 2;
+      const int kpf = (L + 3) / 4 * 4, kpa = (P / 2 + 1 + 3) / 4 * 4;
+      auto it = off.find({P, L});
+      if (it == off.end())
+        it = off.emplace(std::make_pair(P, L),
+                         std::make_pair(add_table(P, H, 1, L, kpf),
+                                        add_table(P, L, 0, P / 2 + 1, kpa)))
+                 .first;
+      const long lines = (long)W.T * W.F;
+      LineJob<R> f{};
+      f.src = X.get() + W.model_off;
+      f.dst = S0.get() + W.model_off;
+      f.lines = lines;
+      f.P = P;
+      f.L = L;
+      f.rows = H;
+      f.kout = L;
+      f.kpad = kpf;
+      f.pid = W.problem;
+      LineJob<R> a = f;
+      a.src = S0.get() + W.model_off;
+      a.dst = X.get() + W.model_off;
+      a.rows = L;
+      a.kout = P / 2 + 1;
+      a.kpad = kpa;
+      jf.push_back(f);
+      ja.push_back(a);
+      tf.push_back(it->second.first);
+      ta.push_back(it->second.second);
+      for (long l = 0; l < lines; l += line_lines<R>()) {
+        line_cj.push_back((int)jf.size() - 1);
+        line_cl.push_back(l);
+      }
+      sf_max = std::max(sf_max, line_fwd_smem<R>(P, H, kpf));
+      sa_max = std::max(sa_max, line_adj_smem<R>(P, L, kpa));
+    }
+    if (jf.empty()) return;
+    line_tab.upload(tab, stream);
+    for (size_t i = 0; i < jf.size(); ++i) {
+      jf[i].tab_c = line_tab.get() + tf[i];
+      jf[i].tab_s = jf[i].tab_c + (long)jf[i].rows * jf[i].kpad;
+      ja[i].tab_c = line_tab.get() + ta[i];
+      ja[i].tab_s = ja[i].tab_c + (long)ja[i].rows * ja[i].kpad;
+    }
+    make_line_launch(line_fwd, jf, sf_max);
+    make_line_launch(line_adj, ja, sa_max);
+    line_adj_host = ja;
+  }
+
+  void make_line_launch(LineLaunch &Lc, const std::vector<LineJob<R>> &jobs, size_t smem) {
+    Lc.jobs.upload(jobs, stream);
+    Lc.cta_job.upload(line_cj, stream);
+    Lc.cta_line0.upload(line_cl, stream);
+    Lc.n_cta = (int)line_cj.size();
+    Lc.smem = smem;
   }
 
   // Times every candidate of a class (three rounds over the candidates, each
@@ -1496,6 +1611,9 @@ class Engine {
       build_wavelet_fast(wj, wt_base);
     }
 
+    // ---- one-axis windows of other lengths (line kernels)
+    build_line_kernels();
+
     // ---- space-axis passes (generic path)
     maxD = max_d_generic;
     fwd.resize(maxD);
@@ -1505,7 +1623,7 @@ class Engine {
       std::vector<AxisJob<R>> jf, ju, jp;
       for (int w = 0; w < nw; ++w) {
         const WindowPlan &W = plan.windows[w];
-        if (W.D <= k || win_class[w] >= 0) continue;
+        if (W.D <= k || win_class[w] >= 0 || win_line[w]) continue;
         const long TF = (long)W.T * W.F;
         {  // forward: axis D-1-k, inverse FFT, crop P -> L
           const int a = W.D - 1 - k;
@@ -1632,11 +1750,18 @@ class Engine {
       size_t i = 0;
       for (int w = 0; w < (int)plan.windows.size(); ++w) {
         const WindowPlan &W = plan.windows[w];
-        if (W.D <= (int)k || win_class[w] >= 0) continue;
+        if (W.D <= (int)k || win_class[w] >= 0 || win_line[w]) continue;
         if ((int)k == W.D - 1) jobs[i].dst = G.get() + W.model_off;
         ++i;
       }
       make_axis_launch(adj_plain[k], jobs);
+    }
+    if (!line_adj_host.empty()) {
+      std::vector<LineJob<R>> jobs = line_adj_host;
+      size_t i = 0;
+      for (int w = 0; w < (int)plan.windows.size(); ++w)
+        if (win_line[w]) jobs[i++].dst = G.get() + plan.windows[w].model_off;
+      make_line_launch(line_adj_plain, jobs, line_adj.smem);
     }
     CK(cudaStreamSynchronize(stream));
   }
@@ -1717,13 +1842,31 @@ class Engine {
     }
   }
 
+  void launch_line_fwd() {
+    if (line_fwd.n_cta == 0) return;
+    line_dft_fwd<R><<<line_fwd.n_cta, kLineThreads, line_fwd.smem, stream>>>(
+        line_fwd.jobs.get(), line_fwd.cta_job.get(), line_fwd.cta_line0.get());
+    CK(cudaGetLastError());
+  }
+
+  void launch_line_adj(const LineLaunch &Lc, int epilogue, R step, R lamb,
+                       const R *lamb_dev = nullptr) {
+    if (Lc.n_cta == 0) return;
+    line_dft_adj<R><<<Lc.n_cta, kLineThreads, Lc.smem, stream>>>(
+        Lc.jobs.get(), Lc.cta_job.get(), Lc.cta_line0.get(), epilogue, step, lamb,
+        multi ? step_dev.get() : nullptr, lamb_dev, multi ? pmax.get() : scalar.get());
+    CK(cudaGetLastError());
+  }
+
   void launch_space_fwd_all() {
     for (const auto &cp : classes) launch_space_fwd(*cp);
+    launch_line_fwd();
     for (size_t k = 0; k < fwd.size(); ++k) launch_axis(fwd[k], 1, kStore, 0, 0);
   }
 
   void launch_space_adj_all(int epilogue, R step, R lamb, const R *lamb_dev) {
     for (const auto &cp : classes) launch_space_adj(*cp, cp->pl_adj, epilogue, step, lamb, lamb_dev);
+    launch_line_adj(line_adj, epilogue, step, lamb, lamb_dev);
     for (size_t k = 0; k < adj_update.size(); ++k)
       launch_axis(adj_update[k], 0, epilogue, step, lamb, lamb_dev);
   }
@@ -1784,7 +1927,9 @@ class Engine {
   int kernels_per_iteration() const {
     int n = 2 * (int)classes.size();  // space passes, forward and adjoint
     for (const auto &gp : tgroups) n += (gp->tf.n_cta ? 1 : 0) + (gp->ta.n_cta ? 1 : 0);
-    n += (int)fwd.size() + (int)adj_update.size();
+    for (const auto *v : {&fwd, &adj_update})
+      for (const AxisLaunch &L : *v) n += L.n_cta ? 1 : 0;
+    n += (line_fwd.n_cta ? 1 : 0) + (line_adj.n_cta ? 1 : 0);
     n += (time_fwd.n_cta ? 1 : 0) + (time_adj.n_cta ? 1 : 0);
     n += (g_fwd.n_chunk ? 1 : 0) + 1;  // residual gather, threshold schedule
     if (wavelets) n += wav_fast ? 2 : 3;
@@ -2280,6 +2425,9 @@ int agd_gpu_problem_info(agd_gpu_problem const *pb, long int *info) {
   info[19] = e.tgroups.empty() ? 0 : (long)e.tgroups[0]->fwd_vars.size();
   info[20] = e.wav_fast ? e.wav_pick : -1;
   info[21] = e.wav_candidates;
+  long n_line = 0;
+  for (char c : e.win_line) n_line += c ? 1 : 0;
+  info[22] = n_line;
   return 0;
 }
 
@@ -2329,6 +2477,7 @@ int agd_gpu_adjoint(agd_gpu_problem *pb, AGD_TYPE const *record, AGD_TYPE *model
     for (const auto &cp : e.classes) e.launch_space_adj(*cp, cp->pl_adj_plain, agd::kStore, 0, 0);
     for (size_t k = 0; k < e.adj_plain.size(); ++k)
       e.launch_axis(e.adj_plain[k], 0, agd::kStore, 0, 0);
+    e.launch_line_adj(e.line_adj_plain, agd::kStore, 0, 0);
     e.model_to_ref(e.G.get(), model);
     return 0;
   });

@@ -164,7 +164,7 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-PROFILES = {"two_volume_3d": "space_time_fast_two_volume_3d_small.md",
+PROFILES = {"two_volume_3d": "kernels_two_volume_3d_small.md",
             "vibroseis_4d": "kernels_vibroseis_4d_small.md"}
 
 

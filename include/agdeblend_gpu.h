@@ -40,7 +40,7 @@ int agd_gpu_problem_create(int n_patches, int const *volumes, int const *n_dims,
 
 void agd_gpu_problem_destroy(agd_gpu_problem *problem);
 
-/* info (22 values): [0] windows, [1] model complex elements, [2] record
+/* info (23 values): [0] windows, [1] model complex elements, [2] record
  * samples, [3] window traces (all windows), [4] record segments, [5] mute
  * spans, [6] device bytes held, [7] blend contributions per forward,
  * [8] 1 if the shape-specialised kernels serve every window, 2 if they
@@ -52,7 +52,9 @@ void agd_gpu_problem_destroy(agd_gpu_problem *problem);
  * the shape-specialised kernels, [16] windows on them, [17] and [18] the
  * time-kernel candidates picked for the first time group (-1 without
  * one), [19] its number of candidates, [20] the wavelet-kernel candidate
- * picked (-1 without the prime-factor kernel), [21] their number. */
+ * picked (-1 without the prime-factor kernel), [21] their number, [22]
+ * windows with one space axis on the line-DFT kernels (lengths without a
+ * shape-specialised kernel, up to 128). */
 int agd_gpu_problem_info(agd_gpu_problem const *problem, long int *info);
 
 /* Kernel families serving the first window class and time group, as a
