@@ -339,8 +339,6 @@ class Engine {
   DevArray<R> line_tab;        // per (P, L): forward and adjoint cos / sin tables
   std::vector<char> win_line;  // 1: window on the line kernels
   std::vector<LineJob<R>> line_adj_host;  // adjoint jobs (the plain adjoint's, re-aimed)
-  std::vector<int> line_cj;
-  std::vector<long> line_cl;
   TimeLaunch time_fwd, time_adj, wav;
 
   // Shape-specialised kernels (fast.cuh).  Windows are grouped into classes
@@ -1064,8 +1062,8 @@ class Engine {
       if (win_class[w] >= 0 || W.D != 1 || W.P[0] > kLineMaxP || W.P[0] < 3) continue;
       const int P = W.P[0], L = W.L[0];
       const int H = (P - 1) / 2;
-      const size_t sf = line_fwd_smem<R>(P, H, (L + 3) / 4 * 4);
-      const size_t sa = line_adj_smem<R>(P, L, (P / 2 + 1 + 3) / 4 * 4);
+      const size_t sf = line_fwd_smem<R>(P, H, (L + 3) / 4 * 4, 4);
+      const size_t sa = line_adj_smem<R>(P, L, (P / 2 + 1 + 3) / 4 * 4, 4);
       if (std::max(sf, sa) <= (size_t)smem_max) win_line[w] = 1;
     }
     n_generic = 0;
@@ -1099,9 +1097,6 @@ class Engine {
     };
     std::vector<LineJob<R>> jf, ja;
     std::vector<long> tf, ta;  // table offsets of each job
-    line_cj.clear();
-    line_cl.clear();
-    size_t sf_max = 0, sa_max = 0;
     for (int w = 0; w < nw; ++w) {
       if (!win_line[w]) continue;
       const WindowPlan &W = plan.windows[w];
@@ -1131,16 +1126,12 @@ class Engine {
       a.rows = L;
       a.kout = P / 2 + 1;
       a.kpad = kpa;
+      f.nl = line_pick_nl(P, L, true);
+      a.nl = line_pick_nl(P, L, false);
       jf.push_back(f);
       ja.push_back(a);
       tf.push_back(it->second.first);
       ta.push_back(it->second.second);
-      for (long l = 0; l < lines; l += line_lines<R>()) {
-        line_cj.push_back((int)jf.size() - 1);
-        line_cl.push_back(l);
-      }
-      sf_max = std::max(sf_max, line_fwd_smem<R>(P, H, kpf));
-      sa_max = std::max(sa_max, line_adj_smem<R>(P, L, kpa));
     }
     if (jf.empty()) return;
     line_tab.upload(tab, stream);
@@ -1150,16 +1141,53 @@ class Engine {
       ja[i].tab_c = line_tab.get() + ta[i];
       ja[i].tab_s = ja[i].tab_c + (long)ja[i].rows * ja[i].kpad;
     }
-    make_line_launch(line_fwd, jf, sf_max);
-    make_line_launch(line_adj, ja, sa_max);
+    make_line_launch(line_fwd, jf, true);
+    make_line_launch(line_adj, ja, false);
     line_adj_host = ja;
   }
 
-  void make_line_launch(LineLaunch &Lc, const std::vector<LineJob<R>> &jobs, size_t smem) {
+  // Lines per block of a window: a multiple of 4 whose 4-line x 4-output
+  // tiles best fill the block's threads, within a shared-memory budget of
+  // three blocks per SM (two in double; more when even 4 lines need it).
+  int line_pick_nl(int P, int L, bool fwd) const {
+    const int H = (P - 1) / 2;
+    const int kpad = fwd ? (L + 3) / 4 * 4 : (P / 2 + 1 + 3) / 4 * 4;
+    auto smem = [&](int nl) {
+      return fwd ? line_fwd_smem<R>(P, H, kpad, nl) : line_adj_smem<R>(P, L, kpad, nl);
+    };
+    const size_t budget =
+        std::max<size_t>(sizeof(R) == sizeof(float) ? 75 * 1024 : 112 * 1024, smem(4));
+    int best = 4;
+    double best_eff = -1.0;
+    for (int nl = 4; nl <= 64 && smem(nl) <= budget; nl += 4) {
+      const int tiles = nl / 4 * (kpad / 4);
+      const int rounds = (tiles + kLineThreads - 1) / kLineThreads;
+      const double eff = (double)tiles / (rounds * kLineThreads);
+      if (eff >= best_eff - 1e-9) {
+        best_eff = eff;
+        best = nl;
+      }
+    }
+    return best;
+  }
+
+  void make_line_launch(LineLaunch &Lc, const std::vector<LineJob<R>> &jobs, bool fwd) {
+    std::vector<int> cj;
+    std::vector<long> cl;
+    size_t smem = 0;
+    for (size_t i = 0; i < jobs.size(); ++i) {
+      const LineJob<R> &j = jobs[i];
+      for (long l = 0; l < j.lines; l += j.nl) {
+        cj.push_back((int)i);
+        cl.push_back(l);
+      }
+      smem = std::max(smem, fwd ? line_fwd_smem<R>(j.P, j.rows, j.kpad, j.nl)
+                                : line_adj_smem<R>(j.P, j.L, j.kpad, j.nl));
+    }
     Lc.jobs.upload(jobs, stream);
-    Lc.cta_job.upload(line_cj, stream);
-    Lc.cta_line0.upload(line_cl, stream);
-    Lc.n_cta = (int)line_cj.size();
+    Lc.cta_job.upload(cj, stream);
+    Lc.cta_line0.upload(cl, stream);
+    Lc.n_cta = (int)cj.size();
     Lc.smem = smem;
   }
 
@@ -1761,7 +1789,7 @@ class Engine {
       size_t i = 0;
       for (int w = 0; w < (int)plan.windows.size(); ++w)
         if (win_line[w]) jobs[i++].dst = G.get() + plan.windows[w].model_off;
-      make_line_launch(line_adj_plain, jobs, line_adj.smem);
+      make_line_launch(line_adj_plain, jobs, false);
     }
     CK(cudaStreamSynchronize(stream));
   }

@@ -33,13 +33,6 @@ namespace agd {
 constexpr int kLineThreads = 128;
 constexpr int kLineMaxP = 128;    // longest axis served
 
-// lines per block: 32 in float, 16 in double (the blocks of the longest
-// axes then still fit in shared memory)
-template <typename R>
-__host__ __device__ constexpr int line_lines() {
-  return sizeof(R) == sizeof(float) ? 32 : 16;
-}
-
 // One window's lines for the line kernels.
 template <typename R>
 struct LineJob {
@@ -52,24 +45,26 @@ struct LineJob {
   int rows;          // forward H = (P - 1) / 2, adjoint L
   int kout;          // forward L, adjoint P / 2 + 1
   int kpad;          // kout rounded up to a multiple of 4
+  int nl;            // lines per block (a multiple of 4), chosen per window
   int pid;           // problem of the window
 };
 
-// Shared-memory bytes of a block (csize / rsize: bytes of a complex / real
-// value).  Forward: lines [NL][P], pair sums and differences [H][NL] each,
-// x_0 and x_{P/2} [NL] each, tables [H][kpad] each.  Adjoint: lines [NL][L]
-// then results [NL][P], transposed lines [L][NL], tables [L][kpad] each.
-// Every part is a whole number of 16-byte units (NL a multiple of 16, kpad
-// of 4).
+// Shared-memory bytes of a block of nl lines (regions rounded to 16 bytes).
+// Forward: lines [nl][P] (then results [nl][L]), pair sums and differences
+// [H][nl + 1] each (an odd row stride: the transposing writes hit distinct
+// banks), x_0 and x_{P/2} [nl] each, tables [H][kpad] each.  Adjoint: lines
+// [nl][L], model lines [nl][P] (updated in place, then stored), tables
+// [L][kpad] each.
+__host__ __device__ inline int line_even(int n) { return n + (n & 1); }
 template <typename R>
-size_t line_fwd_smem(int P, int H, int kpad) {
-  constexpr size_t NL = line_lines<R>();
-  return (NL * P + 2 * (size_t)H * NL + 2 * NL) * sizeof(Cx<R>) + 2 * (size_t)H * kpad * sizeof(R);
+size_t line_fwd_smem(int P, int H, int kpad, int nl) {
+  return (size_t)(line_even(nl * P) + 2 * line_even(H * (nl + 1)) + 2 * nl) * sizeof(Cx<R>) +
+         2 * (size_t)H * kpad * sizeof(R);
 }
 template <typename R>
-size_t line_adj_smem(int P, int L, int kpad) {
-  constexpr size_t NL = line_lines<R>();
-  return (NL * P + (size_t)L * NL) * sizeof(Cx<R>) + 2 * (size_t)L * kpad * sizeof(R);
+size_t line_adj_smem(int P, int L, int kpad, int nl) {
+  return (size_t)(line_even(nl * L) + line_even(nl * P)) * sizeof(Cx<R>) +
+         2 * (size_t)L * kpad * sizeof(R);
 }
 
 template <typename R>
@@ -100,22 +95,29 @@ __device__ __forceinline__ void load4(const R *p, R (&v)[4]) {
   }
 }
 
+// floor(x / d) for 0 <= x < 2^22 from r = 1 / d rounded: (x + 1/2) / d is
+// at least 1/(2d) from an integer, the product's relative error below 2^-23
+__device__ __forceinline__ int line_div(int x, float r) {
+  return __float2int_rz(((float)x + 0.5f) * r);
+}
+
 // Forward operator: Z[line][0..L) = crop(IDFT_P(X[line][0..P))).
 template <typename R>
 __global__ void __launch_bounds__(kLineThreads, 3)
     line_dft_fwd(const LineJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
                  const long *__restrict__ cta_line0) {
   using C = Cx<R>;
-  constexpr int NL = line_lines<R>();
   const LineJob<R> job = jobs[cta_job[blockIdx.x]];
   const long l0 = cta_line0[blockIdx.x];
+  const int NL = job.nl;
   const int nl = (int)min((long)NL, job.lines - l0);
   const int P = job.P, L = job.L, H = job.rows, kpad = job.kpad;
+  const int NS = NL + 1;  // row stride of the pair sums
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *buf = reinterpret_cast<C *>(smem_raw);  // [NL][P] in, then [NL][L] out
-  C *ssum = buf + NL * P;                    // [H][NL]
-  C *sdif = ssum + H * NL;                   // [H][NL]
-  C *x0 = sdif + H * NL;                     // [NL]
+  C *ssum = buf + line_even(NL * P);         // [H][NS]
+  C *sdif = ssum + line_even(H * NS);        // [H][NS]
+  C *x0 = sdif + line_even(H * NS);          // [NL]
   C *xh = x0 + NL;                           // [NL]
   R *tc = reinterpret_cast<R *>(xh + NL);    // [H][kpad]
   R *ts = tc + H * kpad;
@@ -125,28 +127,28 @@ __global__ void __launch_bounds__(kLineThreads, 3)
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
-  // pair sums and differences, lines fastest
-  for (int idx = threadIdx.x; idx < H * NL; idx += kLineThreads) {
-    const int j = idx / NL;
-    const int l = idx - j * NL;
-    C s = cmake<C>((R)0, (R)0), d = s;
-    if (l < nl) {
-      const C a = buf[l * P + j + 1];
-      const C b = buf[l * P + P - 1 - j];
-      s = cadd(a, b);
-      d = csub(a, b);
-    }
-    ssum[idx] = s;
-    sdif[idx] = d;
+  // pair sums and differences: reads along each line, writes at the odd
+  // stride NS
+  const float inv_h = 1.0f / (float)H;
+  for (int idx = threadIdx.x; idx < nl * H; idx += kLineThreads) {
+    const int l = line_div(idx, inv_h);
+    const int j = idx - l * H;
+    const C a = buf[l * P + j + 1];
+    const C b = buf[l * P + P - 1 - j];
+    ssum[j * NS + l] = cadd(a, b);
+    sdif[j * NS + l] = csub(a, b);
   }
   for (int l = threadIdx.x; l < NL; l += kLineThreads) {
     x0[l] = l < nl ? buf[l * P] : cmake<C>((R)0, (R)0);
     xh[l] = (l < nl && P % 2 == 0) ? buf[l * P + P / 2] : cmake<C>((R)0, (R)0);
   }
   __syncthreads();
-  // 4 lines x 4 outputs per thread; results into buf as [nl][L]
+  // 4 lines x 4 outputs per thread; results into buf as [nl][L] (lines past
+  // nl of the window's last block are computed from stale values, never
+  // stored)
   const int kt_n = kpad / 4;
-  for (int tile = threadIdx.x; tile < (NL / 4) * kt_n; tile += kLineThreads) {
+  const int lt_n = (nl + 3) / 4;
+  for (int tile = threadIdx.x; tile < lt_n * kt_n; tile += kLineThreads) {
     const int lt = tile / kt_n;
     const int kt = tile - lt * kt_n;
     R re[4][4], im[4][4];
@@ -162,11 +164,11 @@ __global__ void __launch_bounds__(kLineThreads, 3)
       }
     }
     for (int j = 0; j < H; ++j) {
-      C s[4], d[4];
+      C sv[4], dv[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        s[i] = ssum[j * NL + 4 * lt + i];
-        d[i] = sdif[j * NL + 4 * lt + i];
+        sv[i] = ssum[j * NS + 4 * lt + i];
+        dv[i] = sdif[j * NS + 4 * lt + i];
       }
       R c[4], sn[4];
       load4<R>(tc + j * kpad + 4 * kt, c);
@@ -175,8 +177,8 @@ __global__ void __launch_bounds__(kLineThreads, 3)
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-          re[i][m] += s[i].x * c[m] - d[i].y * sn[m];
-          im[i][m] += s[i].y * c[m] + d[i].x * sn[m];
+          re[i][m] += sv[i].x * c[m] - dv[i].y * sn[m];
+          im[i][m] += sv[i].y * c[m] + dv[i].x * sn[m];
         }
     }
 #pragma unroll
@@ -193,37 +195,58 @@ __global__ void __launch_bounds__(kLineThreads, 3)
 }
 
 // Adjoint with the ISTA update fused (epilogues as axis_pass):
-// G[line][0..P) = DFT_P(pad(Z[line][0..L))), then X <- update(X, G).
+// G[line][0..P) = DFT_P(pad(Z[line][0..L))), then X <- update(X, G).  The
+// block's model lines are copied into shared memory with its input lines,
+// behind the transform; each tile updates its outputs there in place, and
+// the updated lines are stored as one contiguous run.
 template <typename R>
 __global__ void __launch_bounds__(kLineThreads, 3)
     line_dft_adj(const LineJob<R> *__restrict__ jobs, const int *__restrict__ cta_job,
                  const long *__restrict__ cta_line0, int epilogue, R step_arg, R lamb_arg,
                  const R *step_dev, const R *lamb_dev, R *max_out) {
   using C = Cx<R>;
-  constexpr int NL = line_lines<R>();
   const LineJob<R> job = jobs[cta_job[blockIdx.x]];
   const long l0 = cta_line0[blockIdx.x];
+  const int NL = job.nl;
   const int nl = (int)min((long)NL, job.lines - l0);
   const int P = job.P, L = job.L, kpad = job.kpad, KO = job.kout;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *buf = reinterpret_cast<C *>(smem_raw);  // [NL][L] in, then [NL][P] results
-  C *xt = buf + NL * P;                      // [L][NL]
-  R *tc = reinterpret_cast<R *>(xt + L * NL);  // [L][kpad]
+  C *xin = reinterpret_cast<C *>(smem_raw);  // [NL][L]
+  C *xm = xin + line_even(NL * L);           // [NL][P] model, updated in place
+  R *tc = reinterpret_cast<R *>(xm + line_even(NL * P));  // [L][kpad]
   R *ts = tc + L * kpad;
-  line_copy_in<R>(buf, job.src + l0 * L, nl * L);
+  C *dst = job.dst + l0 * P;
+  const bool need_x = epilogue != kStore;
+  line_copy_in<R>(xin, job.src + l0 * L, nl * L);
   line_table_in<R>(tc, job.tab_c, L * kpad);
   line_table_in<R>(ts, job.tab_s, L * kpad);
+  if (need_x) line_copy_in<R>(xm, dst, nl * P);
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
-  for (int idx = threadIdx.x; idx < L * NL; idx += kLineThreads) {
-    const int j = idx / NL;
-    const int l = idx - j * NL;
-    xt[idx] = l < nl ? buf[l * L + j] : cmake<C>((R)0, (R)0);
-  }
-  __syncthreads();
+  const bool multi = step_dev != nullptr;
+  const R step = multi ? step_dev[job.pid] : step_arg;
+  const R lamb = lamb_dev != nullptr ? lamb_dev[multi ? job.pid : 0] : lamb_arg;
+  const R lamb_sq = lamb * lamb;
+  R local_max = (R)0;
+  auto update = [&](C *xp, C g) {
+    if (!need_x) {
+      *xp = g;
+      return;
+    }
+    const C x = *xp;
+    C xn = cmake<C>(sub_rn<R>(x.x, mul_rn<R>(step, g.x)), sub_rn<R>(x.y, mul_rn<R>(step, g.y)));
+    if (epilogue == kUpdateThreshold) {
+      xn = soft_threshold<R>(xn, lamb, lamb_sq);
+    } else {
+      const R a2 = abs_sq<R>(xn);
+      local_max = a2 > local_max ? a2 : local_max;
+    }
+    *xp = xn;
+  };
   const int kt_n = kpad / 4;
-  for (int tile = threadIdx.x; tile < (NL / 4) * kt_n; tile += kLineThreads) {
+  const int lt_n = (nl + 3) / 4;
+  for (int tile = threadIdx.x; tile < lt_n * kt_n; tile += kLineThreads) {
     const int lt = tile / kt_n;
     const int kt = tile - lt * kt_n;
     C a[4][4], bsum[4][4];
@@ -234,7 +257,7 @@ __global__ void __launch_bounds__(kLineThreads, 3)
     for (int j = 0; j < L; ++j) {
       C x[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) x[i] = xt[j * NL + 4 * lt + i];
+      for (int i = 0; i < 4; ++i) x[i] = xin[(4 * lt + i) * L + j];
       R c[4], sn[4];
       load4<R>(tc + j * kpad + 4 * kt, c);
       load4<R>(ts + j * kpad + 4 * kt, sn);
@@ -255,34 +278,12 @@ __global__ void __launch_bounds__(kLineThreads, 3)
         const int l = 4 * lt + i, k = 4 * kt + m;
         if (l >= nl || k >= KO) continue;
         const C A = a[i][m], B = bsum[i][m];
-        buf[l * P + k] = cmake<C>(A.x + B.y, A.y - B.x);  // A - i B
-        if (k > 0 && P - k != k) buf[l * P + P - k] = cmake<C>(A.x - B.y, A.y + B.x);
+        update(xm + l * P + k, cmake<C>(A.x + B.y, A.y - B.x));  // A - i B
+        if (k > 0 && P - k != k) update(xm + l * P + P - k, cmake<C>(A.x - B.y, A.y + B.x));
       }
   }
   __syncthreads();
-  // update the model lines (contiguous over the block's lines)
-  const bool multi = step_dev != nullptr;
-  const R step = multi ? step_dev[job.pid] : step_arg;
-  const R lamb = lamb_dev != nullptr ? lamb_dev[multi ? job.pid : 0] : lamb_arg;
-  const R lamb_sq = lamb * lamb;
-  R local_max = (R)0;
-  C *dst = job.dst + l0 * P;
-  for (int e = threadIdx.x; e < nl * P; e += kLineThreads) {
-    const C g = buf[e];
-    if (epilogue == kStore) {
-      dst[e] = g;
-      continue;
-    }
-    const C x = dst[e];
-    C xn = cmake<C>(sub_rn<R>(x.x, mul_rn<R>(step, g.x)), sub_rn<R>(x.y, mul_rn<R>(step, g.y)));
-    if (epilogue == kUpdateThreshold) {
-      xn = soft_threshold<R>(xn, lamb, lamb_sq);
-    } else {
-      const R a2 = abs_sq<R>(xn);
-      local_max = a2 > local_max ? a2 : local_max;
-    }
-    dst[e] = xn;
-  }
+  for (int e = threadIdx.x; e < nl * P; e += kLineThreads) dst[e] = xm[e];
   if (epilogue == kUpdateMax) {
     __shared__ R red[32];
     const R m = block_max<R>(local_max, red);
