@@ -148,7 +148,10 @@ def deblend(volumes, window_shapes, coords, shottimes, channels, trace_types, in
     fn = lib.agd_deblend
     if capi.call_deblend(fn, args, initial_factor, n_its, print_freq):
         raise RuntimeError("Error in call to agd_deblend")
-    return [d.astype(dtype) for d in args.data]
+    # args.data are this call's own copies of the input, overwritten with the
+    # result: returned as they are (a second copy would cost a full pass
+    # over the data)
+    return args.data
 
 
 def deblend_batch(problems, initial_factor, n_its):
@@ -169,7 +172,7 @@ def deblend_batch(problems, initial_factor, n_its):
     fn = capi.bind_deblend_batch(lib, dtype)
     if fn(*batch.problem_args(), initial_factor, n_its, batch.data_p):
         raise RuntimeError("Error in call to agd_deblend_batch")
-    return [[d.astype(dtype) for d in a.data] for a in args]
+    return [a.data for a in args]
 
 
 def blend(shottimes, channels, trace_types, data, blend_mode, taper_length=0, n_times_out=None,

@@ -13,6 +13,7 @@
 #include <map>
 #include <mutex>
 #include <memory>
+#include <chrono>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -2359,6 +2360,26 @@ int create_from_plan(const std::vector<agd::ProblemArgs> &args, agd::Plan &&plan
   return 0;
 }
 
+// Phase times of an agd_deblend call on stderr when AGD_GPU_TIMING=1: host
+// wall clock between marks, each mark after a device synchronisation.
+struct PhaseTimer {
+  bool on = false;
+  std::chrono::steady_clock::time_point t;
+  PhaseTimer() {
+    const char *env = std::getenv("AGD_GPU_TIMING");
+    on = env != nullptr && env[0] == '1';
+    if (on) t = std::chrono::steady_clock::now();
+  }
+  void mark(const char *phase) {
+    if (!on) return;
+    cudaDeviceSynchronize();
+    const auto n = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "agd timing: %-12s %8.2f ms\n", phase,
+                 std::chrono::duration<double, std::milli>(n - t).count());
+    t = n;
+  }
+};
+
 int create_problem(const agd::ProblemArgs &a, agd_gpu_problem **out) {
   *out = nullptr;
   agd::Plan plan;
@@ -2741,15 +2762,36 @@ int agd_deblend(int n_patches, int const *volumes, int const *n_dims,
     std::fprintf(stderr, "ERROR in agd_deblend\n");
     return 1;
   }
+  PhaseTimer timer;
+  timer.mark("validate");
   agd_gpu_problem *pb = nullptr;
-  if (create_problem(a, &pb)) {
+  agd::Plan plan;
+  if (agd::build_plan(a, plan)) {
     std::fprintf(stderr, "ERROR in agd_deblend\n");
     return 1;
   }
+  timer.mark("plan");
+  if (create_from_plan({a}, std::move(plan), &pb)) {
+    std::fprintf(stderr, "ERROR in agd_deblend\n");
+    return 1;
+  }
+  timer.mark("set-up");
   if (pb->eng->stepsize > (AGD_TYPE)0.3)
     std::printf("WARNING: There does not appear to be any overlap between shots\n");
-  const int rc = agd_gpu_solve(pb, initial_factor, n_its, print_freq, data);
+  const int rc = guarded("agd_deblend", [&] {
+    agd::EngineR &e = *pb->eng;
+    e.upload_data(data);
+    timer.mark("upload");
+    pb->input_blend();
+    timer.mark("input blend");
+    e.solve(initial_factor, n_its, print_freq);
+    timer.mark("solve");
+    e.download_data(data);
+    timer.mark("download");
+    return 0;
+  });
   delete pb;
+  timer.mark("teardown");
   return rc;
 }
 
