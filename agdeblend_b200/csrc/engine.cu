@@ -413,6 +413,8 @@ class Engine {
   int n_generic = 0;            // windows on the generic space kernels
   int max_d_generic = 0;        // space dimensions of those windows
   int n_sm = 148;
+  int sm_smem = 233472;      // shared memory per SM (bytes)
+  int block_reserved = 1024;  // shared memory the system reserves per block
   GatherLaunch g_fwd, g_input;
   std::vector<long> trace_off;   // per window, in reals
   std::vector<long> patch_off;   // per patch, in reals
@@ -443,6 +445,8 @@ class Engine {
       int dev = 0;
       CK(cudaGetDevice(&dev));
       CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+      CK(cudaDeviceGetAttribute(&sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+      CK(cudaDeviceGetAttribute(&block_reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
     }
     set_smem_limits();
     try {
@@ -1149,15 +1153,18 @@ class Engine {
 
   // Lines per block of a window: a multiple of 4 whose 4-line x 4-output
   // tiles best fill the block's threads, within a shared-memory budget of
-  // three blocks per SM (two in double; more when even 4 lines need it).
+  // three blocks per SM (two in double; more when even 4 lines need it),
+  // counting the memory the system reserves per block and the kernels'
+  // static arrays (at most 256 bytes).
   int line_pick_nl(int P, int L, bool fwd) const {
     const int H = (P - 1) / 2;
     const int kpad = fwd ? (L + 3) / 4 * 4 : (P / 2 + 1 + 3) / 4 * 4;
     auto smem = [&](int nl) {
       return fwd ? line_fwd_smem<R>(P, H, kpad, nl) : line_adj_smem<R>(P, L, kpad, nl);
     };
+    const int blocks = sizeof(R) == sizeof(float) ? 3 : 2;
     const size_t budget =
-        std::max<size_t>(sizeof(R) == sizeof(float) ? 75 * 1024 : 112 * 1024, smem(4));
+        std::max<size_t>((size_t)(sm_smem / blocks - block_reserved - 256), smem(4));
     int best = 4;
     double best_eff = -1.0;
     for (int nl = 4; nl <= 64 && smem(nl) <= budget; nl += 4) {
