@@ -81,9 +81,8 @@ class DevicePool {
   static void put(void *p) {
     if (p == nullptr) return;
     int dev = 0;
-    size_t freeb = 0, total = 0;
-    if (!enabled() || cudaGetDevice(&dev) != cudaSuccess ||
-        cudaMemGetInfo(&freeb, &total) != cudaSuccess) {
+    size_t total = 0;
+    if (!enabled() || cudaGetDevice(&dev) != cudaSuccess || (total = device_total(dev)) == 0) {
       drop(p);
       return;
     }
@@ -125,6 +124,27 @@ class DevicePool {
   }
 
  private:
+  // the device's memory size, queried once (a memory-information query on
+  // every return would cost a driver call each)
+  static size_t device_total(int dev) {
+    {
+      std::lock_guard<std::mutex> g(mu());
+      auto it = totals().find(dev);
+      if (it != totals().end()) return it->second;
+    }
+    size_t freeb = 0, total = 0;
+    if (cudaMemGetInfo(&freeb, &total) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    std::lock_guard<std::mutex> g(mu());
+    totals()[dev] = total;
+    return total;
+  }
+  static std::map<int, size_t> &totals() {
+    static std::map<int, size_t> m;
+    return m;
+  }
   static bool enabled() {
     static const bool on = [] {
       const char *env = std::getenv("AGD_GPU_CACHE");
@@ -2851,26 +2871,53 @@ int agd_deblend_batch(int n_problems, int const *n_patches, int const *const *vo
     std::fprintf(stderr, "ERROR: invalid batch arguments\nERROR in agd_deblend_batch\n");
     return 1;
   }
+  PhaseTimer timer;
   std::vector<AGD_TYPE *> all_data;
+  std::vector<agd::ProblemArgs> args;
   for (int q = 0; q < n_problems; ++q) {
-    const agd::ProblemArgs a =
-        batch_args(q, n_patches, volumes, n_dims, window_shapes, coords, shapes, shottimes,
-                   channels, trace_types, wavelet_lengths, wavelet_idxs, wavelets);
-    if (data[q] == nullptr || agd::check_deblend_inputs(a, initial_factor, n_its, data[q])) {
+    if (volumes == nullptr || n_dims == nullptr || window_shapes == nullptr ||
+        coords == nullptr || shapes == nullptr || shottimes == nullptr || channels == nullptr ||
+        trace_types == nullptr) {
+      std::fprintf(stderr, "ERROR: invalid batch arguments\nERROR in agd_deblend_batch\n");
+      return 1;
+    }
+    args.push_back(batch_args(q, n_patches, volumes, n_dims, window_shapes, coords, shapes,
+                              shottimes, channels, trace_types, wavelet_lengths, wavelet_idxs,
+                              wavelets));
+    if (data[q] == nullptr ||
+        agd::check_deblend_inputs(args.back(), initial_factor, n_its, data[q])) {
       std::fprintf(stderr, "ERROR in problem %d of agd_deblend_batch\n", q);
       return 1;
     }
     for (int p = 0; p < n_patches[q]; ++p) all_data.push_back(data[q][p]);
   }
+  timer.mark("validate");
   agd_gpu_problem *pb = nullptr;
-  if (agd_gpu_batch_create(n_problems, n_patches, volumes, n_dims, window_shapes, coords,
-                           shapes, shottimes, channels, trace_types, wavelet_lengths,
-                           wavelet_idxs, wavelets, &pb)) {
+  agd::Plan plan;
+  if (agd::build_batch_plan(args, plan)) {
     std::fprintf(stderr, "ERROR in agd_deblend_batch\n");
     return 1;
   }
-  const int rc = agd_gpu_solve(pb, initial_factor, n_its, 0, all_data.data());
+  timer.mark("plan");
+  if (create_from_plan(args, std::move(plan), &pb)) {
+    std::fprintf(stderr, "ERROR in agd_deblend_batch\n");
+    return 1;
+  }
+  timer.mark("set-up");
+  const int rc = guarded("agd_deblend_batch", [&] {
+    agd::EngineR &e = *pb->eng;
+    e.upload_data(all_data.data());
+    timer.mark("upload");
+    pb->input_blend();
+    timer.mark("input blend");
+    e.solve(initial_factor, n_its, 0);
+    timer.mark("solve");
+    e.download_data(all_data.data());
+    timer.mark("download");
+    return 0;
+  });
   delete pb;
+  timer.mark("teardown");
   return rc;
 }
 
