@@ -9,6 +9,7 @@ the operator checks are those of test_gpu_operators (1e-5 relative L2 and
 the dot test in float, 1e-11 in double).  Solves are compared with the
 generic FFT passes (AGD_GPU_GENERIC=1), and a batch of gathers on the line
 kernels with the same gathers solved one by one."""
+import dataclasses
 import os
 
 import numpy as np
@@ -59,6 +60,20 @@ def test_line_operators_double(name):
     sv = _gather(name, seed=4200)
     assert _line_windows(sv, np.float64)[0] > 0
     _check_operators(sv, np.float64, 1)
+
+
+@pytest.mark.parametrize("name", ["P83_prime", "P42_even_enlarged"])
+def test_line_operators_with_wavelet(name):
+    # a source wavelet on every live trace: the wavelet stage runs on the
+    # traces around the line kernels' space transforms
+    sv = _gather(name, seed=4600)
+    rng = np.random.default_rng(4601)
+    w = (rng.standard_normal(24) * np.hanning(24)).astype(np.float32)
+    n_tr = int(np.asarray(sv.trace_types[0]).size)
+    sv = dataclasses.replace(sv, wavelet_lengths=[len(w)],
+                             wavelet_idxs=[np.zeros(n_tr, np.int32)], wavelets=[w])
+    assert _line_windows(sv)[0] > 0
+    _check_operators(sv, np.float32)
 
 
 def test_lengths_above_the_limit_stay_generic():
