@@ -891,6 +891,7 @@ class Engine {
         add_fwd<2, 20, 40, 1, 384, 16, 2, 1>(c);
         add_fwd<2, 20, 40, 1, 256, 12, 1, 2>(c);
         add_fwd<2, 20, 40, 1, 256, 6, 2, 2>(c);
+        add_fwd<2, 20, 40, 1, 192, 6, 1, 3>(c);
         add_adj<2, 20, 40, 1, 384, 11, 2, 1>(c);
         add_adj<2, 20, 40, 1, 256, 12, 1, 2>(c);
         add_adj<2, 20, 40, 1, 256, 5, 2, 2>(c);
