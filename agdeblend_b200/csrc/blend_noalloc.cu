@@ -1,11 +1,11 @@
 // agd_blend_device_noalloc: blending for callers that cannot allocate device
 // memory.
 //
-// Some callers may not call cudaMalloc at all: code that runs while a CUDA
-// stream is being captured into a graph (allocation is not permitted there),
-// plugin hosts and frameworks that own every byte of device memory through
-// their own pool, or real-time code that has to avoid the allocator's
-// latency and possible failure.  This entry point does the work of agd_blend
+// Some callers may not call cudaMalloc at all: plugin hosts and frameworks
+// that own every byte of device memory through their own pool (an
+// allocation behind their back can fail or break their accounting), or
+// real-time code that has to avoid the allocator's latency and possible
+// failure.  This entry point does the work of agd_blend
 // on data that is already on the device, and keeps every intermediate (the
 // blended record and the lookup tables the kernels read) in one fixed array
 // that is part of the library image: kScratchBytes of device memory that

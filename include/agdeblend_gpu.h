@@ -174,9 +174,9 @@ int agd_gpu_problem_steps(agd_gpu_problem const *problem, AGD_TYPE *steps);
  * to the device.  AGD_GPU_CACHE=0 in the environment disables the cache. */
 void agd_gpu_release_cache(void);
 
-/* agd_blend for callers that cannot allocate device memory (code running
- * inside a CUDA stream capture, hosts whose pool owns all device memory,
- * latency-critical callers).  No counterpart in the reference: it is an
+/* agd_blend for callers that cannot allocate device memory (hosts whose own
+ * pool owns all device memory, real-time callers that must not wait on or
+ * fail in the allocator).  No counterpart in the reference: it is an
  * addition of this library.  Same arguments and results as agd_blend, except
  * that the data are device pointers - data_dev holds all input patches one
  * after another ([n_traces][n_times] each), data_out_dev receives all output

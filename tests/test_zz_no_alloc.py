@@ -1,6 +1,6 @@
 """agd_blend_device_noalloc: blending for callers that may not allocate device
-memory (work recorded into a CUDA graph, hosts whose memory pool owns the
-device, latency-critical code).  It must give what agd_blend gives on the
+memory (hosts whose memory pool owns the device, real-time code that must
+not wait on or fail in the allocator).  It must give what agd_blend gives on the
 same inputs, call after call, while keeping its intermediates in the
 library's fixed device scratch array.  The device buffers here are made by
 the test (torch) - the entry point itself allocates nothing.
