@@ -467,30 +467,32 @@ __global__ void __launch_bounds__(kThreads)
     for (int i = threadIdx.x; i < nt; i += blockDim.x) tile[i] = contrib[base + i];
     __syncthreads();
     if (mode != kGatherMean && chunk == 2 * (int)blockDim.x) {
-      // two samples per thread, two contributions per step: four loads in
+      // two samples per thread, four contributions per step: eight loads in
       // flight, added in list order (the order of the serial sum).  A run
       // lies inside the record, so samples past its end are never covered.
       const long s0 = c0 + threadIdx.x;
       const bool ovw = mode == kGatherOverwrite;
       R a0 = acc[0], a1 = acc[1];
       int c = 0;
-      for (; c + 2 <= nt; c += 2) {
-        const Contrib ca = tile[c], cb = tile[c + 1];
-        const long oa = s0 - ca.rec, ob = s0 - cb.rec;
-        const bool ka0 = (unsigned long)oa < (unsigned long)ca.n;
-        const bool ka1 = (unsigned long)(oa + blockDim.x) < (unsigned long)ca.n;
-        const bool kb0 = (unsigned long)ob < (unsigned long)cb.n;
-        const bool kb1 = (unsigned long)(ob + blockDim.x) < (unsigned long)cb.n;
-        const R va0 = ka0 ? src[ca.src + oa] : (R)0;
-        const R va1 = ka1 ? src[ca.src + oa + blockDim.x] : (R)0;
-        const R vb0 = kb0 ? src[cb.src + ob] : (R)0;
-        const R vb1 = kb1 ? src[cb.src + ob + blockDim.x] : (R)0;
-        if (ka0) a0 = ovw ? va0 : a0 + va0;
-        if (ka1) a1 = ovw ? va1 : a1 + va1;
-        if (kb0) a0 = ovw ? vb0 : a0 + vb0;
-        if (kb1) a1 = ovw ? vb1 : a1 + vb1;
+      for (; c + 4 <= nt; c += 4) {
+        R v[4][2];
+        bool k[4][2];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const Contrib cu = tile[c + u];
+          const long o = s0 - cu.rec;
+          k[u][0] = (unsigned long)o < (unsigned long)cu.n;
+          k[u][1] = (unsigned long)(o + blockDim.x) < (unsigned long)cu.n;
+          v[u][0] = k[u][0] ? src[cu.src + o] : (R)0;
+          v[u][1] = k[u][1] ? src[cu.src + o + blockDim.x] : (R)0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (k[u][0]) a0 = ovw ? v[u][0] : a0 + v[u][0];
+          if (k[u][1]) a1 = ovw ? v[u][1] : a1 + v[u][1];
+        }
       }
-      if (c < nt) {
+      for (; c < nt; ++c) {
         const Contrib ca = tile[c];
         const long oa = s0 - ca.rec;
         if ((unsigned long)oa < (unsigned long)ca.n) {
