@@ -121,8 +121,12 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.lines = []
+        self.first = threading.Event()
 
     def start(self):
+        """Starts nvidia-smi and waits (at most 3 s) for its first sample, so
+        that a short timed region that follows is sampled too; the samples
+        taken before the region (the device idle) are dropped."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
@@ -130,12 +134,15 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            self.first.wait(3.0)
+            self.lines.clear()
         except Exception:
             self.proc = None
 
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+            self.first.set()
 
     def stop(self):
         if self.proc is None:
