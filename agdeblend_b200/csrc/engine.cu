@@ -27,6 +27,24 @@
 
 namespace agd {
 
+// Parts of the engine set-up on stderr when AGD_GPU_TIMING=1: host wall
+// clock since the previous mark of this thread, after a device
+// synchronisation (reset: start a new sequence without printing).
+inline void setup_mark(const char *part, bool reset = false) {
+  static const bool on = [] {
+    const char *env = std::getenv("AGD_GPU_TIMING");
+    return env != nullptr && env[0] == '1';
+  }();
+  if (!on) return;
+  static thread_local std::chrono::steady_clock::time_point t;
+  cudaDeviceSynchronize();
+  const auto n = std::chrono::steady_clock::now();
+  if (!reset)
+    std::fprintf(stderr, "agd timing:   set-up/%-12s %8.2f ms\n", part,
+                 std::chrono::duration<double, std::milli>(n - t).count());
+  t = n;
+}
+
 struct DeviceError : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
@@ -1528,6 +1546,7 @@ class Engine {
   }
 
   void build() {
+    setup_mark("", true);
     const long M = plan.model_size;
     const int nw = (int)plan.windows.size();
     // ---- FFT tables and per-window trace tables
@@ -1588,6 +1607,7 @@ class Engine {
     wt_dst.upload(wdst, stream);
     wt_C.upload(wC, stream);
 
+    setup_mark("tables");
     pick_classes();
     X.alloc_pooled(M);
     S0.alloc_pooled(M);
@@ -1639,6 +1659,7 @@ class Engine {
       v.fft = wavelets ? fft.get(W.C) : 0;
     }
     time_jobs.upload(tj, stream);
+    setup_mark("buffers");
     if (!classes.empty() || !tgroups.empty()) {
       opt_in_classes();
       upload_twiddles();
@@ -1668,6 +1689,7 @@ class Engine {
       build_wavelet_fast(wj, wt_base);
     }
 
+    setup_mark("classes");
     // ---- one-axis windows of other lengths (line kernels)
     build_line_kernels();
 
@@ -1726,6 +1748,7 @@ class Engine {
       pending_plain.push_back(jp);
     }
 
+    setup_mark("line, generic");
     // ---- forward blend: window traces into the record, window then trace
     {
       std::vector<Contrib> list;
@@ -2378,7 +2401,9 @@ int create_from_plan(const std::vector<agd::ProblemArgs> &args, agd::Plan &&plan
       pb->tt_p.push_back(pb->trace_types[p].data());
     }
     pb->eng.reset(new agd::EngineR(std::move(plan)));
+    agd::setup_mark("blend, rest");
     pb->eng->compute_stepsize();
+    agd::setup_mark("step size");
   } catch (const std::exception &e) {
     std::fprintf(stderr, "ERROR: %s\n", e.what());
     delete pb;
