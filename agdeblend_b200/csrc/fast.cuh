@@ -3,14 +3,19 @@
 // Every FFT here runs in registers with a compile-time size: a thread owns a
 // whole line (space axes) or one factor of a four-step transform (time axis),
 // so the radix schedule, the index arithmetic and the twiddle offsets are
-// constants.  Twiddles live in __constant__ memory (filled once per device
-// from double-precision values), so they are read as constant-bank operands.
+// constants.  Lengths with coprime factors (20 = 4 * 5, 40 = 8 * 5, 10 = 2 * 5)
+// use the prime-factor split, which needs no twiddles; the other twiddles
+// live in __constant__ memory (filled once per device from double-precision
+// values), so they are read as constant-bank operands.
 //
 //   space_fwd_fast  all space axes of a batch of (t, f) planes: load the
 //                   planes into shared memory, inverse FFT along every axis
 //                   (cropping P -> L), store the [L..] planes;
 //   space_adj_fast  the adjoint: zero-pad L -> P, forward FFT along every
 //                   axis, then x <- soft_threshold(x - step * g, lambda);
+//   space_adj_pipe  the adjoint with the next batch's input copied into a
+//                   dense staging buffer behind the passes, and the update
+//                   keeping several model loads in flight;
 //   time_fwd_fast   per block of traces, every time window: Hermitian
 //                   combine, half-length inverse FFT (four-step in shared
 //                   memory), taper, overlap-add with a one-hop carry;
