@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "agdeblend.h"
+#include "blend_tables.cuh"
 #include "kernels.cuh"
 #include "plan.hpp"
 
@@ -111,70 +112,21 @@ extern "C" int agd_blend(int n_patches, int const *n_traces, int const *n_times,
     std::fprintf(stderr, "ERROR in agd_blend\n");
     return 1;
   }
-  agd::Plan plan;
-  agd::build_blend_config(n_patches, n_traces, n_times, shottimes, channels, trace_types, plan);
-  const long R = plan.record_size;
-  // any other mode value takes the mean, as the reference's else branch does
-  const int mode = blend_mode == AGDBlendSum         ? agd::kGatherSum
-             : blend_mode == AGDBlendOverwrite ? agd::kGatherOverwrite
-                                               : agd::kGatherMean;
-
-  // contributions of the input traces, patch then trace order
-  std::vector<long> in_off(n_patches);
-  long in_size = 0;
-  std::vector<agd::Contrib> list;
-  for (int p = 0; p < n_patches; ++p) {
-    in_off[p] = in_size;
-    for (int t = 0; t < n_traces[p]; ++t) {
-      const agd::BlendCoord b =
-          plan.coord_of(shottimes[p][t], n_times[p], channels[p][t], (int)trace_types[p][t]);
-      if (b.rec >= 0 && b.n > 0)
-        list.push_back(agd::Contrib{b.rec, in_size + (long)t * n_times[p] + b.trace_start, b.n, 0});
-    }
-    in_size += (long)n_traces[p] * n_times[p];
-  }
-  const int chunk = 512;
-  const long n_chunk = (R + chunk - 1) / chunk;
-  std::vector<long> ptr(n_chunk + 1, 0);
-  for (const auto &c : list)
-    for (long k = c.rec / chunk; k <= (c.rec + c.n - 1) / chunk; ++k) ptr[k + 1]++;
-  for (long k = 0; k < n_chunk; ++k) ptr[k + 1] += ptr[k];
-  std::vector<agd::Contrib> flat(ptr[n_chunk]);
-  {
-    std::vector<long> fill(ptr.begin(), ptr.end() - 1);
-    for (const auto &c : list)
-      for (long k = c.rec / chunk; k <= (c.rec + c.n - 1) / chunk; ++k) flat[fill[k]++] = c;
-  }
-  std::vector<uint8_t> mute(R, 0);
-  for (const auto &m : plan.mute)
-    for (int k = 0; k < m.second; ++k) mute[m.first + k] = 1;
-  // mean-mode edge weights, expression as src/blend.c:1174-1178
-  std::vector<real> taper;
-  if (mode == agd::kGatherMean && taper_length > 1) {
-    taper.resize(taper_length);
-    for (int i = 0; i < taper_length; ++i)
-      taper[i] = (real)std::cos((real)0.5 * (real)3.14159265358979323846 *
-                                (real)(taper_length - i) / (real)(taper_length + 1));
-  }
-  // output traces
-  std::vector<long> o_rec, o_dst;
-  std::vector<int> o_ts, o_n, o_nt;
-  std::vector<long> out_off(n_patches_out);
-  long out_size = 0;
-  for (int p = 0; p < n_patches_out; ++p) {
-    out_off[p] = out_size;
-    for (int t = 0; t < n_traces_out[p]; ++t) {
-      const agd::BlendCoord b = plan.coord_of(shottimes_out[p][t], n_times_out[p],
-                                              channels_out[p][t], (int)trace_types_out[p][t]);
-      o_rec.push_back(b.rec);
-      o_ts.push_back(b.trace_start);
-      o_n.push_back(b.n);
-      o_dst.push_back(out_size + (long)t * n_times_out[p]);
-      o_nt.push_back(n_times_out[p]);
-    }
-    out_size += (long)n_traces_out[p] * n_times_out[p];
-  }
-  const long n_out_tr = (long)o_rec.size();
+  agd::BlendTables bt;
+  agd::build_blend_tables(n_patches, n_traces, n_times, shottimes, channels, trace_types,
+                          blend_mode, taper_length, n_patches_out, n_traces_out, n_times_out,
+                          shottimes_out, channels_out, trace_types_out, bt);
+  const long R = bt.record_size;
+  const long n_chunk = bt.n_chunk();
+  const long n_out_tr = bt.n_out();
+  const long in_size = bt.in_size, out_size = bt.out_size;
+  const std::vector<long> &in_off = bt.in_off, &out_off = bt.out_off;
+  const std::vector<long> &ptr = bt.ptr;
+  const std::vector<agd::Contrib> &flat = bt.flat;
+  const std::vector<uint8_t> &mute = bt.mute;
+  const std::vector<real> &taper = bt.taper;
+  const std::vector<long> &o_rec = bt.o_rec, &o_dst = bt.o_dst;
+  const std::vector<int> &o_ts = bt.o_ts, &o_n = bt.o_n, &o_nt = bt.o_nt;
 
   cudaStream_t s = nullptr;
   Dev d_in, d_rec, d_flat, d_ptr, d_mute, d_taper, d_out, d_orec, d_ots, d_on, d_odst, d_ont;
@@ -212,8 +164,9 @@ extern "C" int agd_blend(int n_patches, int const *n_traces, int const *n_times,
   }
   if (n_chunk > 0) {
     agd::blend_gather<real><<<(unsigned)n_chunk, agd::kThreads, 0, s>>>(
-        (const agd::Contrib *)d_flat.p, (const long *)d_ptr.p, chunk, R, (const real *)d_in.p,
-        (real *)d_rec.p, mode, (const uint8_t *)d_mute.p, nullptr, (const real *)d_taper.p,
+        (const agd::Contrib *)d_flat.p, (const long *)d_ptr.p, agd::BlendTables::kChunk, R,
+        (const real *)d_in.p, (real *)d_rec.p, bt.mode, (const uint8_t *)d_mute.p, nullptr,
+        (const real *)d_taper.p,
         (int)taper.size(), nullptr);
     BCK(cudaGetLastError());
   }

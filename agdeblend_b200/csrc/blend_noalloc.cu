@@ -14,17 +14,21 @@
 // The array's name in host code is only a host-side handle, not a device
 // address, so the device address is looked up with cudaGetSymbolAddress the
 // first time the entry point runs on a device (with that device current) and
-// cached per device.  That first call therefore does set-up work and should
-// happen before any stream capture begins.
+// cached per device for the life of the process.  That first call therefore
+// does set-up work and should happen before any stream capture begins.  The
+// cached address belongs to the device's context at that time: resetting the
+// device (cudaDeviceReset, or destroying and re-creating its primary context)
+// between calls is not supported.
 //
 // All calls on one device share that device's array, and the array keeps
 // whatever the previous call left in it.  Nothing here relies on it starting
 // at zero: every record sample is written by the blend kernel before it is
 // read, and every table is copied in before the kernels run.  Calls whose GPU
 // work overlaps on the same device - two host threads calling at once, say -
-// race on the array and corrupt each other's results.  Each call returns only
-// after its own work on `stream` has finished, so consecutive calls from one
-// host thread never overlap.
+// race on the array and corrupt each other's results.  Every call copies its
+// tables from temporary host memory and then waits on `stream` until its own
+// work has finished (the calling thread blocks), so consecutive calls from
+// one host thread never overlap.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -33,6 +37,7 @@
 #include <vector>
 
 #include "agdeblend_gpu.h"
+#include "blend_tables.cuh"
 #include "kernels.cuh"
 #include "plan.hpp"
 
@@ -115,62 +120,17 @@ extern "C" int agd_blend_device_noalloc(
   }
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
 
-  // host tables: the same blend configuration agd_blend builds
-  agd::Plan plan;
-  agd::build_blend_config(n_patches, n_traces, n_times, shottimes, channels, trace_types, plan);
-  const long R = plan.record_size;
-  std::vector<agd::Contrib> list;
-  long in_off = 0;
-  for (int p = 0; p < n_patches; ++p) {
-    for (int t = 0; t < n_traces[p]; ++t) {
-      const agd::BlendCoord b =
-          plan.coord_of(shottimes[p][t], n_times[p], channels[p][t], (int)trace_types[p][t]);
-      if (b.rec >= 0 && b.n > 0)
-        list.push_back(agd::Contrib{b.rec, in_off + (long)t * n_times[p] + b.trace_start, b.n, 0});
-    }
-    in_off += (long)n_traces[p] * n_times[p];
-  }
-  const int chunk = 512;
-  const long n_chunk = (R + chunk - 1) / chunk;
-  std::vector<long> ptr(n_chunk + 1, 0);
-  for (const auto &c : list)
-    for (long k = c.rec / chunk; k <= (c.rec + c.n - 1) / chunk; ++k) ptr[k + 1]++;
-  for (long k = 0; k < n_chunk; ++k) ptr[k + 1] += ptr[k];
-  std::vector<agd::Contrib> flat(ptr[n_chunk]);
-  {
-    std::vector<long> fill(ptr.begin(), ptr.end() - 1);
-    for (const auto &c : list)
-      for (long k = c.rec / chunk; k <= (c.rec + c.n - 1) / chunk; ++k) flat[fill[k]++] = c;
-  }
-  std::vector<uint8_t> mute(R, 0);
-  for (const auto &m : plan.mute)
-    for (int k = 0; k < m.second; ++k) mute[m.first + k] = 1;
-  const int mode = blend_mode == AGDBlendSum         ? agd::kGatherSum
-                   : blend_mode == AGDBlendOverwrite ? agd::kGatherOverwrite
-                                                     : agd::kGatherMean;
-  std::vector<real> taper;
-  if (mode == agd::kGatherMean && taper_length > 1) {
-    taper.resize(taper_length);
-    for (int i = 0; i < taper_length; ++i)
-      taper[i] = (real)std::cos((real)0.5 * (real)3.14159265358979323846 *
-                                (real)(taper_length - i) / (real)(taper_length + 1));
-  }
-  std::vector<long> o_rec, o_dst;
-  std::vector<int> o_ts, o_n, o_nt;
-  long out_off = 0;
-  for (int p = 0; p < n_patches_out; ++p) {
-    for (int t = 0; t < n_traces_out[p]; ++t) {
-      const agd::BlendCoord b = plan.coord_of(shottimes_out[p][t], n_times_out[p],
-                                              channels_out[p][t], (int)trace_types_out[p][t]);
-      o_rec.push_back(b.rec);
-      o_ts.push_back(b.trace_start);
-      o_n.push_back(b.n);
-      o_dst.push_back(out_off + (long)t * n_times_out[p]);
-      o_nt.push_back(n_times_out[p]);
-    }
-    out_off += (long)n_traces_out[p] * n_times_out[p];
-  }
-  const long n_out = (long)o_rec.size();
+  // host tables: the same ones agd_blend builds
+  agd::BlendTables bt;
+  agd::build_blend_tables(n_patches, n_traces, n_times, shottimes, channels, trace_types,
+                          blend_mode, taper_length, n_patches_out, n_traces_out, n_times_out,
+                          shottimes_out, channels_out, trace_types_out, bt);
+  const long R = bt.record_size;
+  const long n_chunk = bt.n_chunk();
+  const long n_out = bt.n_out();
+  const std::vector<long> &ptr = bt.ptr;
+  const std::vector<agd::Contrib> &flat = bt.flat;
+  const std::vector<real> &taper = bt.taper;
 
   // carve the fixed scratch array
   size_t off = 0;
@@ -211,18 +171,19 @@ extern "C" int agd_blend_device_noalloc(
   cudaError_t e = cudaSuccess;
   if (e == cudaSuccess) e = put(at_ptr, ptr.data(), ptr.size() * sizeof(long));
   if (e == cudaSuccess) e = put(at_flat, flat.data(), flat.size() * sizeof(agd::Contrib));
-  if (e == cudaSuccess) e = put(at_mute, mute.data(), (size_t)R);
+  if (e == cudaSuccess) e = put(at_mute, bt.mute.data(), (size_t)R);
   if (e == cudaSuccess) e = put(at_taper, taper.data(), taper.size() * sizeof(real));
-  if (e == cudaSuccess) e = put(at_orec, o_rec.data(), (size_t)n_out * sizeof(long));
-  if (e == cudaSuccess) e = put(at_odst, o_dst.data(), (size_t)n_out * sizeof(long));
-  if (e == cudaSuccess) e = put(at_ots, o_ts.data(), (size_t)n_out * sizeof(int));
-  if (e == cudaSuccess) e = put(at_on, o_n.data(), (size_t)n_out * sizeof(int));
-  if (e == cudaSuccess) e = put(at_ont, o_nt.data(), (size_t)n_out * sizeof(int));
+  if (e == cudaSuccess) e = put(at_orec, bt.o_rec.data(), (size_t)n_out * sizeof(long));
+  if (e == cudaSuccess) e = put(at_odst, bt.o_dst.data(), (size_t)n_out * sizeof(long));
+  if (e == cudaSuccess) e = put(at_ots, bt.o_ts.data(), (size_t)n_out * sizeof(int));
+  if (e == cudaSuccess) e = put(at_on, bt.o_n.data(), (size_t)n_out * sizeof(int));
+  if (e == cudaSuccess) e = put(at_ont, bt.o_nt.data(), (size_t)n_out * sizeof(int));
   real *record = reinterpret_cast<real *>(base + at_record);
   if (e == cudaSuccess && n_chunk > 0) {
     agd::blend_gather<real><<<(unsigned)n_chunk, agd::kThreads, 0, stream>>>(
         reinterpret_cast<const agd::Contrib *>(base + at_flat),
-        reinterpret_cast<const long *>(base + at_ptr), chunk, R, data_dev, record, mode,
+        reinterpret_cast<const long *>(base + at_ptr), agd::BlendTables::kChunk, R, data_dev,
+        record, bt.mode,
         reinterpret_cast<const uint8_t *>(base + at_mute), nullptr,
         reinterpret_cast<const real *>(base + at_taper), (int)taper.size(), nullptr);
     e = cudaGetLastError();

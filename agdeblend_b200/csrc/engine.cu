@@ -2101,13 +2101,23 @@ class Engine {
     return v;
   }
 
-  double record_norm(const R *rec) {
+  // FP64 L2 norm of n values on the device
+  double device_norm(const R *x, long n) {
     CK(cudaMemsetAsync(dscalar.get(), 0, sizeof(double), stream));
-    if (plan.record_size)
-      record_sumsq<R><<<grid_for(plan.record_size), kThreads, 0, stream>>>(
-          rec, plan.record_size, dscalar.get());
+    if (n) record_sumsq<R><<<grid_for(n), kThreads, 0, stream>>>(x, n, dscalar.get());
     CK(cudaGetLastError());
     return std::sqrt(read_dscalar());
+  }
+
+  double record_norm(const R *rec) { return device_norm(rec, plan.record_size); }
+
+  // Guard on the FP64 residual norm (no counterpart in the reference, whose
+  // get_residual_norm, src/model.c:1343-1384, returns whatever it sums): a
+  // NaN or Inf norm ends the call with an error instead of a NaN output.
+  static void require_finite(double norm, const char *what) {
+    if (!std::isfinite(norm))
+      throw std::runtime_error(std::string(what) +
+                               " is not finite (NaN or Inf values in the data)");
   }
 
   static unsigned grid_for(long n) {
@@ -2290,6 +2300,9 @@ class Engine {
   // that model's output.
   void solve_range(R initial_factor, int n_its, int begin, int end, int print_freq,
                    const R *model_in, R *model_out) {
+    // the blended input's norm is the residual of the zero model
+    const double r0 = record_norm(rec_d.get());
+    require_finite(r0, "the norm of the blended input data");
     start_schedule(initial_factor, n_its, std::max(1, n_its - 1));
     int first = 1;
     if (begin > 0) {
@@ -2301,15 +2314,15 @@ class Engine {
       first = begin;
     }
     if (print_freq > 0) {
-      if (begin == 0) {
-        const double r = record_norm(rec_d.get());
-        std::printf("Iteration 0 Residual %f\n", r);
-      }
+      if (begin == 0) std::printf("Iteration 0 Residual %f\n", r0);
       for (int it = first; it < end; ++it) {
         const bool print_residual = it % print_freq == 0;
         iteration_body(print_residual);
-        if (print_residual)
-          std::printf("Iteration %d Residual %f\n", it, std::sqrt(read_dscalar()));
+        if (print_residual) {
+          const double r = std::sqrt(read_dscalar());
+          require_finite(r, "the residual norm");
+          std::printf("Iteration %d Residual %f\n", it, r);
+        }
       }
     } else if (end > first) {
       capture_iteration();
@@ -2317,6 +2330,7 @@ class Engine {
     }
     if (model_out != nullptr) model_to_ref(X.get(), model_out);
     output();
+    require_finite(device_norm(data_dev.get(), data_size), "the norm of the deblended output");
   }
 
   // host <-> device model in the reference layout

@@ -192,6 +192,28 @@ def profiled_traffic(kernel: str, name: str):
     return float(m.group(1)) if m else None
 
 
+def physical_cores() -> int:
+    """Physical cores of this host (logical CPUs when the split is unknown)."""
+    try:
+        import psutil
+
+        n = psutil.cpu_count(logical=False)
+        if n:
+            return int(n)
+    except Exception:
+        pass
+    return os.cpu_count() or 1
+
+
+# The reference's OpenMP path runs with one thread per physical core; the
+# variable must be set before the OpenMP runtime starts (the first load of the
+# reference library).
+os.environ.setdefault("OMP_NUM_THREADS", str(physical_cores()))
+
+FFT_BACKEND = ("the project's FFTW3-API stand-in (oracle/fftw_shim): this image has no "
+               "system FFTW3 library")
+
+
 def cpu_reference_rate(sv, its: int, lib_name="libagdeblend_ref.so"):
     """Iterations/s of the reference's CPU path: time agd_deblend with
     n_its = 1 and 1 + its; the difference is `its` loop iterations."""
@@ -213,10 +235,14 @@ def cpu_reference_rate(sv, its: int, lib_name="libagdeblend_ref.so"):
         if rc:
             raise RuntimeError("reference agd_deblend failed")
     dt = max(times[1] - times[0], 1e-9)
-    return {"value": its / dt, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+    serial = lib_name.endswith("_serial.so")
+    threads = 1 if serial else int(os.environ["OMP_NUM_THREADS"])
+    return {"value": its / dt, "unit": UNIT, "cores": threads, "kind": "reference",
             "sample": f"agd_deblend n_its=1 vs 1+{its} on the full workload (difference = "
-                      f"{its} iterations, {dt:.1f} s), OpenMP over windows, "
-                      f"OMP_NUM_THREADS={os.environ.get('OMP_NUM_THREADS', 'all')}"}
+                      f"{its} iterations, {dt:.1f} s), "
+                      + ("serial build" if serial else
+                         f"OpenMP over windows, OMP_NUM_THREADS={threads} (physical cores)"),
+            "fft": FFT_BACKEND}
 
 
 def cpu_port_rate(sv, its: int):
@@ -304,12 +330,13 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def run_gpu(args, rank, world, local):
+def measure_single(args, name, rank, world, local, cpu_its):
+    """One workload of one survey: the bench line of rank 0 (None elsewhere)."""
     import torch
 
     import agdeblend_b200 as A
 
-    sv = workload(args.workload, seed_offset=rank)
+    sv = workload(name, seed_offset=rank)
     torch.cuda.set_device(local)
     prob = A.Problem.from_survey(sv)
     # warm-up + timed region (CUDA events inside the library, on its stream)
@@ -359,7 +386,7 @@ def run_gpu(args, rank, world, local):
     M = int(info[1])
     Rn = int(info[2])
     peak, peak_kind = hbm_peak()
-    # Algorithmic bytes per launch (DESIGN.md section 5): the share of
+    # Algorithmic bytes per launch: the share of
     # B_iter = 3 M 8 + 4 R 4 each kernel is responsible for - the forward
     # space kernel reads the model once, the adjoint space kernel reads and
     # writes it once, the blend gather writes A x and reads d, the adjoint
@@ -392,7 +419,7 @@ def run_gpu(args, rank, world, local):
     iter_bytes = 3 * 8.0 * M + 4 * 4.0 * Rn
     ms_iter = ms / args.steps
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 and dom_bytes > 0 else 0.0
-    traffic = profiled_traffic(dom, args.workload)
+    traffic = profiled_traffic(dom, name)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "algorithmic_bytes": dom_bytes, "peak_source": peak_kind,
@@ -402,16 +429,21 @@ def run_gpu(args, rank, world, local):
                 "iteration_frac": iter_bytes / (ms_iter / 1e3) / 1e9 / peak}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_reference_rate(sv, args.cpu_its) or cpu_port_rate(sv, 1)
+        cpu = cpu_reference_rate(sv, cpu_its) or cpu_port_rate(sv, 1)
+        if cpu is not None and cpu["kind"] == "reference" and name == "two_volume_3d":
+            serial = cpu_reference_rate(sv, 1, "libagdeblend_ref_serial.so")
+            if serial is not None:
+                cpu["serial"] = {k: serial[k] for k in ("value", "unit", "cores", "sample")}
+    line = None
     if rank == 0:
         # kernels per iteration as the library counts them (space and time
         # kernels both ways per window class, generic passes, the blend
         # gather, the threshold-schedule step, wavelet kernels)
         launches = args.steps * int(info[14])
-        line = {"metric": metric_of(args.workload), "value": value, "unit": UNIT, "n_gpus": world,
+        line = {"metric": metric_of(name), "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_iter,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32", "data": "synthetic", "config": config_of(sv, args.workload),
+                "dtype": "f32", "data": "synthetic", "config": config_of(sv, name),
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                 "clocks": clk,
                 "e2e": {"value": e2e_value, "unit": UNIT,
@@ -420,8 +452,8 @@ def run_gpu(args, rank, world, local):
                         "call_s": e2e_s, "n_its": sv.n_its, "snr_db": snr},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
                 "ms_forward_half": ms_fwd, "ms_adjoint_half": ms_adj}
-        print(json.dumps(line), flush=True)
     prob.close()
+    return line
 
 
 def batch_workload(name, seed_offset=0):
@@ -460,17 +492,21 @@ def cpu_batch_rate(gathers, its: int):
                 raise RuntimeError("reference agd_deblend failed")
             times.append(time.perf_counter() - t0)
         total += max(times[1] - times[0], 1e-9)
-    return {"value": its / total, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+    threads = int(os.environ["OMP_NUM_THREADS"])
+    return {"value": its / total, "unit": UNIT, "cores": threads, "kind": "reference",
             "sample": f"agd_deblend n_its=1 vs 1+{its} on each of the {len(gathers)} gathers "
-                      f"(sum of differences {total:.1f} s), OpenMP over windows"}
+                      f"(sum of differences {total:.1f} s), OpenMP over windows, "
+                      f"OMP_NUM_THREADS={threads} (physical cores)",
+            "fft": FFT_BACKEND}
 
 
-def run_gpu_batch(args, rank, world, local):
+def measure_batch(args, name, rank, world, local):
+    """The batch workload: the bench line of rank 0 (None elsewhere)."""
     import torch
 
     import agdeblend_b200 as A
 
-    gathers = batch_workload(args.workload, seed_offset=rank)
+    gathers = batch_workload(name, seed_offset=rank)
     torch.cuda.set_device(local)
     n_its = gathers[0].n_its
     data = [d for g in gathers for d in g.data]
@@ -529,13 +565,14 @@ def run_gpu_batch(args, rank, world, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_batch_rate(gathers, 1)
+    line = None
     if rank == 0:
         data_bytes = sum(d.nbytes for d in data)
-        line = {"metric": metric_of(args.workload), "value": value, "unit": UNIT,
+        line = {"metric": metric_of(name), "value": value, "unit": UNIT,
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms_iter, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": batch_config(gathers, args.workload),
+                "config": batch_config(gathers, name),
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                 "clocks": clk,
                 "per_gather_loop": {"value": world * args.steps / (loop_ms / 1e3), "unit": UNIT,
@@ -547,8 +584,16 @@ def run_gpu_batch(args, rank, world, local):
                 "gpu_launches": args.steps * int(info[14]), "roofline": roofline,
                 "cpu_baseline": cpu, "window_classes_fast": int(info[15]),
                 "windows_fast": int(info[16]), "windows": int(info[0])}
-        print(json.dumps(line), flush=True)
     prob.close()
+    return line
+
+
+SUMMARY_KEYS = ("metric", "value", "unit", "ms_per_step", "config", "clocks", "e2e",
+                "gpu_launches", "roofline", "cpu_baseline", "per_gather_loop")
+
+
+def workload_summary(line):
+    return {k: line[k] for k in SUMMARY_KEYS if k in line}
 
 
 def main():
@@ -560,6 +605,8 @@ def main():
     ap.add_argument("--cpu-its", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="only the headline workload (no vibroseis_4d / uneven_gathers entries)")
     ap.add_argument("--workload", default="two_volume_3d",
                     choices=sorted(WORKLOADS) + sorted(BATCHES))
     args = ap.parse_args()
@@ -571,9 +618,21 @@ def main():
     rank, world, local = dist_setup(args.gpus)
     try:
         if args.workload in BATCHES:
-            run_gpu_batch(args, rank, world, local)
+            line = measure_batch(args, args.workload, rank, world, local)
         else:
-            run_gpu(args, rank, world, local)
+            line = measure_single(args, args.workload, rank, world, local, args.cpu_its)
+        if (world == 1 and args.workload == "two_volume_3d" and not args.no_workloads
+                and line is not None):
+            # the other benchmark workloads, each measured the same way, in
+            # the same JSON line
+            line["workloads"] = {
+                "vibroseis_4d": workload_summary(
+                    measure_single(args, "vibroseis_4d", rank, world, local, 1)),
+                "uneven_gathers": workload_summary(
+                    measure_batch(args, "uneven_gathers", rank, world, local)),
+            }
+        if line is not None:
+            print(json.dumps(line), flush=True)
     finally:
         if world > 1:
             import torch.distributed as dist

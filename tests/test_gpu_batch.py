@@ -14,6 +14,7 @@ import agd_oracle as O
 import agdeblend_b200 as A
 from agdeblend_b200 import synthetic as S
 from conftest import rel_l2
+from golden_io import GOLDEN, sketch
 from problems import random_problem
 
 pytestmark = pytest.mark.gpu
@@ -175,3 +176,30 @@ def test_every_space_candidate_at_odd_model_offsets():
             os.environ.pop("AGD_GPU_SPACE_VARIANT", None)
         else:
             os.environ["AGD_GPU_SPACE_VARIANT"] = old
+
+
+def test_uneven_gathers_batch_matches_reference_per_gather():
+    """The benchmark's 96 uneven gathers (shots U{100..400}, time
+    U{512..2048}, three window shapes), solved together by
+    agd_deblend_batch, against the reference float build run separately on
+    each gather (tests/golden/make_batch_fixture.py): per gather, SNR
+    within 0.05 dB and a 32-projection sketch of the output within 1e-3
+    relative difference (an estimate of the relative L2 difference)."""
+    ref = np.load(os.path.join(GOLDEN, "uneven_gathers_reference.npz"))
+    gathers = S.uneven_gathers(len(ref["snr_db"]), base_seed=int(ref["base_seed"]))
+    n_its = int(ref["n_its"])
+    for g, c in zip(gathers, ref["input_checksum"]):
+        assert g.n_its == n_its
+        assert sum(float(np.sum(d.astype(np.float64))) for d in g.data) == \
+            pytest.approx(float(c), rel=1e-12)
+    outs = A.deblend_batch([_kw(g) for g in gathers], 1.0, n_its)
+    k = ref["sketch"].shape[1]
+    for i, (g, out) in enumerate(zip(gathers, outs)):
+        assert all(np.isfinite(o).all() for o in out), i
+        snr = S.snr_db(out, g.truth, g.trace_types)
+        assert abs(snr - float(ref["snr_db"][i])) <= 0.05, (i, snr, float(ref["snr_db"][i]))
+        sk = sketch(out, k=k)
+        rs = ref["sketch"][i]
+        assert np.linalg.norm(sk - rs) <= 1e-3 * np.linalg.norm(rs), i
+        norm = np.sqrt(sum(float(np.sum(np.asarray(o, np.float64) ** 2)) for o in out))
+        assert norm == pytest.approx(float(ref["norm"][i]), rel=1e-3), i

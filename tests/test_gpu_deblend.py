@@ -16,6 +16,8 @@ import agdeblend_b200 as A
 from agdeblend_b200 import synthetic as S
 from conftest import ROOT, rel_l2
 from problems import random_problem
+from residual_cases import CASES as RESIDUAL_CASES
+from residual_cases import make_case as residual_case
 
 pytestmark = pytest.mark.gpu
 
@@ -148,3 +150,33 @@ def test_print_freq_lines(capfd):
     out = capfd.readouterr().out
     lines = [ln for ln in out.splitlines() if ln.startswith("Iteration")]
     assert [ln.split()[1] for ln in lines] == ["0", "2", "4"]
+
+
+def _residual_lines(text):
+    its, vals = [], []
+    for ln in text.splitlines():
+        parts = ln.split()
+        if len(parts) == 4 and parts[0] == "Iteration" and parts[2] == "Residual":
+            its.append(int(parts[1]))
+            vals.append(float(parts[3]))
+    return np.array(its), np.array(vals)
+
+
+@pytest.mark.parametrize("name", RESIDUAL_CASES)
+def test_print_freq_residuals_match_reference(name, capfd):
+    """The residual norms printed with print_freq > 0 (FP64 on the device)
+    against the lines the reference float build printed on the same survey
+    (tests/golden/make_residual_fixture.py): same iterations, values within
+    1e-3 relative."""
+    ref = np.load(os.path.join(GOLDEN, "residual_lines_reference.npz"))
+    sv, print_freq = residual_case(name)
+    kw = {}
+    if sv.wavelets is not None:
+        kw = dict(wavelet_idxs=sv.wavelet_idxs, wavelets=sv.wavelets)
+    capfd.readouterr()
+    A.deblend(sv.volumes, sv.window_shapes, sv.coords, sv.shottimes, sv.channels,
+              sv.trace_types, sv.initial_factor, sv.n_its, print_freq, sv.data, **kw)
+    its, vals = _residual_lines(capfd.readouterr().out)
+    assert np.array_equal(its, ref[f"{name}_its"])
+    want = ref[f"{name}_residual"]
+    assert np.all(np.abs(vals - want) <= 1e-3 * np.abs(want) + 1e-6)

@@ -119,3 +119,26 @@ def test_every_allocation_failure_returns_1_and_releases_memory(capfd):
     # the library still works, with the same result
     for a, b in zip(deblend(), ref):
         assert rel_l2(a, b) <= 1e-6
+
+
+@pytest.mark.parametrize("print_freq", [0, 2])
+def test_non_finite_input_returns_error(print_freq, capfd):
+    """A NaN in the host input makes the FP64 residual norm non-finite: the
+    call returns 1 (RuntimeError here) with an error message instead of
+    writing NaN output, and the library stays usable.  The NaN reaches the
+    device only as data; no kernel faults."""
+    sv = S.gather_2d(seed=3300, n_shots=48, nt=256, window=(16, 128), n_its=6)
+    bad = [d.copy() for d in sv.data]
+    bad[0][7, 100] = np.nan
+    with pytest.raises(RuntimeError):
+        A.deblend(sv.volumes, sv.window_shapes, sv.coords, sv.shottimes, sv.channels,
+                  sv.trace_types, 1.0, 6, print_freq, bad)
+    assert "not finite" in capfd.readouterr().err
+    inf = [d.copy() for d in sv.data]
+    inf[0][3, 50] = np.inf
+    prob = A.Problem.from_survey(sv)
+    with pytest.raises(RuntimeError):
+        prob.solve(inf, 1.0, 6)
+    out = prob.solve(sv.data, 1.0, 6)
+    prob.close()
+    assert all(np.isfinite(o).all() for o in out)
