@@ -16,8 +16,10 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
-SOURCES = ["plan.cpp", "engine.cu", "blend.cu", "blend_noalloc.cu"]
-HEADERS = ["plan.hpp", "fft.cuh", "kernels.cuh", "fast.cuh", "wavelet_fast.cuh"]
+SOURCES = ["plan.cpp", "engine.cu", "blend.cu", "blend_noalloc.cu", "nn.cu"]
+# every header in csrc/ is an input of both libraries (a stale library must
+# not travel to the device after a header-only change)
+HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp", ".h")))
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 LIBS = {

@@ -184,9 +184,11 @@ void agd_gpu_release_cache(void);
  * stream) orders the work.  It allocates nothing: every intermediate lives
  * in a fixed 16 MiB device array built into the library; larger problems are
  * rejected with an error (use agd_blend).  The first call on a device looks
- * up that array's device address, so make it before any stream capture.
- * Calls overlapping on one device race on the shared array; each call
- * returns after its work has finished. */
+ * up that array's device address and keeps it for the life of the process,
+ * so make it before any stream capture, and do not reset the device between
+ * calls.  Calls overlapping on one device race on the shared array.  Each
+ * call copies its tables from temporary host memory and waits on `stream`
+ * until its own work has finished before it returns (it blocks). */
 int agd_blend_device_noalloc(int n_patches, int const *n_traces, int const *n_times,
                              long int const *const *shottimes, int const *const *channels,
                              enum AGDTraceType const *const *trace_types,
@@ -196,6 +198,18 @@ int agd_blend_device_noalloc(int n_patches, int const *n_traces, int const *n_ti
                              int const *const *channels_out,
                              enum AGDTraceType const *const *trace_types_out,
                              AGD_TYPE *data_out_dev, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Learned warm start (no counterpart in the reference, whose solver starts
+ * every solve from a zero model, src/model.c:1160-1185).
+ * ------------------------------------------------------------------------- */
+
+/* C = alpha A B^T + beta C on the tcgen05 tensor cores: A (M x K) and B
+ * (N x K) row-major BF16 device arrays (16-byte aligned, K, lda, ldb
+ * multiples of 8), C row-major FP32, FP32 accumulation.  `stream` is a
+ * cudaStream_t (NULL: default stream); returns after the product is done. */
+int agd_nn_gemm_bf16(const void *A, const void *B, float *C, int M, int N, int K, int lda,
+                     int ldb, int ldc, float alpha, float beta, void *stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,46 @@
+"""The tcgen05 BF16 GEMM (agd_nn_gemm_bf16) against an FP32 product of the
+same BF16 operands (torch on the GPU): relative L2 error within 1e-5 (the
+tensor cores accumulate in FP32, in another order), on shapes with partial
+tiles in M, N and K, with alpha and beta, through the C-ABI."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import agdeblend_b200 as A
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _gemm():
+    lib = A.load_library(np.float32)
+    fn = lib.agd_nn_gemm_bf16
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 6 + \
+        [ctypes.c_float, ctypes.c_float, ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    return fn
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 64, 64), (200, 100, 72), (1000, 256, 520),
+                                   (37, 16, 8), (513, 129, 1024)])
+def test_tc_gemm_matches_fp32_product(M, N, K):
+    torch = pytest.importorskip("torch")
+    g = torch.Generator(device="cuda").manual_seed(M * 7 + N * 3 + K)
+    a = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    b = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    c0 = torch.randn(M, N, device="cuda", generator=g)
+    want = 0.5 * (a.float() @ b.float().T) + 2.0 * c0
+    c = c0.clone()
+    torch.cuda.synchronize()
+    rc = _gemm()(a.data_ptr(), b.data_ptr(), c.data_ptr(), M, N, K, K, K, N, 0.5, 2.0, None)
+    assert rc == 0
+    assert rel_l2(c.cpu().numpy(), want.cpu().numpy()) <= 1e-5
+
+
+def test_tc_gemm_rejects_misaligned_k():
+    torch = pytest.importorskip("torch")
+    a = torch.zeros(16, 12, device="cuda", dtype=torch.bfloat16)
+    c = torch.zeros(16, 16, device="cuda")
+    assert _gemm()(a.data_ptr(), a.data_ptr(), c.data_ptr(), 16, 16, 12, 12, 12, 16, 1.0, 0.0,
+                   None) == 1
