@@ -82,11 +82,13 @@ def _bind_extension(lib, dtype):
         POINTER(POINTER(ip)), POINTER(POINTER(lip)), POINTER(POINTER(ip)), POINTER(POINTER(ip)),
         POINTER(ip), POINTER(POINTER(ip)), POINTER(POINTER(rp)), POINTER(c_void_p)]
     lib.agd_gpu_problem_steps.argtypes = [c_void_p, rp]
+    lib.agd_gpu_problem_set_precision.argtypes = [c_void_p, c_int, POINTER(c_long)]
     for name in ("agd_gpu_problem_info", "agd_gpu_problem_kernels", "agd_gpu_stepsize", "agd_gpu_forward",
                  "agd_gpu_adjoint", "agd_gpu_blend_input", "agd_gpu_set_output",
                  "agd_gpu_solve", "agd_gpu_time_iterations", "agd_plan_export",
                  "agd_gpu_solve_range",
-                 "agd_gpu_batch_create", "agd_gpu_problem_steps"):
+                 "agd_gpu_batch_create", "agd_gpu_problem_steps",
+                 "agd_gpu_problem_set_precision"):
         getattr(lib, name).restype = c_int
 
 
@@ -274,6 +276,19 @@ class Problem:
         self._check(self.lib.agd_gpu_problem_kernels(self.h, buf, len(buf)),
                     "agd_gpu_problem_kernels")
         return dict(kv.split("=", 1) for kv in buf.value.decode().split())
+
+    PRECISION_FP32 = 0
+    PRECISION_SPLIT_BF16 = 1
+
+    def set_precision(self, mode: int) -> int:
+        """Precision of the space DFTs (agd_gpu_problem_set_precision): 0
+        FP32, 1 split-BF16 tensor-core contractions for windows of padded
+        space shape 20 x 20 x 20.  Returns the number of windows the
+        tensor-core kernels serve."""
+        n = c_long(0)
+        self._check(self.lib.agd_gpu_problem_set_precision(self.h, int(mode), ctypes.byref(n)),
+                    "agd_gpu_problem_set_precision")
+        return int(n.value)
 
     def steps(self) -> np.ndarray:
         """Step size of every problem of the handle."""

@@ -16,6 +16,7 @@
 #include <chrono>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "agdeblend_gpu.h"
@@ -24,6 +25,7 @@
 #include "plan.hpp"
 #include "wavelet_fast.cuh"
 #include "line_dft.cuh"
+#include "space_tc.cuh"
 
 namespace agd {
 
@@ -415,7 +417,11 @@ class Engine {
     std::vector<AdjVariant> adj_vars;
     int fwd_pick = 0, adj_pick = 0;
     PlaneLaunch pl_fwd, pl_adj, pl_adj_plain;
+    std::vector<PlaneJob<R>> fwd_jobs;    // forward jobs
     std::vector<PlaneJob<R>> plain_jobs;  // adjoint jobs without the update
+    // split-BF16 tensor-core kernels (precision mode 1, space_tc.cuh)
+    bool tc = false;
+    PlaneLaunch tc_fwd, tc_adj, tc_adj_plain;
     std::vector<long> planes;             // (t, f) planes per window
     const FwdVariant &fv() const { return fwd_vars[fwd_pick]; }
     const AdjVariant &av() const { return adj_vars[adj_pick]; }
@@ -1342,8 +1348,9 @@ class Engine {
   template <typename K>
   void make_plane_launch(PlaneLaunch &L, const std::vector<PlaneJob<R>> &jobs,
                          const std::vector<long> &planes, int nt, int np, size_t smem,
-                         K kernel) {
-    if (smem > (size_t)smem_max) throw DeviceError("space planes too large");
+                         K kernel, size_t smem_limit = 0) {
+    if (smem > (smem_limit ? smem_limit : (size_t)smem_max))
+      throw DeviceError("space planes too large");
     std::vector<PlaneBatch<R>> bt;
     for (size_t i = 0; i < jobs.size(); ++i)
       for (long q = 0; q < planes[i]; q += np) {
@@ -1406,7 +1413,149 @@ class Engine {
     autotune_space(c, jf, ja);
     make_plane_launch(c.pl_fwd, jf, c.planes, c.fv().nt, c.fv().np, c.fv().smem, c.fv().fn);
     make_plane_launch(c.pl_adj, ja, c.planes, c.av().nt, c.av().np, c.av().smem, c.av().fn);
+    c.fwd_jobs = jf;
     c.plain_jobs = ja;
+  }
+
+  // ------------------------------------------------------------ precision modes
+  //
+  // Mode 0 (default): FP32 space kernels.  Mode 1: the space axes of every
+  // window class of padded shape kTcP^3 and window kTcL^3 run as split-BF16
+  // tensor-core contractions (space_tc.cuh); the time axis, the wavelet, the
+  // blend and the update arithmetic stay FP32.  Float library only.
+  static constexpr int kTcP = 20, kTcL = 16;
+  using TcS = TcDft3<kTcP, kTcL>;
+  int precision = 0;
+  DevArray<uint16_t> tc_mat;  // forward hi | forward lo | adjoint hi | adjoint lo
+  DevArray<int> tc_err;       // 1 when a tensor-core wait gave up
+  long tc_windows = 0;
+
+  static bool tc_shape(const WindowPlan &W) {
+    return W.D == 3 && W.P[0] == kTcP && W.P[1] == kTcP && W.P[2] == kTcP && W.L[0] == kTcL &&
+           W.L[1] == kTcL && W.L[2] == kTcL;
+  }
+
+  // BF16 bits of a float, rounded to nearest even (finite values)
+  static uint16_t bf16_bits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+  }
+  static double bf16_value(uint16_t h) {
+    const uint32_t u = (uint32_t)h << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+  }
+  // hi, lo BF16 parts of v (v ~ hi + lo to about 16 significant bits)
+  static void split_host(double v, uint16_t &hi, uint16_t &lo) {
+    hi = bf16_bits((float)v);
+    lo = bf16_bits((float)(v - bf16_value(hi)));
+  }
+
+  // B[n][k] of the forward (n = 2 i + (re, im) for output i < L, k = 2 j +
+  // (re, im) for input j < P; exp(+2 pi i i j / P)) and of the adjoint (n = 2 k
+  // + .. for output k < P, k = 2 j + .. for input j < L; exp(-2 pi i j k / P)),
+  // as real matrices acting on interleaved (re, im) values, zero-padded to
+  // the kernels' N x K; computed in double precision, then split.
+  void upload_tc_matrices() {
+    const int nf = TcS::kFwdN * TcS::kFwdK, na = TcS::kAdjN * TcS::kAdjK;
+    std::vector<uint16_t> h(2 * nf + 2 * na, 0);
+    const double two_pi = 6.283185307179586476925286766559;
+    auto put = [&](int base, int n_off, int K, int row_i, int col_j, double c, double sgn_s) {
+      // complex entry w = c + i s at (output row_i, input col_j), s = sgn_s
+      const double vals[2][2] = {{c, -sgn_s}, {sgn_s, c}};
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+          uint16_t hi, lo;
+          split_host(vals[a][b], hi, lo);
+          const int idx = (2 * row_i + a) * K + 2 * col_j + b;
+          h[base + idx] = hi;
+          h[base + n_off + idx] = lo;
+        }
+    };
+    for (int i = 0; i < kTcL; ++i)
+      for (int j = 0; j < kTcP; ++j) {
+        const double th = two_pi * (double)((i * j) % kTcP) / kTcP;
+        put(0, nf, TcS::kFwdK, i, j, std::cos(th), std::sin(th));
+      }
+    for (int k = 0; k < kTcP; ++k)
+      for (int j = 0; j < kTcL; ++j) {
+        const double th = two_pi * (double)((j * k) % kTcP) / kTcP;
+        put(2 * nf, na, TcS::kAdjK, k, j, std::cos(th), -std::sin(th));
+      }
+    tc_mat.alloc(h.size());
+    CK(cudaMemcpyAsync(tc_mat.get(), h.data(), h.size() * sizeof(uint16_t),
+                       cudaMemcpyHostToDevice, stream));
+    tc_err.alloc(1);
+    CK(cudaMemsetAsync(tc_err.get(), 0, sizeof(int), stream));
+  }
+
+  TcMatrices tc_fwd_mats() const {
+    const int nf = TcS::kFwdN * TcS::kFwdK;
+    return TcMatrices{tc_mat.get(), tc_mat.get() + nf};
+  }
+  TcMatrices tc_adj_mats() const {
+    const int nf = TcS::kFwdN * TcS::kFwdK, na = TcS::kAdjN * TcS::kAdjK;
+    return TcMatrices{tc_mat.get() + 2 * nf, tc_mat.get() + 2 * nf + na};
+  }
+
+  void build_tc_plain(FastClass &c) {
+    if constexpr (std::is_same<R, float>::value) {
+      std::vector<PlaneJob<R>> jobs = c.plain_jobs;
+      for (size_t i = 0; i < jobs.size(); ++i)
+        jobs[i].dst = G.get() + plan.windows[c.win[i]].model_off;
+      make_plane_launch(c.tc_adj_plain, jobs, c.planes, kTcThreads, kTcBatch,
+                        TcS::kAdjSmem, space_adj_tc<kTcP, kTcL>, (size_t)optin_smem());
+    }
+  }
+
+  static constexpr int kTcBatch = 4;  // planes per batch record of the tensor-core kernels
+
+  void set_precision(int mode) {
+    if (mode != 0 && mode != 1) throw DeviceError("unknown precision mode");
+    if (mode == precision) return;
+    release_graph();
+    CK(cudaStreamSynchronize(stream));
+    for (auto &cp : classes) cp->tc = false;
+    tc_windows = 0;
+    if (mode == 1) {
+      if constexpr (!std::is_same<R, float>::value) {
+        throw DeviceError("the split-BF16 tensor-core kernels serve the float library only");
+      } else {
+        if (tc_mat.get() == nullptr) upload_tc_matrices();
+        const int limit = optin_smem();
+        if ((int)TcS::kFwdSmem > limit || (int)TcS::kAdjSmem > limit)
+          throw DeviceError("not enough shared memory for the tensor-core kernels");
+        CK(cudaFuncSetAttribute(space_fwd_tc<kTcP, kTcL>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, TcS::kFwdSmem));
+        CK(cudaFuncSetAttribute(space_adj_tc<kTcP, kTcL>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, TcS::kAdjSmem));
+        for (auto &cp : classes) {
+          FastClass &c = *cp;
+          if (!tc_shape(plan.windows[c.win[0]])) continue;
+          make_plane_launch(c.tc_fwd, c.fwd_jobs, c.planes, kTcThreads, kTcBatch,
+                            TcS::kFwdSmem, space_fwd_tc<kTcP, kTcL>, (size_t)limit);
+          make_plane_launch(c.tc_adj, c.plain_jobs, c.planes, kTcThreads, kTcBatch,
+                            TcS::kAdjSmem, space_adj_tc<kTcP, kTcL>, (size_t)limit);
+          if (G.get() != nullptr) build_tc_plain(c);
+          c.tc = true;
+          tc_windows += (long)c.win.size();
+        }
+        CK(cudaStreamSynchronize(stream));
+      }
+    }
+    precision = mode;
+  }
+
+  // error word of the tensor-core kernels (read after the stream's work)
+  void check_tc_error() {
+    if (precision != 1 || tc_err.get() == nullptr) return;
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, tc_err.get(), sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    if (h) throw DeviceError("a tensor-core kernel gave up waiting for its MMAs");
   }
 
   void build_time_group(TimeGroup &g) {
@@ -1824,6 +1973,7 @@ class Engine {
         jobs[i].dst = G.get() + plan.windows[c.win[i]].model_off;
       make_plane_launch(c.pl_adj_plain, jobs, c.planes, c.av().nt, c.av().np, c.av().smem,
                         c.av().fn);
+      if (c.tc) build_tc_plain(c);
     }
     for (size_t k = 0; k < pending_plain.size(); ++k) {
       auto jobs = pending_plain[k];
@@ -1872,6 +2022,15 @@ class Engine {
   }
 
   void launch_space_fwd(const FastClass &c) {
+    if constexpr (std::is_same<R, float>::value) {
+      if (c.tc) {
+        if (c.tc_fwd.n_batch == 0) return;
+        space_fwd_tc<kTcP, kTcL><<<c.tc_fwd.grid, kTcThreads, TcS::kFwdSmem, stream>>>(
+            c.tc_fwd.batches(), tc_fwd_mats(), tc_err.get());
+        CK(cudaGetLastError());
+        return;
+      }
+    }
     if (c.pl_fwd.n_batch == 0) return;
     c.fv().fn<<<c.pl_fwd.grid, c.pl_fwd.nt, c.pl_fwd.smem, stream>>>(c.pl_fwd.batches());
     CK(cudaGetLastError());
@@ -1879,6 +2038,17 @@ class Engine {
 
   void launch_space_adj(const FastClass &c, const PlaneLaunch &L, int epilogue, R step, R lamb,
                         const R *lamb_dev = nullptr) {
+    if constexpr (std::is_same<R, float>::value) {
+      if (c.tc) {
+        const PlaneLaunch &T = &L == &c.pl_adj_plain ? c.tc_adj_plain : c.tc_adj;
+        if (T.n_batch == 0) return;
+        space_adj_tc<kTcP, kTcL><<<T.grid, kTcThreads, TcS::kAdjSmem, stream>>>(
+            T.batches(), tc_adj_mats(), epilogue, step, lamb, multi ? step_dev.get() : nullptr,
+            lamb_dev, multi ? pmax.get() : scalar.get(), tc_err.get());
+        CK(cudaGetLastError());
+        return;
+      }
+    }
     if (L.n_batch == 0) return;
     c.av().fn<<<L.grid, L.nt, L.smem, stream>>>(L.batches(), epilogue, step, lamb,
                                                  multi ? step_dev.get() : nullptr, lamb_dev,
@@ -2330,6 +2500,7 @@ class Engine {
     }
     if (model_out != nullptr) model_to_ref(X.get(), model_out);
     output();
+    check_tc_error();
     require_finite(device_norm(data_dev.get(), data_size), "the norm of the deblended output");
   }
 
@@ -2553,7 +2724,8 @@ int agd_gpu_problem_kernels(agd_gpu_problem const *pb, char *buf, int len) {
   const bool sc = !e.classes.empty(), tg = !e.tgroups.empty();
   const int n = std::snprintf(
       buf, (size_t)len, "space_fwd=%s space_adj=%s time_fwd=%s time_adj=%s wavelet=%s",
-      sc ? e.classes[0]->fv().name : "axis_pass", sc ? e.classes[0]->av().name : "axis_pass",
+      !sc ? "axis_pass" : (e.classes[0]->tc ? "space_fwd_tc" : e.classes[0]->fv().name),
+      !sc ? "axis_pass" : (e.classes[0]->tc ? "space_adj_tc" : e.classes[0]->av().name),
       tg ? e.tgroups[0]->fv().name : "time_c2r_ola", tg ? e.tgroups[0]->av().name : "time_r2c",
       !e.wavelets ? "none" : (e.wav_fast ? "wavelet_fast" : "wavelet_apply"));
   return n < 0 || n >= len ? 1 : 0;
@@ -2577,6 +2749,7 @@ int agd_gpu_forward(agd_gpu_problem *pb, AGD_TYPE const *model, AGD_TYPE *record
       agd::CK(cudaMemcpyAsync(record, e.rec_r.get(), e.rec_r.bytes(), cudaMemcpyDeviceToHost,
                               e.stream));
     agd::CK(cudaStreamSynchronize(e.stream));
+    e.check_tc_error();
     return 0;
   });
 }
@@ -2595,6 +2768,7 @@ int agd_gpu_adjoint(agd_gpu_problem *pb, AGD_TYPE const *record, AGD_TYPE *model
       e.launch_axis(e.adj_plain[k], 0, agd::kStore, 0, 0);
     e.launch_line_adj(e.line_adj_plain, agd::kStore, 0, 0);
     e.model_to_ref(e.G.get(), model);
+    e.check_tc_error();
     return 0;
   });
 }
@@ -2891,6 +3065,15 @@ int agd_gpu_batch_create(int n_problems, int const *n_patches, int const *const 
 }
 
 void agd_gpu_release_cache(void) { agd::DevicePool::release_all(); }
+
+int agd_gpu_problem_set_precision(agd_gpu_problem *pb, int precision, long int *tc_windows) {
+  if (pb == nullptr) return 1;
+  return guarded("agd_gpu_problem_set_precision", [&] {
+    pb->eng->set_precision(precision);
+    if (tc_windows != nullptr) *tc_windows = pb->eng->tc_windows;
+    return 0;
+  });
+}
 
 int agd_gpu_problem_steps(agd_gpu_problem const *pb, AGD_TYPE *steps) {
   if (pb == nullptr || steps == nullptr) return 1;

@@ -339,6 +339,7 @@ def measure_single(args, name, rank, world, local, cpu_its):
     sv = workload(name, seed_offset=rank)
     torch.cuda.set_device(local)
     prob = A.Problem.from_survey(sv)
+    tc_windows = prob.set_precision(args.precision) if args.precision else 0
     # warm-up + timed region (CUDA events inside the library, on its stream)
     barrier(world)
     torch.cuda.synchronize()
@@ -358,11 +359,23 @@ def measure_single(args, name, rank, world, local, cpu_its):
     wavelet_kw = {}
     if sv.wavelets is not None:
         wavelet_kw = dict(wavelet_idxs=sv.wavelet_idxs, wavelets=sv.wavelets)
+    def public_call(n_its):
+        """The public API on host data: agd_deblend, or for a precision
+        mode the extension calls (plan, set the mode, solve, release)."""
+        if not args.precision:
+            return A.deblend(sv.volumes, sv.window_shapes, sv.coords, sv.shottimes,
+                             sv.channels, sv.trace_types, sv.initial_factor, n_its, 0, sv.data,
+                             **wavelet_kw)
+        p = A.Problem.from_survey(sv)
+        p.set_precision(args.precision)
+        res = p.solve(sv.data, sv.initial_factor, n_its)
+        p.close()
+        return res
+
     if not args.no_e2e:
         # one untimed call first: the first call in a process also pays the
         # one-time mapping of fresh device memory
-        A.deblend(sv.volumes, sv.window_shapes, sv.coords, sv.shottimes, sv.channels,
-                  sv.trace_types, sv.initial_factor, 2, 0, sv.data, **wavelet_kw)
+        public_call(2)
         # three timed calls, the median counts (one call is a single sample of
         # host-side set-up time)
         calls = []
@@ -370,9 +383,7 @@ def measure_single(args, name, rank, world, local, cpu_its):
             torch.cuda.synchronize()
             barrier(world)
             t0 = time.perf_counter()
-            out = A.deblend(sv.volumes, sv.window_shapes, sv.coords, sv.shottimes,
-                            sv.channels, sv.trace_types, sv.initial_factor, sv.n_its, 0,
-                            sv.data, **wavelet_kw)
+            out = public_call(sv.n_its)
             torch.cuda.synchronize()
             calls.append(barrier_max(world, time.perf_counter() - t0))
         e2e_s = float(np.median(calls))
@@ -452,6 +463,10 @@ def measure_single(args, name, rank, world, local, cpu_its):
                         "call_s": e2e_s, "n_its": sv.n_its, "snr_db": snr},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
                 "ms_forward_half": ms_fwd, "ms_adjoint_half": ms_adj}
+        if args.precision:
+            line["precision"] = {"mode": "split_bf16", "tc_windows": tc_windows}
+            line["metric"] = line["metric"].replace("plain FP32", "split-BF16 space DFTs")
+            line["dtype"] = "f32 + split-bf16 tensor cores"
     prob.close()
     return line
 
@@ -605,6 +620,8 @@ def main():
     ap.add_argument("--cpu-its", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision", type=int, default=0, choices=[0, 1],
+                    help="1: split-BF16 tensor-core space DFTs (agd_gpu_problem_set_precision)")
     ap.add_argument("--no-workloads", action="store_true",
                     help="only the headline workload (no vibroseis_4d / uneven_gathers entries)")
     ap.add_argument("--workload", default="two_volume_3d",
@@ -622,7 +639,7 @@ def main():
         else:
             line = measure_single(args, args.workload, rank, world, local, args.cpu_its)
         if (world == 1 and args.workload == "two_volume_3d" and not args.no_workloads
-                and line is not None):
+                and not args.precision and line is not None):
             # the other benchmark workloads, each measured the same way, in
             # the same JSON line
             line["workloads"] = {

@@ -199,6 +199,20 @@ int agd_blend_device_noalloc(int n_patches, int const *n_traces, int const *n_ti
                              enum AGDTraceType const *const *trace_types_out,
                              AGD_TYPE *data_out_dev, void *stream);
 
+/* Precision of the space axes of the FK operator (no counterpart in the
+ * reference, whose FFTs are FFTW's in AGD_TYPE; src/fk.c:307-452).
+ * 0 (default): FP32 FFT kernels.  1: split-BF16 tensor-core contractions -
+ * the space DFT of every window whose three space axes have padded length 20
+ * and window length 16 (windows (16, 16, 16, nt)) runs as hi + lo BF16
+ * products with FP32 accumulation on the tcgen05 tensor cores (about 16
+ * significant bits per operand); the time axis, the wavelet, the blend and
+ * the ISTA update stay FP32.  Mode 1 needs the float library.  tc_windows
+ * (may be NULL) receives the number of windows the tensor-core kernels
+ * serve.  Applies to later operator, solver and timing calls on the
+ * handle. */
+int agd_gpu_problem_set_precision(agd_gpu_problem *problem, int precision,
+                                  long int *tc_windows);
+
 /* ---------------------------------------------------------------------------
  * Learned warm start (no counterpart in the reference, whose solver starts
  * every solve from a zero model, src/model.c:1160-1185).
