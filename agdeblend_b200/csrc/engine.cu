@@ -1508,10 +1508,14 @@ class Engine {
         jobs[i].dst = G.get() + plan.windows[c.win[i]].model_off;
       make_plane_launch(c.tc_adj_plain, jobs, c.planes, kTcThreads, kTcBatch,
                         TcS::kAdjSmem, space_adj_tc<kTcP, kTcL>, (size_t)optin_smem());
+      tc_grid(c.tc_adj_plain);
     }
   }
 
   static constexpr int kTcBatch = 4;  // planes per batch record of the tensor-core kernels
+  // the tensor-core kernels are sized for two CTAs per SM (shared memory,
+  // registers and TMEM columns), whatever the occupancy query answers
+  void tc_grid(PlaneLaunch &L) const { L.grid = std::max(1, std::min(L.n_batch, 2 * n_sm)); }
 
   void set_precision(int mode) {
     if (mode != 0 && mode != 1) throw DeviceError("unknown precision mode");
@@ -1532,6 +1536,11 @@ class Engine {
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, TcS::kFwdSmem));
         CK(cudaFuncSetAttribute(space_adj_tc<kTcP, kTcL>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, TcS::kAdjSmem));
+        // all of the unified L1 / shared memory as shared memory: two CTAs per SM
+        CK(cudaFuncSetAttribute(space_fwd_tc<kTcP, kTcL>,
+                                cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        CK(cudaFuncSetAttribute(space_adj_tc<kTcP, kTcL>,
+                                cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         for (auto &cp : classes) {
           FastClass &c = *cp;
           if (!tc_shape(plan.windows[c.win[0]])) continue;
@@ -1539,6 +1548,8 @@ class Engine {
                             TcS::kFwdSmem, space_fwd_tc<kTcP, kTcL>, (size_t)limit);
           make_plane_launch(c.tc_adj, c.plain_jobs, c.planes, kTcThreads, kTcBatch,
                             TcS::kAdjSmem, space_adj_tc<kTcP, kTcL>, (size_t)limit);
+          tc_grid(c.tc_fwd);
+          tc_grid(c.tc_adj);
           if (G.get() != nullptr) build_tc_plain(c);
           c.tc = true;
           tc_windows += (long)c.win.size();

@@ -3,6 +3,7 @@
 // always starts from a zero model (src/model.c:1160-1185).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 
 #include "agdeblend_gpu.h"
@@ -12,19 +13,21 @@ namespace {
 
 template <int BN>
 cudaError_t launch_gemm(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K,
-                        int lda, int ldb, int ldc, float alpha, float beta, int *err,
-                        cudaStream_t s) {
+                        int lda, int ldb, int ldc, float alpha, float beta, int splits,
+                        int *err, cudaStream_t s) {
   using L = agd::TcGemmSmem<BN>;
-  static bool configured = false;  // the attribute is per function, set once
-  if (!configured) {
-    const cudaError_t e = cudaFuncSetAttribute(
-        agd::tc_gemm_bf16<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
-  const dim3 grid((M + agd::kTcBM - 1) / agd::kTcBM, (N + BN - 1) / BN);
+  // per function and device; cheap enough to set on every launch
+  const cudaError_t e = cudaFuncSetAttribute(
+      agd::tc_gemm_bf16<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
+  if (e != cudaSuccess) return e;
+  // split K: slices of whole 64-wide steps
+  const int steps = (K + agd::kTcBK - 1) / agd::kTcBK;
+  splits = std::max(1, std::min(splits, steps));
+  const int k_split = (steps + splits - 1) / splits * agd::kTcBK;
+  splits = (K + k_split - 1) / k_split;
+  const dim3 grid((M + agd::kTcBM - 1) / agd::kTcBM, (N + BN - 1) / BN, std::max(1, splits));
   agd::tc_gemm_bf16<BN><<<grid, 128, L::kBytes, s>>>(A, B, C, M, N, K, lda, ldb, ldc, alpha,
-                                                      beta, err);
+                                                      beta, k_split, err);
   return cudaGetLastError();
 }
 
@@ -34,12 +37,15 @@ namespace agd {
 
 // C = alpha A B^T + beta C on the tensor cores (see tc_gemm.cuh for the
 // operand rules); err receives 1 if an MMA wait gave up.
+// With splits > 1 the K range is cut into slices whose partial products are
+// added into C with atomics: C must hold beta C already (beta is ignored).
 cudaError_t tc_gemm(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K,
                     int lda, int ldb, int ldc, float alpha, float beta, int *err,
-                    cudaStream_t s) {
+                    cudaStream_t s, int splits = 1) {
   if (M <= 0 || N <= 0) return cudaSuccess;
-  if (N <= 64) return launch_gemm<64>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, err, s);
-  return launch_gemm<128>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, err, s);
+  if (N <= 64)
+    return launch_gemm<64>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, splits, err, s);
+  return launch_gemm<128>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, splits, err, s);
 }
 
 }  // namespace agd
@@ -73,3 +79,551 @@ extern "C" int agd_nn_gemm_bf16(const void *A, const void *B, float *C, int M, i
   }
   return 0;
 }
+
+// ============================================================== the network
+//
+// A 4-level 2-D convolutional encoder-decoder on (n, h, w) images (traces x
+// time samples of a pseudo-deblended gather; h, w multiples of 8).  Level
+// channels c, 2c, 4c, 8c for base c (32: 1,162,945 parameters):
+//   enc  conv(1,c) conv(c,c) | pool | conv(c,2c) conv(2c,2c) | pool |
+//        conv(2c,4c) conv(4c,4c) | pool | conv(4c,8c) conv(8c,4c)
+//   dec  up + skip | conv(4c,4c) conv(4c,2c) | up + skip | conv(2c,2c)
+//        conv(2c,c) | up + skip | conv(c,c) conv(c,1, linear)
+//   output = input + last conv (the network predicts a correction)
+// 3 x 3 convolutions with padding 1 and ReLU, 2 x 2 average pooling, nearest
+// 2x upsampling, additive skips.  Each convolution is an im2col copy and a
+// BF16 tensor-core GEMM with FP32 accumulation; the backward pass computes
+// weight gradients as split-K GEMMs over the pixels and input gradients as
+// GEMMs followed by the transpose of im2col.  Parameters: per layer the
+// weights [cout][ky][kx][cin] then the biases [cout], FP32 masters updated
+// by Adam, BF16 copies for the GEMMs.
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "nn_kernels.cuh"
+
+namespace agd {
+namespace nn {
+
+struct NnError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+inline void ck(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) throw NnError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define NCK(x) ck((x), #x)
+
+template <typename T>
+struct Buf {
+  T *p = nullptr;
+  size_t n = 0;
+  Buf() = default;
+  Buf(const Buf &) = delete;
+  Buf &operator=(const Buf &) = delete;
+  Buf(Buf &&o) noexcept : p(o.p), n(o.n) {
+    o.p = nullptr;
+    o.n = 0;
+  }
+  Buf &operator=(Buf &&o) noexcept {
+    if (this != &o) {
+      reset();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~Buf() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void ensure(size_t count) {
+    if (count <= n) return;
+    reset();
+    NCK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    n = count;
+  }
+  T *get() const { return p; }
+};
+
+inline unsigned grid_of(long n) {
+  return (unsigned)std::max<long>(1, std::min<long>((n + kNnThreads - 1) / kNnThreads, 148L * 16));
+}
+inline int pad8(int c) { return (c + 7) / 8 * 8; }
+
+class Net {
+ public:
+  struct Layer {
+    int in, out;      // tensor indices
+    int cin, cout;
+    int relu;
+    long w_off, b_off;  // offsets in the parameter vector
+    int cin_s, cout_s, kp;
+  };
+  enum OpKind { kConv, kPool, kUpAdd };
+  struct Op {
+    OpKind kind;
+    int a, b, out;  // conv: layer a; pool: in a; up-add: low a, skip b
+  };
+  struct Tensor {
+    int level, C, Cs;
+    Buf<uint16_t> v;
+    Buf<float> g;
+  };
+
+  int base;
+  long n_params = 0;
+  std::vector<Layer> layers;
+  std::vector<Op> ops;
+  std::vector<Tensor> t;
+  // parameters and optimiser state
+  Buf<float> w, grad, m, v;
+  std::vector<Buf<uint16_t>> wp, wpt;  // per layer: [cout_s][kp], [kp][cout_s] BF16
+  Buf<float> dwp;                      // weight-gradient GEMM output
+  // scratch
+  Buf<uint16_t> col, colT, dz, dzT;
+  Buf<float> z, dcol, in_f, out_f, tgt_f, last_f;
+  Buf<double> loss_d;
+  Buf<int> err;
+  cudaStream_t s = nullptr;
+  long adam_t = 0;
+  int cur_n = 0, cur_h = 0, cur_w = 0;
+
+  explicit Net(int base_c, unsigned seed) : base(base_c) {
+    NCK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    const int c = base;
+    auto tensor = [&](int level, int C) {
+      Tensor x;
+      x.level = level;
+      x.C = C;
+      x.Cs = pad8(C);
+      t.push_back(std::move(x));
+      return (int)t.size() - 1;
+    };
+    auto conv = [&](int in, int cout, int relu) {
+      Layer L{};
+      L.in = in;
+      L.cin = t[in].C;
+      L.cout = cout;
+      L.relu = relu;
+      L.out = tensor(t[in].level, cout);
+      L.cin_s = t[in].Cs;
+      L.cout_s = pad8(cout);
+      L.kp = (9 * L.cin + 15) / 16 * 16;
+      L.w_off = n_params;
+      n_params += 9L * L.cin * L.cout;
+      L.b_off = n_params;
+      n_params += L.cout;
+      layers.push_back(L);
+      ops.push_back(Op{kConv, (int)layers.size() - 1, 0, L.out});
+      return L.out;
+    };
+    auto pool = [&](int in) {
+      const int o = tensor(t[in].level + 1, t[in].C);
+      ops.push_back(Op{kPool, in, 0, o});
+      return o;
+    };
+    auto upadd = [&](int low, int skip) {
+      const int o = tensor(t[skip].level, t[skip].C);
+      ops.push_back(Op{kUpAdd, low, skip, o});
+      return o;
+    };
+    const int x0 = tensor(0, 1);
+    const int s1 = conv(conv(x0, c, 1), c, 1);
+    const int s2 = conv(conv(pool(s1), 2 * c, 1), 2 * c, 1);
+    const int s3 = conv(conv(pool(s2), 4 * c, 1), 4 * c, 1);
+    const int bn = conv(conv(pool(s3), 8 * c, 1), 4 * c, 1);
+    const int d3 = conv(conv(upadd(bn, s3), 4 * c, 1), 2 * c, 1);
+    const int d2 = conv(conv(upadd(d3, s2), 2 * c, 1), c, 1);
+    conv(conv(upadd(d2, s1), c, 1), 1, 0);
+    // He-normal weights (the last layer scaled down: the network starts
+    // near the identity), zero biases
+    std::vector<float> h(n_params, 0.f);
+    std::mt19937 rng(seed);
+    std::normal_distribution<float> nd(0.f, 1.f);
+    for (size_t li = 0; li < layers.size(); ++li) {
+      const Layer &L = layers[li];
+      const float sd = std::sqrt(2.f / (9.f * L.cin)) * (li + 1 == layers.size() ? 0.1f : 1.f);
+      for (long i = 0; i < 9L * L.cin * L.cout; ++i) h[L.w_off + i] = sd * nd(rng);
+    }
+    w.ensure(n_params);
+    grad.ensure(n_params);
+    m.ensure(n_params);
+    v.ensure(n_params);
+    NCK(cudaMemcpy(w.get(), h.data(), n_params * sizeof(float), cudaMemcpyHostToDevice));
+    NCK(cudaMemset(m.get(), 0, n_params * sizeof(float)));
+    NCK(cudaMemset(v.get(), 0, n_params * sizeof(float)));
+    wp.resize(layers.size());
+    wpt.resize(layers.size());
+    size_t dwp_max = 0;
+    for (size_t li = 0; li < layers.size(); ++li) {
+      const Layer &L = layers[li];
+      wp[li].ensure((size_t)L.cout_s * L.kp);
+      wpt[li].ensure((size_t)L.kp * L.cout_s);
+      dwp_max = std::max(dwp_max, (size_t)L.cout_s * L.kp);
+    }
+    dwp.ensure(dwp_max);
+    loss_d.ensure(1);
+    err.ensure(1);
+    NCK(cudaMemset(err.get(), 0, sizeof(int)));
+    pack_weights();
+  }
+
+  ~Net() {
+    if (s) cudaStreamDestroy(s);
+  }
+
+  // BF16 GEMM copies of the weights: Wp[co][k] and WpT[k][co], zero-padded
+  void pack_weights() {
+    for (size_t li = 0; li < layers.size(); ++li) {
+      const Layer &L = layers[li];
+      pack_kernel<<<grid_of((long)L.cout_s * L.kp), kNnThreads, 0, s>>>(
+          w.get() + L.w_off, L.cout, 9 * L.cin, L.cout_s, L.kp, wp[li].get(), wpt[li].get());
+      NCK(cudaGetLastError());
+    }
+  }
+
+
+
+
+
+
+  long pixels(int level) const {
+    return (long)cur_n * (cur_h >> level) * (cur_w >> level);
+  }
+
+  // buffers for n images of h x w
+  void shape(int n, int h, int wd) {
+    if (h % 8 || wd % 8 || n <= 0) throw NnError("image sides must be multiples of 8");
+    cur_n = n;
+    cur_h = h;
+    cur_w = wd;
+    size_t col_max = 0, z_max = 0;
+    for (Tensor &x : t) {
+      const long P = pixels(x.level);
+      x.v.ensure((size_t)P * x.Cs);
+      x.g.ensure((size_t)P * x.Cs);
+    }
+    for (const Layer &L : layers) {
+      const long P = pixels(t[L.in].level);
+      col_max = std::max(col_max, (size_t)P * L.kp);
+      z_max = std::max(z_max, (size_t)P * L.cout_s);
+    }
+    col.ensure(col_max);
+    colT.ensure(col_max);
+    dcol.ensure(col_max);
+    z.ensure(z_max);
+    dz.ensure(z_max);
+    dzT.ensure(z_max);
+    const long P0 = pixels(0);
+    in_f.ensure(P0);
+    out_f.ensure(P0);
+    tgt_f.ensure(P0);
+    last_f.ensure((size_t)P0 * t.back().Cs);
+  }
+
+  void gemm(const uint16_t *A, const uint16_t *B, float *C, long M, int N, long K, long lda,
+            long ldb, int ldc, float beta, int splits = 1) {
+    if (M > INT32_MAX || K > INT32_MAX || lda > INT32_MAX || ldb > INT32_MAX)
+      throw NnError("GEMM too large");
+    NCK(tc_gemm(A, B, C, (int)M, N, (int)K, (int)lda, (int)ldb, ldc, 1.f, beta, err.get(), s,
+                splits));
+  }
+
+  void conv_forward(const Layer &L, bool keep_f32) {
+    const Tensor &X = t[L.in];
+    Tensor &Y = t[L.out];
+    const long P = pixels(X.level);
+    const int H = cur_h >> X.level, Wd = cur_w >> X.level;
+    im2col3x3<<<grid_of(P * L.kp), kNnThreads, 0, s>>>(X.v.get(), cur_n, H, Wd, L.cin, X.Cs,
+                                                       L.kp, col.get());
+    NCK(cudaGetLastError());
+    gemm(col.get(), wp[&L - layers.data()].get(), z.get(), P, L.cout_s, L.kp, L.kp, L.kp,
+         L.cout_s, 0.f);
+    bias_act<<<grid_of(P * L.cout_s), kNnThreads, 0, s>>>(
+        z.get(), w.get() + L.b_off, P, L.cout, L.cout_s, L.relu, Y.v.get(),
+        keep_f32 ? last_f.get() : nullptr);
+    NCK(cudaGetLastError());
+  }
+
+  // n images (device fp32 [n][h][w]) -> out_f = input + network correction
+  void forward(const float *in_dev) {
+    const long P0 = pixels(0);
+    NCK(cudaMemcpyAsync(in_f.get(), in_dev, P0 * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    load_input<<<grid_of(P0 * t[0].Cs), kNnThreads, 0, s>>>(in_f.get(), P0, t[0].Cs,
+                                                             t[0].v.get());
+    NCK(cudaGetLastError());
+    for (const Op &op : ops) {
+      if (op.kind == kConv) {
+        conv_forward(layers[op.a], op.a + 1 == (int)layers.size());
+      } else if (op.kind == kPool) {
+        const Tensor &X = t[op.a];
+        avgpool2<<<grid_of(pixels(X.level + 1) * X.Cs), kNnThreads, 0, s>>>(
+            X.v.get(), cur_n, cur_h >> X.level, cur_w >> X.level, X.Cs, t[op.out].v.get());
+        NCK(cudaGetLastError());
+      } else {
+        const Tensor &S = t[op.b];
+        upsample2_add<<<grid_of(pixels(S.level) * S.Cs), kNnThreads, 0, s>>>(
+            t[op.a].v.get(), S.v.get(), cur_n, cur_h >> S.level, cur_w >> S.level, S.Cs,
+            t[op.out].v.get());
+        NCK(cudaGetLastError());
+      }
+    }
+    residual_out<<<grid_of(P0), kNnThreads, 0, s>>>(in_f.get(), last_f.get(), P0, t.back().Cs,
+                                                     out_f.get());
+    NCK(cudaGetLastError());
+  }
+
+  // gradients of the MSE loss against tgt_f (device, [n][h][w]) after
+  // forward(): grad (zeroed here) and loss_d
+  void backward() {
+    const long P0 = pixels(0);
+    NCK(cudaMemsetAsync(grad.get(), 0, n_params * sizeof(float), s));
+    for (Tensor &x : t) NCK(cudaMemsetAsync(x.g.get(), 0, x.g.n * sizeof(float), s));
+    NCK(cudaMemsetAsync(loss_d.get(), 0, sizeof(double), s));
+    mse_grad<<<grid_of(P0), kNnThreads, 0, s>>>(out_f.get(), tgt_f.get(), P0, t.back().Cs,
+                                                 t.back().g.get(), loss_d.get());
+    NCK(cudaGetLastError());
+    for (int oi = (int)ops.size() - 1; oi >= 0; --oi) {
+      const Op &op = ops[oi];
+      if (op.kind == kConv) {
+        conv_backward(layers[op.a], op.a > 0);
+      } else if (op.kind == kPool) {
+        const Tensor &X = t[op.a];
+        avgpool2_backward<<<grid_of(pixels(X.level) * X.Cs), kNnThreads, 0, s>>>(
+            t[op.out].g.get(), cur_n, cur_h >> X.level, cur_w >> X.level, X.Cs, t[op.a].g.get());
+        NCK(cudaGetLastError());
+      } else {
+        const Tensor &S = t[op.b];
+        upsample2_backward<<<grid_of(pixels(S.level + 1) * S.Cs), kNnThreads, 0, s>>>(
+            t[op.out].g.get(), cur_n, cur_h >> S.level, cur_w >> S.level, S.Cs,
+            t[op.a].g.get());
+        NCK(cudaGetLastError());
+        const long n = pixels(S.level) * S.Cs;
+        axpy1<<<grid_of(n), kNnThreads, 0, s>>>(t[op.out].g.get(), n, t[op.b].g.get());
+        NCK(cudaGetLastError());
+      }
+    }
+  }
+
+  void conv_backward(const Layer &L, bool need_dx) {
+    const size_t li = &L - layers.data();
+    const Tensor &X = t[L.in];
+    const Tensor &Y = t[L.out];
+    const long P = pixels(X.level);
+    const int H = cur_h >> X.level, Wd = cur_w >> X.level;
+    act_backward<<<grid_of(P * L.cout_s), kNnThreads, 0, s>>>(Y.g.get(), Y.v.get(), P, L.cout,
+                                                               L.cout_s, L.relu, dz.get());
+    NCK(cudaGetLastError());
+    bias_grad<<<L.cout, kNnThreads, 0, s>>>(dz.get(), P, L.cout, L.cout_s,
+                                            grad.get() + L.b_off);
+    NCK(cudaGetLastError());
+    // dW = dZ^T col: both transposed so that the pixels are the K dimension
+    im2col3x3<<<grid_of(P * L.kp), kNnThreads, 0, s>>>(X.v.get(), cur_n, H, Wd, L.cin, X.Cs,
+                                                       L.kp, col.get());
+    NCK(cudaGetLastError());
+    const dim3 tb(32, 8);
+    transpose_bf16<<<dim3((unsigned)((P + 31) / 32), (unsigned)((L.kp + 31) / 32)), tb, 0, s>>>(
+        col.get(), P, L.kp, L.kp, colT.get(), P);
+    NCK(cudaGetLastError());
+    transpose_bf16<<<dim3((unsigned)((P + 31) / 32), (unsigned)((L.cout_s + 31) / 32)), tb, 0,
+                     s>>>(dz.get(), P, L.cout_s, L.cout_s, dzT.get(), P);
+    NCK(cudaGetLastError());
+    NCK(cudaMemsetAsync(dwp.get(), 0, (size_t)L.cout_s * L.kp * sizeof(float), s));
+    const long tiles = ((L.cout_s + 127) / 128) * ((L.kp + (L.kp <= 64 ? 63 : 127)) /
+                                                   (L.kp <= 64 ? 64 : 128));
+    const int splits = (int)std::max<long>(1, std::min<long>(592 / std::max<long>(tiles, 1),
+                                                             (P + 63) / 64));
+    gemm(dzT.get(), colT.get(), dwp.get(), L.cout_s, L.kp, P, P, P, L.kp, 0.f, splits);
+    unpack_grad<<<grid_of((long)L.cout * 9 * L.cin), kNnThreads, 0, s>>>(
+        dwp.get(), L.cout, 9 * L.cin, L.kp, grad.get() + L.w_off);
+    NCK(cudaGetLastError());
+    if (!need_dx) return;
+    // dX = col2im(dZ W)
+    gemm(dz.get(), wpt[li].get(), dcol.get(), P, L.kp, L.cout_s, L.cout_s, L.cout_s, L.kp, 0.f);
+    col2im3x3<<<grid_of(P * L.cin), kNnThreads, 0, s>>>(dcol.get(), cur_n, H, Wd, L.cin, L.kp,
+                                                        t[L.in].g.get(), X.Cs, 1);
+    NCK(cudaGetLastError());
+  }
+
+  void adam(float lr) {
+    ++adam_t;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, (float)adam_t), c2 = 1.f - std::pow(b2, (float)adam_t);
+    adam_step<<<grid_of(n_params), kNnThreads, 0, s>>>(w.get(), grad.get(), m.get(), v.get(),
+                                                        n_params, lr, b1, b2, 1e-8f, c1, c2,
+                                                        nullptr);
+    NCK(cudaGetLastError());
+    pack_weights();
+  }
+
+  void check_errors() {
+    int h = 0;
+    NCK(cudaMemcpyAsync(&h, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    NCK(cudaStreamSynchronize(s));
+    if (h) throw NnError("a tensor-core GEMM gave up waiting for its MMAs");
+  }
+
+  double read_loss() {
+    double l = 0;
+    NCK(cudaMemcpyAsync(&l, loss_d.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+    NCK(cudaStreamSynchronize(s));
+    return l;
+  }
+};
+
+}  // namespace nn
+}  // namespace agd
+
+struct agd_nn {
+  std::unique_ptr<agd::nn::Net> net;
+};
+
+namespace {
+
+template <typename F>
+int nn_guarded(const char *name, F &&f) {
+  try {
+    return f();
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "ERROR: %s\nERROR in %s\n", e.what(), name);
+    return 1;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int agd_nn_create(int base_channels, unsigned seed, agd_nn **net) {
+  if (net == nullptr || base_channels < 1 || base_channels > 256) return 1;
+  *net = nullptr;
+  return nn_guarded("agd_nn_create", [&] {
+    auto h = std::make_unique<agd_nn>();
+    h->net = std::make_unique<agd::nn::Net>(base_channels, seed);
+    *net = h.release();
+    return 0;
+  });
+}
+
+void agd_nn_destroy(agd_nn *net) { delete net; }
+
+long agd_nn_param_count(const agd_nn *net) { return net ? net->net->n_params : -1; }
+
+int agd_nn_get_params(const agd_nn *net, float *params) {
+  if (net == nullptr || params == nullptr) return 1;
+  return nn_guarded("agd_nn_get_params", [&] {
+    agd::nn::Net &n = *net->net;
+    agd::nn::NCK(cudaMemcpyAsync(params, n.w.get(), n.n_params * sizeof(float),
+                                 cudaMemcpyDeviceToHost, n.s));
+    agd::nn::NCK(cudaStreamSynchronize(n.s));
+    return 0;
+  });
+}
+
+int agd_nn_set_params(agd_nn *net, const float *params) {
+  if (net == nullptr || params == nullptr) return 1;
+  return nn_guarded("agd_nn_set_params", [&] {
+    agd::nn::Net &n = *net->net;
+    agd::nn::NCK(cudaMemcpyAsync(n.w.get(), params, n.n_params * sizeof(float),
+                                 cudaMemcpyHostToDevice, n.s));
+    n.pack_weights();
+    agd::nn::NCK(cudaStreamSynchronize(n.s));
+    return 0;
+  });
+}
+
+int agd_nn_forward(agd_nn *net, const float *input, int n, int h, int w, float *output) {
+  if (net == nullptr || input == nullptr || output == nullptr) return 1;
+  return nn_guarded("agd_nn_forward", [&] {
+    agd::nn::Net &nt = *net->net;
+    nt.shape(n, h, w);
+    const long P0 = (long)n * h * w;
+    agd::nn::NCK(cudaMemcpyAsync(nt.tgt_f.get(), input, P0 * sizeof(float),
+                                 cudaMemcpyHostToDevice, nt.s));
+    nt.forward(nt.tgt_f.get());
+    agd::nn::NCK(cudaMemcpyAsync(output, nt.out_f.get(), P0 * sizeof(float),
+                                 cudaMemcpyDeviceToHost, nt.s));
+    nt.check_errors();
+    return 0;
+  });
+}
+
+int agd_nn_loss_grad(agd_nn *net, const float *input, const float *target, int n, int h, int w,
+                     double *loss, float *grad) {
+  if (net == nullptr || input == nullptr || target == nullptr) return 1;
+  return nn_guarded("agd_nn_loss_grad", [&] {
+    agd::nn::Net &nt = *net->net;
+    nt.shape(n, h, w);
+    const long P0 = (long)n * h * w;
+    agd::nn::NCK(cudaMemcpyAsync(nt.tgt_f.get(), input, P0 * sizeof(float),
+                                 cudaMemcpyHostToDevice, nt.s));
+    nt.forward(nt.tgt_f.get());
+    agd::nn::NCK(cudaMemcpyAsync(nt.tgt_f.get(), target, P0 * sizeof(float),
+                                 cudaMemcpyHostToDevice, nt.s));
+    nt.backward();
+    if (loss) *loss = nt.read_loss();
+    if (grad)
+      agd::nn::NCK(cudaMemcpyAsync(grad, nt.grad.get(), nt.n_params * sizeof(float),
+                                   cudaMemcpyDeviceToHost, nt.s));
+    nt.check_errors();
+    return 0;
+  });
+}
+
+int agd_nn_train(agd_nn *net, const float *inputs, const float *targets, long n_samples, int h,
+                 int w, int batch, int epochs, float lr, unsigned seed, double *epoch_loss) {
+  if (net == nullptr || inputs == nullptr || targets == nullptr || n_samples < batch ||
+      batch <= 0 || epochs <= 0)
+    return 1;
+  return nn_guarded("agd_nn_train", [&] {
+    agd::nn::Net &nt = *net->net;
+    nt.shape(batch, h, w);
+    const long hw = (long)h * w;
+    agd::nn::Buf<float> din, dtg, dbatch;
+    agd::nn::Buf<int> didx;
+    din.ensure((size_t)n_samples * hw);
+    dtg.ensure((size_t)n_samples * hw);
+    dbatch.ensure((size_t)batch * hw);
+    didx.ensure(batch);
+    agd::nn::NCK(cudaMemcpyAsync(din.get(), inputs, n_samples * hw * sizeof(float),
+                                 cudaMemcpyHostToDevice, nt.s));
+    agd::nn::NCK(cudaMemcpyAsync(dtg.get(), targets, n_samples * hw * sizeof(float),
+                                 cudaMemcpyHostToDevice, nt.s));
+    std::mt19937 rng(seed);
+    std::vector<int> perm(n_samples);
+    for (long i = 0; i < n_samples; ++i) perm[i] = (int)i;
+    const long steps = n_samples / batch;
+    for (int ep = 0; ep < epochs; ++ep) {
+      std::shuffle(perm.begin(), perm.end(), rng);
+      double sum = 0;
+      for (long st = 0; st < steps; ++st) {
+        agd::nn::NCK(cudaMemcpyAsync(didx.get(), perm.data() + st * batch, batch * sizeof(int),
+                                     cudaMemcpyHostToDevice, nt.s));
+        agd::nn::gather_samples<<<agd::nn::grid_of(batch * hw), agd::nn::kNnThreads, 0,
+                                       nt.s>>>(din.get(), didx.get(), batch, hw, dbatch.get());
+        nt.forward(dbatch.get());
+        agd::nn::gather_samples<<<agd::nn::grid_of(batch * hw), agd::nn::kNnThreads, 0,
+                                       nt.s>>>(dtg.get(), didx.get(), batch, hw,
+                                               nt.tgt_f.get());
+        nt.backward();
+        nt.adam(lr);
+        sum += nt.read_loss();  // also keeps the host in step with the device
+      }
+      if (epoch_loss) epoch_loss[ep] = sum / (double)steps;
+    }
+    nt.check_errors();
+    return 0;
+  });
+}
+
+}  // extern "C"

@@ -3,6 +3,10 @@
 // A (M x K) and B (N x K) row-major BF16 with row strides lda, ldb (elements,
 // multiples of 8, 16-byte aligned rows), K a multiple of 8; C row-major FP32.
 //
+// Split K (gridDim.z > 1): CTA z sums k in [z * k_split, (z + 1) * k_split)
+// and adds alpha times its partial tile into C with atomics (C holds beta C
+// beforehand; the caller scales or zeroes it).
+//
 // One CTA of 128 threads computes a 128 x BN tile: K is walked in 64-wide
 // steps through two shared-memory stages filled by 16-byte cp.async copies
 // (rows and k chunks past the matrix edges are zero-filled); thread 0 issues
@@ -59,7 +63,7 @@ __global__ void __launch_bounds__(128) tc_gemm_bf16(const uint16_t *__restrict__
                                                     const uint16_t *__restrict__ B,
                                                     float *__restrict__ C, int M, int N, int K,
                                                     int lda, int ldb, int ldc, float alpha,
-                                                    float beta, int *err) {
+                                                    float beta, int k_split, int *err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   using L = TcGemmSmem<BN>;
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * L::kStage);
@@ -81,6 +85,13 @@ __global__ void __launch_bounds__(128) tc_gemm_bf16(const uint16_t *__restrict__
   const uint32_t s0 = umma::smem_u32(smem);
   constexpr uint32_t idesc = umma::idesc_bf16(kTcBM, BN);
 
+  // this CTA's K range (split K: a slice of k_split, a multiple of kTcBK)
+  const int kz0 = gridDim.z > 1 ? blockIdx.z * k_split : 0;
+  const int kz1 = gridDim.z > 1 ? min(K, kz0 + k_split) : K;
+  A += kz0;
+  B += kz0;
+  K = kz1 > kz0 ? kz1 - kz0 : 0;
+  const bool split = gridDim.z > 1;
   const int nk = (K + kTcBK - 1) / kTcBK;
   bool ok = true;
   auto stage_a = [&](int s) { return s0 + (uint32_t)s * L::kStage; };
@@ -136,9 +147,15 @@ __global__ void __launch_bounds__(128) tc_gemm_bf16(const uint16_t *__restrict__
       }
       if (row < M) {
         float *c = C + (long)row * ldc + n0 + cc * 16;
+        if (split) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i)
-          if (n0 + cc * 16 + i < N) c[i] = alpha * v[i] + (beta != 0.f ? beta * c[i] : 0.f);
+          for (int i = 0; i < 16; ++i)
+            if (n0 + cc * 16 + i < N && nk > 0) atomicAdd(c + i, alpha * v[i]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            if (n0 + cc * 16 + i < N) c[i] = alpha * v[i] + (beta != 0.f ? beta * c[i] : 0.f);
+        }
       }
     }
   }

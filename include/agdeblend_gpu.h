@@ -225,6 +225,32 @@ int agd_gpu_problem_set_precision(agd_gpu_problem *problem, int precision,
 int agd_nn_gemm_bf16(const void *A, const void *B, float *C, int M, int N, int K, int lda,
                      int ldb, int ldc, float alpha, float beta, void *stream);
 
+/* The warm-start network: a 4-level 2-D convolutional encoder-decoder on
+ * images of n x h x w samples (traces x time; h, w multiples of 8), base
+ * channels c (32: 1,162,945 parameters), output = input + a learned
+ * correction.  Convolutions run as BF16 tensor-core GEMMs with FP32
+ * accumulation, forward and backward; FP32 master parameters, Adam.  Arrays
+ * are host memory, [n][h][w] row-major float.  Parameter layout: per layer
+ * (encoder, bottleneck, decoder order) the weights [cout][3][3][cin] then
+ * the biases [cout]. */
+typedef struct agd_nn agd_nn;
+int agd_nn_create(int base_channels, unsigned seed, agd_nn **net);
+void agd_nn_destroy(agd_nn *net);
+long agd_nn_param_count(const agd_nn *net);
+int agd_nn_get_params(const agd_nn *net, float *params);
+int agd_nn_set_params(agd_nn *net, const float *params);
+/* output = network(input) */
+int agd_nn_forward(agd_nn *net, const float *input, int n, int h, int w, float *output);
+/* mean squared error of network(input) against target, and its gradient
+ * with respect to the parameters (grad may be NULL) */
+int agd_nn_loss_grad(agd_nn *net, const float *input, const float *target, int n, int h, int w,
+                     double *loss, float *grad);
+/* Adam (learning rate lr) over shuffled batches of the n_samples pairs
+ * (inputs, targets), `epochs` passes; epoch_loss (may be NULL) receives the
+ * mean loss of each pass. */
+int agd_nn_train(agd_nn *net, const float *inputs, const float *targets, long n_samples, int h,
+                 int w, int batch, int epochs, float lr, unsigned seed, double *epoch_loss);
+
 #ifdef __cplusplus
 }
 #endif

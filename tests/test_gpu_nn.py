@@ -1,0 +1,54 @@
+"""The warm-start network's tensor-core forward and backward passes against
+the float64 oracle (oracle/nn_oracle.py, which rounds to BF16 where the GPU
+feeds its tensor cores, and whose backpropagation is itself checked against
+finite differences): output, loss and every parameter gradient on small
+shapes; then a short training run lowers the loss.
+
+Tolerances: output and loss 1e-3 relative, gradient vector 2e-2 relative L2
+with cosine similarity above 0.999 (BF16 operands: a sum that lands on the
+other side of a BF16 rounding boundary moves a value by 2^-8)."""
+import numpy as np
+import pytest
+
+import nn_oracle as N
+from agdeblend_b200.nn import WarmStartNet
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("base,n,h,w", [(4, 2, 16, 32), (8, 3, 8, 64), (32, 2, 32, 256)])
+def test_forward_and_gradients_match_oracle(base, n, h, w):
+    net = WarmStartNet(base, seed=base)
+    assert net.n_params == N.param_count(base)
+    rng = np.random.default_rng(base + n)
+    # non-trivial weights everywhere (the network's own last layer starts small)
+    p = N.init_params(base, seed=3).astype(np.float32)
+    net.set_params(p)
+    x = rng.standard_normal((n, h, w)).astype(np.float32)
+    t = (x + 0.5 * rng.standard_normal(x.shape)).astype(np.float32)
+    ora = N.Net(base, p.astype(np.float64), bf16_like_gpu=True)
+    loss_o, g_o = ora.loss_grad(x.astype(np.float64), t.astype(np.float64))
+    y = net.forward(x)
+    assert rel_l2(y, ora.out) <= 1e-3
+    loss, g = net.loss_grad(x, t)
+    assert abs(loss - loss_o) <= 1e-3 * loss_o
+    err = rel_l2(g, g_o)
+    cos = float(np.dot(g.astype(np.float64), g_o) / np.linalg.norm(g) / np.linalg.norm(g_o))
+    print(f"base {base}: gradient rel L2 {err:.2e}, cosine {cos:.6f}")
+    assert err <= 2e-2 and cos >= 0.999
+    net.close()
+
+
+def test_training_lowers_the_loss():
+    rng = np.random.default_rng(9)
+    n, h, w = 64, 16, 64
+    # a task the network can learn quickly: remove a fixed spike pattern
+    clean = np.cumsum(rng.standard_normal((n, h, w)), axis=2).astype(np.float32)
+    clean /= np.std(clean)
+    noisy = clean.copy()
+    noisy[:, ::4, ::8] += 2.0
+    net = WarmStartNet(8, seed=1)
+    losses = net.train(noisy, clean, batch=16, epochs=30, lr=2e-3)
+    assert losses[-1] < 0.3 * losses[0]
+    net.close()

@@ -1,0 +1,32 @@
+"""The float64 network oracle (oracle/nn_oracle.py) against itself: its
+hand-written backpropagation equals central finite differences of its loss
+(float64, no BF16 rounding), and its parameter count is the CUDA network's
+(1,162,945 for base 32 channels)."""
+import numpy as np
+
+import nn_oracle as N
+
+
+def test_param_count_base32():
+    assert N.param_count(32) == 1162945
+
+
+def test_backprop_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    base = 2
+    params = N.init_params(base, seed=1)
+    x = rng.standard_normal((2, 8, 16))
+    target = x + 0.3 * rng.standard_normal(x.shape)
+    net = N.Net(base, params, bf16_like_gpu=False)
+    loss, g = net.loss_grad(x, target)
+    idx = rng.choice(params.size, 60, replace=False)
+    h = 1e-6
+    for i in idx:
+        p1 = params.copy()
+        p1[i] += h
+        p2 = params.copy()
+        p2[i] -= h
+        l1 = N.Net(base, p1, False).loss_grad(x, target)[0]
+        l2 = N.Net(base, p2, False).loss_grad(x, target)[0]
+        fd = (l1 - l2) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd)) + 1e-8, (i, fd, g[i])

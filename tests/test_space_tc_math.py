@@ -131,27 +131,31 @@ def test_adjoint_passes_equal_padded_forward_dft():
     assert np.vdot(fwd_model(x), g) == pytest.approx(np.vdot(x, got), rel=1e-12)
 
 
-@pytest.mark.parametrize("kch,k_used,rows_by_pass", [
-    (6, 2 * P, [P * P, L * P, L * L]),   # forward: K 48 (40 used)
-    (4, 2 * L, [L * L, P * L, P * P]),   # adjoint: K 32
+@pytest.mark.parametrize("kch,k_used,rows_by_pass,smem_end", [
+    # forward: K 48 (40 used); A hi at 0, A lo at 50 row groups; the barrier
+    # sits where the last tile of A lo ends (no MMA reads past it)
+    (6, 2 * P, [P * P, L * P, L * L], 2 * 50 * sbo(6) + 14 * sbo(6)),
+    # adjoint: K 32; the model plane (64000 bytes) is staged over the A area,
+    # the B matrices start at 64000
+    (4, 2 * L, [L * L, P * L, P * P], 64000),
 ])
-def test_operand_offsets_distinct_and_in_bounds(kch, k_used, rows_by_pass):
-    tiles_max = (P * P + 127) // 128
-    size = (tiles_max * 128 // 8) * sbo(kch)
+def test_operand_offsets_distinct_and_in_bounds(kch, k_used, rows_by_pass, smem_end):
+    a_bytes = (P * P // 8) * sbo(kch)  # one operand (hi or lo): the P * P rows
     for rows in rows_by_pass:
         offs = np.array([offset(r, k, kch) for r in range(rows) for k in range(0, k_used, 2)])
-        assert offs.min() >= 0 and offs.max() + 4 <= size
+        assert offs.min() >= 0 and offs.max() + 4 <= a_bytes
         assert len(np.unique(offs)) == offs.size
-        # bytes an MMA can read: tiles of the pass, K steps of 2 chunks
+        # bytes an MMA can read: tiles of the pass, K steps of 2 chunks, from
+        # A lo (the later of the two operands)
         tiles = (rows + 127) // 128
         for t in range(tiles):
             for s in range(kch // 2):
-                start = t * 16 * sbo(kch) + s * 2 * LBO
+                start = a_bytes + t * 16 * sbo(kch) + s * 2 * LBO
                 last = start + 15 * sbo(kch) + LBO + 128
-                assert last <= size
+                assert last <= smem_end
     # the padding chunk (forward: k 40..47) is never written by an epilogue
     if kch * 8 > k_used:
-        pad = {offset(r, k, kch) for r in range(tiles_max * 128) for k in range(k_used, kch * 8, 2)}
+        pad = {offset(r, k, kch) for r in range(P * P) for k in range(k_used, kch * 8, 2)}
         used = {offset(r, k, kch) for r in range(P * P) for k in range(0, k_used, 2)}
         assert not pad & used
 
