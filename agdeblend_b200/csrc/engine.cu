@@ -25,6 +25,7 @@
 #include "plan.hpp"
 #include "wavelet_fast.cuh"
 #include "line_dft.cuh"
+#include "nn_api.hpp"
 #include "space_tc.cuh"
 
 namespace agd {
@@ -2515,6 +2516,111 @@ class Engine {
     require_finite(device_norm(data_dev.get(), data_size), "the norm of the deblended output");
   }
 
+  // ------------------------------------------------------------ warm start
+  //
+  // A model x0 whose FK operator reproduces an estimate v of the deblended
+  // data: per window, x0_w = r2c(taper_w * v / fold2) / (N scaler) with
+  // fold2 = sum over windows of taper_w^2 (space and time tapers at each
+  // data sample).  Then F x0 = sum_w taper_w^2 v / fold2 = v exactly, since
+  // within a zero-padded window c2r(r2c(u)) = N u.  The adjoint kernels
+  // compute r2c(taper * .) * scaler with bins 1..(Pt-1)/2 doubled
+  // (src/fk.c:375-452); with N scaler^2 = 1, x0 is the adjoint of v / fold2
+  // with those bins halved.  With a source wavelet, v is first correlated
+  // with it (the wavelet operator is all-pass: its adjoint inverts it on
+  // live traces).  No counterpart in the reference, which starts from zero.
+  DevArray<R> inv_fold2;  // 1 / fold2 per patch data sample
+  // fold2 is at least 0.5^(D+1) (D space axes) on the samples the model
+  // represents; with a source wavelet the last samples of a trace lie in the
+  // tapered tail of the last time window, where fold2 falls towards 0: the
+  // floor keeps 1 / fold2 bounded there (such samples are only approached).
+  static constexpr R kFoldFloor = (R)0.05;
+
+  void halve_model_interior() {
+    for (const WindowPlan &W : plan.windows)
+      if (W.model_size)
+        halve_interior_bins<R><<<grid_for(W.model_size), kThreads, 0, stream>>>(
+            X.get() + W.model_off, W.T, W.F, W.plane(), (W.Pt - 1) / 2);
+    CK(cudaGetLastError());
+  }
+
+  // X <- adjoint of the window traces Y (no wavelet), bins halved
+  void model_from_traces() {
+    launch_time_adj(nullptr, 0);
+    launch_space_adj_all(kStore, (R)0, (R)0, nullptr);
+    halve_model_interior();
+  }
+
+  void scatter_to_traces(const R *data, const R *scale) {
+    if (Y.get() != nullptr) CK(cudaMemsetAsync(Y.get(), 0, Y.bytes(), stream));
+    if (out_traces)
+      traces_from_data<R><<<(unsigned)out_traces, kThreads, 0, stream>>>(
+          out_ptr.get(), out_src.get(), out_dst.get(), out_nt.get(), data, scale, Y.get());
+    CK(cudaGetLastError());
+  }
+
+  void ensure_fold2() {
+    if (inv_fold2.get() != nullptr || data_size == 0) return;
+    inv_fold2.alloc(data_size);
+    scatter_to_traces(nullptr, nullptr);  // ones on every data sample
+    model_from_traces();
+    launch_space_fwd_all();
+    launch_time_fwd();
+    if (out_traces)
+      output_gather<R><<<(unsigned)out_traces, kThreads, 0, stream>>>(
+          out_ptr.get(), out_src.get(), out_dst.get(), out_nt.get(), Y.get(), inv_fold2.get());
+    reciprocal_floor<R><<<grid_for(data_size), kThreads, 0, stream>>>(inv_fold2.get(),
+                                                                      data_size, kFoldFloor);
+    CK(cudaGetLastError());
+  }
+
+  // X <- the warm model of the estimate held in data_dev
+  void warm_model() {
+    ensure_fold2();
+    scatter_to_traces(data_dev.get(), inv_fold2.get());
+    if (wavelets) launch_wavelet(-1);
+    model_from_traces();
+  }
+
+  // The solver from a warm model: the initial step and the thresholds of
+  // the n_its schedule as agd_gpu_solve computes them from the blended
+  // input in rec_d, then X <- warm_model(estimate) and iterations [begin,
+  // n_its) (begin >= 1: the schedule continues from iteration begin).
+  void solve_warm(R initial_factor, int n_its, int begin, R const *const *estimate,
+                  int print_freq) {
+    const double r0 = record_norm(rec_d.get());
+    require_finite(r0, "the norm of the blended input data");
+    start_schedule(initial_factor, n_its, std::max(1, n_its - 1));
+    upload_data(estimate);
+    warm_iterations(n_its, begin, print_freq);
+  }
+
+  // data_dev holds the estimate; the schedule is loaded: X <- warm model,
+  // then iterations [begin, n_its) and the output
+  void warm_iterations(int n_its, int begin, int print_freq) {
+    require_finite(device_norm(data_dev.get(), data_size), "the norm of the estimate");
+    warm_model();
+    const int counter = begin - 1;  // iteration `begin` uses table row begin - 1
+    CK(cudaMemcpyAsync(lamb_counter.get(), &counter, sizeof(int), cudaMemcpyHostToDevice,
+                       stream));
+    if (print_freq > 0) {
+      for (int it = begin; it < n_its; ++it) {
+        const bool print_residual = it % print_freq == 0;
+        iteration_body(print_residual);
+        if (print_residual) {
+          const double r = std::sqrt(read_dscalar());
+          require_finite(r, "the residual norm");
+          std::printf("Iteration %d Residual %f\n", it, r);
+        }
+      }
+    } else if (n_its > begin) {
+      capture_iteration();
+      for (int it = begin; it < n_its; ++it) replay_iteration();
+    }
+    output();
+    check_tc_error();
+    require_finite(device_norm(data_dev.get(), data_size), "the norm of the deblended output");
+  }
+
   // host <-> device model in the reference layout
   void model_from_ref(const R *host) {
     DevArray<C> tmp;
@@ -2549,6 +2655,7 @@ using EngineR = Engine<real>;
 
 struct agd_gpu_problem {
   std::unique_ptr<agd::EngineR> eng;
+  std::vector<std::vector<int>> shapes;  // per patch: space sizes..., time samples
   // kept for blend_input (raw shot times, channels, trace types)
   std::vector<std::vector<long>> shottimes;
   std::vector<std::vector<int>> channels;
@@ -2588,6 +2695,7 @@ int create_from_plan(const std::vector<agd::ProblemArgs> &args, agd::Plan &&plan
       for (int p = 0; p < a.n_patches; ++p, ++gp) {
         const int n = plan.n_traces[gp];
         pb->shottimes.emplace_back(a.shottimes[p], a.shottimes[p] + n);
+        pb->shapes.emplace_back(a.shapes[p], a.shapes[p] + a.n_dims[a.volumes[p]]);
         pb->channels.emplace_back(a.channels[p], a.channels[p] + n);
         pb->trace_types.emplace_back(a.trace_types[p], a.trace_types[p] + n);
       }
@@ -3076,6 +3184,123 @@ int agd_gpu_batch_create(int n_problems, int const *n_patches, int const *const 
 }
 
 void agd_gpu_release_cache(void) { agd::DevicePool::release_all(); }
+
+int agd_gpu_solve_warm(agd_gpu_problem *pb, AGD_TYPE initial_factor, int n_its, int it_begin,
+                       int print_freq, AGD_TYPE const *const *estimate, AGD_TYPE *const *data) {
+  if (pb == nullptr || data == nullptr || estimate == nullptr) return 1;
+  if (n_its <= 0 || it_begin < 1 || it_begin > n_its) {
+    std::fprintf(stderr,
+                 "ERROR: need n_its > 0 and 1 <= it_begin <= n_its\nERROR in agd_gpu_solve_warm\n");
+    return 1;
+  }
+  return guarded("agd_gpu_solve_warm", [&] {
+    agd::EngineR &e = *pb->eng;
+    e.upload_data(data);
+    pb->input_blend();
+    e.solve_warm(initial_factor, n_its, it_begin, estimate, print_freq);
+    e.download_data(data);
+    return 0;
+  });
+}
+
+namespace {
+
+// Images for the network: every line of a patch along its trace axis (the
+// space axis along which the shot times change least, but change: receiver
+// gathers of consecutive shots) is one image of (traces x time samples).
+std::vector<agd::nn::ImageGroup> image_groups(const agd_gpu_problem &pb) {
+  std::vector<agd::nn::ImageGroup> groups;
+  const agd::EngineR &e = *pb.eng;
+  for (size_t p = 0; p < pb.shapes.size(); ++p) {
+    const std::vector<int> &sh = pb.shapes[p];
+    const int D = (int)sh.size() - 1;
+    std::vector<long> stride(sh.size(), 1);
+    for (int d = (int)sh.size() - 2; d >= 0; --d) stride[d] = stride[d + 1] * sh[d + 1];
+    // mean |shot-time step| along each space axis (traces in C order)
+    int axis = D - 1;
+    double best = 0;
+    for (int d = 0; d < D; ++d) {
+      if (sh[d] < 2) continue;
+      const long st = stride[d] / sh[D];  // trace stride of axis d
+      double sum = 0;
+      long cnt = 0;
+      const long n_tr = (long)pb.shottimes[p].size();
+      for (long t = 0; t < n_tr; ++t)
+        if ((t / st) % sh[d] + 1 < sh[d]) {
+          sum += std::fabs((double)(pb.shottimes[p][t + st] - pb.shottimes[p][t]));
+          ++cnt;
+        }
+      const double m = cnt ? sum / cnt : 0;
+      if (m > 0 && (best == 0 || m < best)) {
+        best = m;
+        axis = d;
+      }
+    }
+    agd::nn::ImageGroup *g = nullptr;
+    for (auto &x : groups)
+      if (x.rows == sh[axis] && x.cols == sh[D] && x.row_stride == stride[axis]) g = &x;
+    if (g == nullptr) {
+      groups.push_back(agd::nn::ImageGroup{});
+      g = &groups.back();
+      g->rows = sh[axis];
+      g->cols = sh[D];
+      g->row_stride = stride[axis];
+    }
+    // every combination of the other space indices
+    const long n_img = stride[0] * sh[0] / ((long)sh[axis] * sh[D]);
+    for (long i = 0; i < n_img; ++i) {
+      long rem = i, off = 0;
+      for (int d = D - 1; d >= 0; --d) {
+        if (d == axis) continue;
+        off += (rem % sh[d]) * stride[d];
+        rem /= sh[d];
+      }
+      g->base.push_back(e.patch_off[p] + off);
+    }
+  }
+  return groups;
+}
+
+}  // namespace
+
+int agd_gpu_solve_learned(agd_gpu_problem *pb, agd_nn *net, AGD_TYPE initial_factor, int n_its,
+                          int it_begin, int print_freq, AGD_TYPE *const *data) {
+  if (pb == nullptr || net == nullptr || data == nullptr) return 1;
+  if (n_its <= 0 || it_begin < 1 || it_begin > n_its) {
+    std::fprintf(stderr,
+                 "ERROR: need n_its > 0 and 1 <= it_begin <= n_its\nERROR in agd_gpu_solve_learned\n");
+    return 1;
+  }
+  return guarded("agd_gpu_solve_learned", [&] {
+#ifdef AGD_DOUBLE
+    throw std::runtime_error("the warm-start network serves the float library only");
+#else
+    agd::EngineR &e = *pb->eng;
+    e.upload_data(data);
+    pb->input_blend();
+    const double r0 = e.record_norm(e.rec_d.get());
+    agd::EngineR::require_finite(r0, "the norm of the blended input data");
+    e.start_schedule(initial_factor, n_its, std::max(1, n_its - 1));
+    // the pseudo-deblended input in data_dev becomes the network's estimate
+    agd::nn::estimate_images(net, e.data_dev.get(), image_groups(*pb), e.stream);
+    e.warm_iterations(n_its, it_begin, print_freq);
+    e.download_data(data);
+#endif
+    return 0;
+  });
+}
+
+int agd_gpu_warm_model(agd_gpu_problem *pb, AGD_TYPE const *const *estimate, AGD_TYPE *model) {
+  if (pb == nullptr || estimate == nullptr || model == nullptr) return 1;
+  return guarded("agd_gpu_warm_model", [&] {
+    agd::EngineR &e = *pb->eng;
+    e.upload_data(estimate);
+    e.warm_model();
+    e.model_to_ref(e.X.get(), model);
+    e.check_tc_error();
+    return 0;
+  });
+}
 
 int agd_gpu_problem_set_precision(agd_gpu_problem *pb, int precision, long int *tc_windows) {
   if (pb == nullptr) return 1;

@@ -641,6 +641,51 @@ __global__ void next_lambda(const R *__restrict__ table, int *counter, R *out, i
   if (threadIdx.x == 0) *counter = k + 1;
 }
 
+// Window traces from patch data (the transpose of output_gather): for every
+// patch trace and every window trace covering it, y[src + t] = data[dst + t]
+// * scale[dst + t] (scale NULL: 1; data NULL: 1) for t < nt.  One block per
+// patch trace; y is zeroed beforehand.
+template <typename R>
+__global__ void __launch_bounds__(kThreads)
+    traces_from_data(const long *__restrict__ out_ptr, const long *__restrict__ out_src,
+                     const long *__restrict__ out_dst, const int *__restrict__ out_nt,
+                     const R *__restrict__ data, const R *__restrict__ scale, R *y) {
+  const long tr = blockIdx.x;
+  const long b0 = out_ptr[tr];
+  const long b1 = out_ptr[tr + 1];
+  const int nt = out_nt[tr];
+  const long d0 = out_dst[tr];
+  for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+    R v = data != nullptr ? data[d0 + t] : (R)1;
+    if (scale != nullptr) v *= scale[d0 + t];
+    for (long c = b0; c < b1; ++c) y[out_src[c] + t] = v;
+  }
+}
+
+// x = 1 / max(x, floor) where x > 0 (else 0)
+template <typename R>
+__global__ void reciprocal_floor(R *x, long n, R floor) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    x[i] = x[i] > (R)0 ? (R)1 / (x[i] > floor ? x[i] : floor) : (R)0;
+}
+
+// Halves the time-frequency planes f = 1 .. (Pt - 1) / 2 of one window's
+// model ([T][F][plane] complex): undoes the factor 2 that the adjoint
+// applies to those bins (src/fk.c:446), leaving the plain r2c.
+template <typename R>
+__global__ void halve_interior_bins(Cx<R> *x, int T, int F, long plane, int f_last) {
+  const long n = (long)T * F * plane;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    const int f = (int)((i / plane) % F);
+    if (f >= 1 && f <= f_last) {
+      x[i].x *= (R)0.5;
+      x[i].y *= (R)0.5;
+    }
+  }
+}
+
 template <typename R>
 __global__ void model_threshold(Cx<R> *x, long n, R lamb) {
   const R lamb_sq = lamb * lamb;

@@ -14,7 +14,8 @@ namespace {
 template <int BN>
 cudaError_t launch_gemm(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K,
                         int lda, int ldb, int ldc, float alpha, float beta, int splits,
-                        int *err, cudaStream_t s) {
+                        const agd::ConvGeom &conv, const agd::BiasActOut &act, int *err,
+                        cudaStream_t s) {
   using L = agd::TcGemmSmem<BN>;
   // per function and device; cheap enough to set on every launch
   const cudaError_t e = cudaFuncSetAttribute(
@@ -27,7 +28,7 @@ cudaError_t launch_gemm(const uint16_t *A, const uint16_t *B, float *C, int M, i
   splits = (K + k_split - 1) / k_split;
   const dim3 grid((M + agd::kTcBM - 1) / agd::kTcBM, (N + BN - 1) / BN, std::max(1, splits));
   agd::tc_gemm_bf16<BN><<<grid, 128, L::kBytes, s>>>(A, B, C, M, N, K, lda, ldb, ldc, alpha,
-                                                      beta, k_split, err);
+                                                      beta, k_split, conv, act, err);
   return cudaGetLastError();
 }
 
@@ -41,11 +42,16 @@ namespace agd {
 // added into C with atomics: C must hold beta C already (beta is ignored).
 cudaError_t tc_gemm(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K,
                     int lda, int ldb, int ldc, float alpha, float beta, int *err,
-                    cudaStream_t s, int splits = 1) {
+                    cudaStream_t s, int splits = 1,
+                    const ConvGeom &conv = ConvGeom{nullptr, 0, 0, 0, 0, 0},
+                    const BiasActOut &act = BiasActOut{nullptr, nullptr, 0, 0, 0}) {
   if (M <= 0 || N <= 0) return cudaSuccess;
+  if (conv.x != nullptr || act.y != nullptr) splits = 1;
   if (N <= 64)
-    return launch_gemm<64>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, splits, err, s);
-  return launch_gemm<128>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, splits, err, s);
+    return launch_gemm<64>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, splits, conv, act, err,
+                           s);
+  return launch_gemm<128>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, splits, conv, act, err,
+                          s);
 }
 
 }  // namespace agd
@@ -105,6 +111,7 @@ extern "C" int agd_nn_gemm_bf16(const void *A, const void *B, float *C, int M, i
 #include <string>
 #include <vector>
 
+#include "nn_api.hpp"
 #include "nn_kernels.cuh"
 
 namespace agd {
@@ -301,8 +308,8 @@ class Net {
     return (long)cur_n * (cur_h >> level) * (cur_w >> level);
   }
 
-  // buffers for n images of h x w
-  void shape(int n, int h, int wd) {
+  // buffers for n images of h x w (training: also the backward buffers)
+  void shape(int n, int h, int wd, bool training = true) {
     if (h % 8 || wd % 8 || n <= 0) throw NnError("image sides must be multiples of 8");
     cur_n = n;
     cur_h = h;
@@ -311,19 +318,25 @@ class Net {
     for (Tensor &x : t) {
       const long P = pixels(x.level);
       x.v.ensure((size_t)P * x.Cs);
-      x.g.ensure((size_t)P * x.Cs);
+      if (training) x.g.ensure((size_t)P * x.Cs);
     }
+    size_t col_fwd = 0;  // im2col of the layers that are not implicit GEMMs
     for (const Layer &L : layers) {
       const long P = pixels(t[L.in].level);
       col_max = std::max(col_max, (size_t)P * L.kp);
+      if (L.cin % 8) col_fwd = std::max(col_fwd, (size_t)P * L.kp);
       z_max = std::max(z_max, (size_t)P * L.cout_s);
     }
-    col.ensure(col_max);
-    colT.ensure(col_max);
-    dcol.ensure(col_max);
-    z.ensure(z_max);
-    dz.ensure(z_max);
-    dzT.ensure(z_max);
+    col.ensure(training ? col_max : col_fwd);
+    // FP32 GEMM output: the last layer's in the forward pass (the others go
+    // to BF16 in the GEMM epilogue); any layer's gradient GEMMs in training
+    z.ensure(training ? z_max : (size_t)pixels(0) * layers.back().cout_s);
+    if (training) {
+      colT.ensure(col_max);
+      dcol.ensure(col_max);
+      dz.ensure(z_max);
+      dzT.ensure(z_max);
+    }
     const long P0 = pixels(0);
     in_f.ensure(P0);
     out_f.ensure(P0);
@@ -344,15 +357,28 @@ class Net {
     Tensor &Y = t[L.out];
     const long P = pixels(X.level);
     const int H = cur_h >> X.level, Wd = cur_w >> X.level;
-    im2col3x3<<<grid_of(P * L.kp), kNnThreads, 0, s>>>(X.v.get(), cur_n, H, Wd, L.cin, X.Cs,
-                                                       L.kp, col.get());
-    NCK(cudaGetLastError());
-    gemm(col.get(), wp[&L - layers.data()].get(), z.get(), P, L.cout_s, L.kp, L.kp, L.kp,
-         L.cout_s, 0.f);
-    bias_act<<<grid_of(P * L.cout_s), kNnThreads, 0, s>>>(
-        z.get(), w.get() + L.b_off, P, L.cout, L.cout_s, L.relu, Y.v.get(),
-        keep_f32 ? last_f.get() : nullptr);
-    NCK(cudaGetLastError());
+    if (P > INT32_MAX) throw NnError("GEMM too large");
+    // all but the last layer: bias, activation and the BF16 store in the
+    // GEMM epilogue (the last one keeps its FP32 output for the residual)
+    const BiasActOut act = keep_f32 ? BiasActOut{nullptr, nullptr, 0, 0, 0}
+                                    : BiasActOut{Y.v.get(), w.get() + L.b_off, L.cout,
+                                                 L.cout_s, L.relu};
+    const uint16_t *A = nullptr;
+    ConvGeom geom{X.v.get(), cur_n, H, Wd, L.cin, X.Cs};  // implicit GEMM
+    if (L.cin % 8 != 0) {
+      im2col3x3<<<grid_of(P * L.kp), kNnThreads, 0, s>>>(X.v.get(), cur_n, H, Wd, L.cin, X.Cs,
+                                                         L.kp, col.get());
+      NCK(cudaGetLastError());
+      A = col.get();
+      geom.x = nullptr;
+    }
+    NCK(tc_gemm(A, wp[&L - layers.data()].get(), z.get(), (int)P, L.cout_s, L.kp, L.kp, L.kp,
+                L.cout_s, 1.f, 0.f, err.get(), s, 1, geom, act));
+    if (keep_f32) {
+      bias_act<<<grid_of(P * L.cout_s), kNnThreads, 0, s>>>(
+          z.get(), w.get() + L.b_off, P, L.cout, L.cout_s, L.relu, Y.v.get(), last_f.get());
+      NCK(cudaGetLastError());
+    }
   }
 
   // n images (device fp32 [n][h][w]) -> out_f = input + network correction
@@ -488,6 +514,52 @@ struct agd_nn {
   std::unique_ptr<agd::nn::Net> net;
 };
 
+namespace agd {
+namespace nn {
+
+void estimate_images(agd_nn *handle, float *data, const std::vector<ImageGroup> &groups,
+                     cudaStream_t stream) {
+  Net &nt = *handle->net;
+  // the network's stream follows the caller's and the caller's the network's
+  cudaEvent_t ev = nullptr;
+  NCK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  NCK(cudaEventRecord(ev, stream));
+  NCK(cudaStreamWaitEvent(nt.s, ev, 0));
+  const long max_pixels = 1L << 23;  // images per network pass
+  Buf<float> imgs, rms;
+  Buf<long> bases;
+  for (const ImageGroup &g : groups) {
+    if (g.base.empty()) continue;
+    const int hp = pad8(g.rows), wp = pad8(g.cols);
+    const long per = (long)hp * wp;
+    const int chunk = (int)std::max<long>(1, std::min<long>((long)g.base.size(),
+                                                            max_pixels / per));
+    imgs.ensure((size_t)chunk * per);
+    rms.ensure(chunk);
+    bases.ensure(g.base.size());
+    NCK(cudaMemcpyAsync(bases.get(), g.base.data(), g.base.size() * sizeof(long),
+                        cudaMemcpyHostToDevice, nt.s));
+    for (size_t i0 = 0; i0 < g.base.size(); i0 += chunk) {
+      const int n = (int)std::min<size_t>(chunk, g.base.size() - i0);
+      gather_images<<<n, kNnThreads, 0, nt.s>>>(data, bases.get() + i0, g.rows, g.cols,
+                                                 g.row_stride, hp, wp, imgs.get(), rms.get());
+      NCK(cudaGetLastError());
+      nt.shape(n, hp, wp, false);
+      nt.forward(imgs.get());
+      scatter_images<<<n, kNnThreads, 0, nt.s>>>(nt.out_f.get(), bases.get() + i0, g.rows,
+                                                  g.cols, g.row_stride, hp, wp, rms.get(), data);
+      NCK(cudaGetLastError());
+    }
+  }
+  NCK(cudaEventRecord(ev, nt.s));
+  NCK(cudaStreamWaitEvent(stream, ev, 0));
+  nt.check_errors();  // synchronises the network's stream
+  cudaEventDestroy(ev);
+}
+
+}  // namespace nn
+}  // namespace agd
+
 namespace {
 
 template <typename F>
@@ -546,7 +618,7 @@ int agd_nn_forward(agd_nn *net, const float *input, int n, int h, int w, float *
   if (net == nullptr || input == nullptr || output == nullptr) return 1;
   return nn_guarded("agd_nn_forward", [&] {
     agd::nn::Net &nt = *net->net;
-    nt.shape(n, h, w);
+    nt.shape(n, h, w, false);
     const long P0 = (long)n * h * w;
     agd::nn::NCK(cudaMemcpyAsync(nt.tgt_f.get(), input, P0 * sizeof(float),
                                  cudaMemcpyHostToDevice, nt.s));

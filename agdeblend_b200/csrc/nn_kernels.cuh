@@ -324,5 +324,51 @@ __global__ void axpy1(const float *__restrict__ x, long n, float *__restrict__ y
     y[i] += x[i];
 }
 
+
+// Images of an ImageGroup (nn_api.hpp) gathered into [n][hp][wp] (zero
+// padding), and their RMS over the real rows x cols samples: one block per
+// image; the image is divided by its RMS (1 for a zero image) and the RMS
+// kept for scatter_images.
+__global__ void gather_images(const float *__restrict__ data, const long *__restrict__ base,
+                              int rows, int cols, long row_stride, int hp, int wp,
+                              float *__restrict__ out, float *__restrict__ rms) {
+  const int i = blockIdx.x;
+  const float *src = data + base[i];
+  float *dst = out + (long)i * hp * wp;
+  float s = 0.f;
+  for (long e = threadIdx.x; e < (long)hp * wp; e += blockDim.x) {
+    const int r = (int)(e / wp), c = (int)(e - (long)r * wp);
+    const float v = (r < rows && c < cols) ? src[(long)r * row_stride + c] : 0.f;
+    dst[e] = v;
+    s += v * v;
+  }
+  __shared__ float red[kNnThreads];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  const float rm = sqrtf(red[0] / (float)((long)rows * cols));
+  const float r = rm > 0.f ? rm : 1.f;
+  const float inv = 1.f / r;
+  for (long e = threadIdx.x; e < (long)hp * wp; e += blockDim.x) dst[e] *= inv;
+  if (threadIdx.x == 0) rms[i] = r;
+}
+
+// data[image i, row r, col c] = est[i][r][c] * rms[i] (real rows and cols)
+__global__ void scatter_images(const float *__restrict__ est, const long *__restrict__ base,
+                               int rows, int cols, long row_stride, int hp, int wp,
+                               const float *__restrict__ rms, float *__restrict__ data) {
+  const int i = blockIdx.x;
+  float *dst = data + base[i];
+  const float *src = est + (long)i * hp * wp;
+  const float r = rms[i];
+  for (long e = threadIdx.x; e < (long)rows * cols; e += blockDim.x) {
+    const int rr = (int)(e / cols), c = (int)(e - (long)rr * cols);
+    dst[(long)rr * row_stride + c] = src[(long)rr * wp + c] * r;
+  }
+}
+
 }  // namespace nn
 }  // namespace agd

@@ -58,12 +58,55 @@ __device__ __forceinline__ void tc_load_tile(uint32_t sbase, const uint16_t *g, 
   }
 }
 
+// Implicit GEMM of a 3 x 3, padding 1 convolution: A[p][k] is read straight
+// from NHWC BF16 activations x (n, h, w, channel stride cs) - row p a pixel,
+// k = (ky * 3 + kx) * cin + ci - instead of from an im2col matrix.  Needs cin
+// and cs multiples of 8 (a 16-byte chunk holds 8 channels of one tap).
+struct ConvGeom {
+  const uint16_t *x;  // nullptr: A is a plain matrix
+  int n, h, w, cin, cs;
+};
+
+// Epilogue that writes BF16 activations instead of FP32 C: y[m][n] =
+// bf16(act(acc + bias[n])) for n < n_real (ReLU when relu), 0 for the padded
+// columns n_real <= n < N; y rows ldy apart.
+struct BiasActOut {
+  uint16_t *y;  // nullptr: the FP32 epilogue
+  const float *bias;
+  int n_real, ldy, relu;
+};
+
+template <int ROWS>
+__device__ __forceinline__ void tc_load_conv_tile(uint32_t sbase, const ConvGeom &g, int n_rows,
+                                                  int K, int r0, int k0) {
+  constexpr int kChunks = ROWS * (kTcBK / 8);
+  for (int q = threadIdx.x; q < kChunks; q += blockDim.x) {
+    const int row = q >> 3, c = q & 7;
+    const int p = r0 + row, k = k0 + 8 * c;
+    bool valid = p < n_rows && k < K;
+    const uint16_t *src = g.x;
+    if (valid) {
+      const int tap = k / g.cin, ci = k - tap * g.cin;
+      const int ky = tap / 3, kx = tap - 3 * ky;
+      const int xx = p % g.w, t = p / g.w;
+      const int yy = t % g.h, n = t / g.h;
+      const int sy = yy + ky - 1, sx = xx + kx - 1;
+      valid = sy >= 0 && sy < g.h && sx >= 0 && sx < g.w;
+      if (valid) src = g.x + ((long)(n * g.h + sy) * g.w + sx) * g.cs + ci;
+    }
+    const uint32_t dst = sbase + (uint32_t)(row >> 3) * kTcSbo + (uint32_t)c * kTcLbo +
+                         (uint32_t)(row & 7) * 16u;
+    cp_async16_zfill(dst, src, valid);
+  }
+}
+
 template <int BN>
 __global__ void __launch_bounds__(128) tc_gemm_bf16(const uint16_t *__restrict__ A,
                                                     const uint16_t *__restrict__ B,
                                                     float *__restrict__ C, int M, int N, int K,
                                                     int lda, int ldb, int ldc, float alpha,
-                                                    float beta, int k_split, int *err) {
+                                                    float beta, int k_split, ConvGeom conv,
+                                                    BiasActOut act, int *err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   using L = TcGemmSmem<BN>;
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * L::kStage);
@@ -88,15 +131,22 @@ __global__ void __launch_bounds__(128) tc_gemm_bf16(const uint16_t *__restrict__
   // this CTA's K range (split K: a slice of k_split, a multiple of kTcBK)
   const int kz0 = gridDim.z > 1 ? blockIdx.z * k_split : 0;
   const int kz1 = gridDim.z > 1 ? min(K, kz0 + k_split) : K;
+  // (implicit convolutions are not split: kz0 = 0 for them)
   A += kz0;
   B += kz0;
   K = kz1 > kz0 ? kz1 - kz0 : 0;
+  auto load_a = [&](uint32_t sbase, int k0) {
+    if (conv.x != nullptr)
+      tc_load_conv_tile<kTcBM>(sbase, conv, M, K, m0, k0);
+    else
+      tc_load_tile<kTcBM>(sbase, A, M, K, lda, m0, k0);
+  };
   const bool split = gridDim.z > 1;
   const int nk = (K + kTcBK - 1) / kTcBK;
   bool ok = true;
   auto stage_a = [&](int s) { return s0 + (uint32_t)s * L::kStage; };
   auto stage_b = [&](int s) { return s0 + (uint32_t)s * L::kStage + L::kABytes; };
-  tc_load_tile<kTcBM>(stage_a(0), A, M, K, lda, m0, 0);
+  load_a(stage_a(0), 0);
   tc_load_tile<BN>(stage_b(0), B, N, K, ldb, n0, 0);
   asm volatile("cp.async.commit_group;" ::: "memory");
   for (int kt = 0; kt < nk && ok; ++kt) {
@@ -105,7 +155,7 @@ __global__ void __launch_bounds__(128) tc_gemm_bf16(const uint16_t *__restrict__
       // stage s^1 was read by the MMAs of step kt - 1
       if (kt >= 1) ok = umma::bar_wait(&bars[s ^ 1], ((kt - 1) >> 1) & 1);
       if (ok) {
-        tc_load_tile<kTcBM>(stage_a(s ^ 1), A, M, K, lda, m0, (kt + 1) * kTcBK);
+        load_a(stage_a(s ^ 1), (kt + 1) * kTcBK);
         tc_load_tile<BN>(stage_b(s ^ 1), B, N, K, ldb, n0, (kt + 1) * kTcBK);
       }
       asm volatile("cp.async.commit_group;" ::: "memory");
@@ -145,7 +195,31 @@ __global__ void __launch_bounds__(128) tc_gemm_bf16(const uint16_t *__restrict__
 #pragma unroll
         for (int i = 0; i < 16; ++i) v[i] = 0.f;
       }
-      if (row < M) {
+      if (row < M && act.y != nullptr) {
+        uint32_t packed[8];
+#pragma unroll
+        for (int i = 0; i < 16; i += 2) {
+          const int n = n0 + cc * 16 + i;
+          float a = n < act.n_real ? v[i] + act.bias[n] : 0.f;
+          float b = n + 1 < act.n_real ? v[i + 1] + act.bias[n + 1] : 0.f;
+          if (act.relu) {
+            a = fmaxf(a, 0.f);
+            b = fmaxf(b, 0.f);
+          }
+          const __nv_bfloat162 h2 = __floats2bfloat162_rn(a, b);
+          packed[i / 2] = *reinterpret_cast<const uint32_t *>(&h2);
+        }
+        uint16_t *y = act.y + (long)row * act.ldy + n0 + cc * 16;
+        if (n0 + cc * 16 + 16 <= N) {  // 16 columns: two 16-byte stores
+          reinterpret_cast<uint4 *>(y)[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+          reinterpret_cast<uint4 *>(y)[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            if (n0 + cc * 16 + i < N)
+              y[i] = (uint16_t)(packed[i / 2] >> (16 * (i & 1)));
+        }
+      } else if (row < M) {
         float *c = C + (long)row * ldc + n0 + cc * 16;
         if (split) {
 #pragma unroll

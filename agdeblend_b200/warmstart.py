@@ -1,0 +1,218 @@
+"""Learned warm start of the deblending solver.
+
+The network (agdeblend_b200.nn.WarmStartNet, a convolutional encoder-decoder
+run on the tensor cores) maps 2-D gathers of pseudo-deblended data (traces x
+time samples, each normalised by its RMS) to an estimate of the deblended
+data.  The solver then starts from the model that reproduces that estimate
+(agd_gpu_solve_warm) and runs only the tail of the plain method's threshold
+schedule.  The plain method is unchanged and stays the judge: the warm
+start only changes where its iterations begin.
+
+Training pairs are made by the plain method itself: seeded synthetic 2-D
+receiver gathers (agdeblend_b200.synthetic.gather_2d, 128 shots x 512
+samples, base seed 4000) deblended by the GPU solver, cut into 32 x 256
+windows of (pseudo-deblended input, deblended output).
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_int
+
+import numpy as np
+
+from . import capi, load_library
+from . import synthetic as S
+from .nn import WarmStartNet
+
+TRAIN_SEED = 4000
+
+
+def trace_axis(shape, shottimes) -> int:
+    """The space axis of a patch along which shot times change least (but
+    change): its lines are receiver gathers of consecutive shots, where the
+    blending noise is incoherent."""
+    st = np.asarray(shottimes, np.float64).reshape(shape[:-1])
+    best, best_d = len(shape) - 2, np.inf
+    for ax in range(len(shape) - 1):
+        if shape[ax] < 2:
+            continue
+        d = float(np.mean(np.abs(np.diff(st, axis=ax))))
+        if 0 < d < best_d:
+            best, best_d = ax, d
+    return best
+
+
+def to_images(patch, axis):
+    """(images [n][traces][time], restore) of one patch: every line along
+    `axis` becomes one image."""
+    a = np.moveaxis(np.asarray(patch, np.float32), axis, -2)
+    lead = a.shape[:-2]
+    imgs = a.reshape(-1, a.shape[-2], a.shape[-1])
+
+    def restore(out):
+        return np.moveaxis(out.reshape(lead + out.shape[-2:]), -2, axis)
+
+    return imgs, restore
+
+
+def _pad8(n):
+    return (n + 7) // 8 * 8
+
+
+def infer(net: WarmStartNet, images, max_pixels: int = 1 << 23):
+    """Network estimate of each image, RMS-normalised in and out; sides
+    zero-padded to multiples of 8."""
+    imgs = np.asarray(images, np.float32)
+    n, h, w = imgs.shape
+    rms = np.sqrt(np.mean(imgs.astype(np.float64) ** 2, axis=(1, 2)))
+    rms[rms == 0] = 1.0
+    hp, wp = _pad8(h), _pad8(w)
+    x = np.zeros((n, hp, wp), np.float32)
+    x[:, :h, :w] = imgs / rms[:, None, None]
+    out = np.empty_like(x)
+    step = max(1, max_pixels // (hp * wp))
+    for i in range(0, n, step):
+        out[i: i + step] = net.forward(x[i: i + step])
+    return out[:, :h, :w] * rms[:, None, None].astype(np.float32)
+
+
+def estimate(net: WarmStartNet, sv):
+    """Network estimate of the deblended data of every patch of a survey."""
+    est = []
+    for d, st in zip(sv.data, sv.shottimes):
+        ax = trace_axis(d.shape, st)
+        imgs, restore = to_images(d, ax)
+        est.append(restore(infer(net, imgs)).astype(np.float32))
+    return est
+
+
+def training_set(n_gathers: int = 2000, crops: int = 8, n_its: int = 100, seed: int = TRAIN_SEED,
+                 batch: int = 100):
+    """(inputs, targets) of n_gathers * crops windows of 32 x 256: seeded
+    128 x 512 gathers (gather_2d, seeds seed + i) blended in sum mode, read
+    back at their shot times (the pseudo-deblended input), and deblended by
+    the plain method on the GPU (n_its iterations, windows (32, 256)); both
+    normalised by the input gather's RMS."""
+    from . import deblend_batch
+
+    rng = np.random.default_rng(seed)
+    xs, ts = [], []
+    for g0 in range(0, n_gathers, batch):
+        gathers = [S.gather_2d(seed=seed + g, n_shots=128, nt=512, window=(32, 256),
+                               n_its=n_its) for g in range(g0, min(n_gathers, g0 + batch))]
+        outs = deblend_batch([dict(volumes=g.volumes, window_shapes=g.window_shapes,
+                                   coords=g.coords, shottimes=g.shottimes, channels=g.channels,
+                                   trace_types=g.trace_types, data=g.data) for g in gathers],
+                             1.0, n_its)
+        for g, o in zip(gathers, outs):
+            x = g.data[0].astype(np.float32)
+            y = np.asarray(o[0], np.float32)
+            rms = float(np.sqrt(np.mean(x.astype(np.float64) ** 2))) or 1.0
+            for _ in range(crops):
+                i0 = int(rng.integers(0, x.shape[0] - 32 + 1))
+                j0 = int(rng.integers(0, x.shape[1] - 256 + 1))
+                xs.append(x[i0: i0 + 32, j0: j0 + 256] / rms)
+                ts.append(y[i0: i0 + 32, j0: j0 + 256] / rms)
+    return np.stack(xs), np.stack(ts)
+
+
+def training_set_vibroseis(n_surveys: int = 40, crops: int = 1, n_its: int = 150,
+                           seed: int = TRAIN_SEED):
+    """(inputs, targets) of 32 x 256 windows of receiver gathers from seeded
+    small vibroseis surveys (vibroseis_4d with seeds seed + i: 16 sY x 32 sX
+    x 16 channels x 2048 samples, the 256-sample 8-80 Hz sweep, windows
+    (16, 16, 16, 256)) deblended by the plain method on the GPU; every line
+    along sX (32 shots x 2048 samples) gives `crops` windows, normalised by
+    the line's RMS."""
+    from . import Problem
+
+    rng = np.random.default_rng(seed + 100000)
+    xs, ts = [], []
+    for i in range(n_surveys):
+        sv = S.vibroseis_4d(seed=seed + i, n_sy=16, n_sx=32, n_ch=16, nt=2048,
+                            window=(16, 16, 16, 256), n_its=n_its)
+        p = Problem.from_survey(sv)
+        out = p.solve(sv.data, 1.0, n_its)
+        p.close()
+        x = np.moveaxis(sv.data[0], 1, 2).reshape(-1, 32, 2048)  # (sY, ch) lines along sX
+        y = np.moveaxis(np.asarray(out[0], np.float32), 1, 2).reshape(-1, 32, 2048)
+        for xi, yi in zip(x, y):
+            rms = float(np.sqrt(np.mean(xi.astype(np.float64) ** 2))) or 1.0
+            for _ in range(crops):
+                j0 = int(rng.integers(0, 2048 - 256 + 1))
+                xs.append(xi[:, j0: j0 + 256] / rms)
+                ts.append(yi[:, j0: j0 + 256] / rms)
+    return np.stack(xs).astype(np.float32), np.stack(ts).astype(np.float32)
+
+
+def train(family: str = "gather_2d", n: int = 2000, epochs: int = 8, batch: int = 32,
+          lr: float = 1e-3, base_channels: int = 32, seed: int = 0):
+    """A network trained on the plain method's own results: family
+    "gather_2d" (n receiver gathers, training_set) or "vibroseis" (n small
+    surveys, training_set_vibroseis).  Returns (net, per-epoch mean loss)."""
+    if family == "vibroseis":
+        x, t = training_set_vibroseis(n)
+    else:
+        x, t = training_set(n)
+    net = WarmStartNet(base_channels, seed=seed)
+    losses = net.train(x, t, batch=batch, epochs=epochs, lr=lr, seed=seed)
+    return net, losses
+
+
+def _bind_warm(lib, dtype):
+    if getattr(lib, "_agd_warm_bound", False):
+        return
+    rc = capi.real_ctype(dtype)
+    rp = POINTER(rc)
+    lib.agd_gpu_solve_warm.argtypes = [ctypes.c_void_p, rc, c_int, c_int, c_int, POINTER(rp),
+                                       POINTER(rp)]
+    lib.agd_gpu_solve_warm.restype = c_int
+    lib.agd_gpu_warm_model.argtypes = [ctypes.c_void_p, POINTER(rp), rp]
+    lib.agd_gpu_warm_model.restype = c_int
+    lib._agd_warm_bound = True
+
+
+def solve_warm(problem, data, estimate_patches, initial_factor: float, n_its: int,
+               it_begin: int, print_freq: int = 0):
+    """agd_gpu_solve_warm on a planned problem (agdeblend_b200.Problem):
+    iterations [it_begin, n_its) of the plain schedule from the warm model
+    of the estimate.  Returns the deblended patches."""
+    lib = problem.lib
+    _bind_warm(lib, problem.dtype)
+    ptrs, keep = problem._data_ptrs(data, writable=True)
+    eptrs, ekeep = problem._data_ptrs(estimate_patches)
+    if lib.agd_gpu_solve_warm(problem.h, initial_factor, n_its, it_begin, print_freq, eptrs,
+                              ptrs):
+        raise RuntimeError("agd_gpu_solve_warm failed")
+    return [k.reshape(s) for k, s in zip(keep, problem.shapes)]
+
+
+def warm_model(problem, estimate_patches) -> np.ndarray:
+    """The model (interleaved re, im) whose operator reproduces the estimate."""
+    lib = problem.lib
+    _bind_warm(lib, problem.dtype)
+    eptrs, ekeep = problem._data_ptrs(estimate_patches)
+    out = np.zeros(2 * problem.model_size, problem.dtype)
+    if lib.agd_gpu_warm_model(problem.h, eptrs, out.ctypes.data_as(problem._rp)):
+        raise RuntimeError("agd_gpu_warm_model failed")
+    return out
+
+
+def solve_learned(problem, net: WarmStartNet, data, initial_factor: float, n_its: int,
+                  it_begin: int, print_freq: int = 0):
+    """agd_gpu_solve_learned: the network's estimate of the deblended data
+    (computed on the device from the uploaded input) as the warm start,
+    then iterations [it_begin, n_its) of the plain schedule."""
+    lib = problem.lib
+    _bind_warm(lib, problem.dtype)
+    if not getattr(lib, "_agd_learned_bound", False):
+        rc = capi.real_ctype(problem.dtype)
+        lib.agd_gpu_solve_learned.argtypes = [ctypes.c_void_p, ctypes.c_void_p, rc, c_int, c_int,
+                                              c_int, POINTER(POINTER(rc))]
+        lib.agd_gpu_solve_learned.restype = c_int
+        lib._agd_learned_bound = True
+    ptrs, keep = problem._data_ptrs(data, writable=True)
+    if lib.agd_gpu_solve_learned(problem.h, net.h, initial_factor, n_its, it_begin, print_freq,
+                                 ptrs):
+        raise RuntimeError("agd_gpu_solve_learned failed")
+    return [k.reshape(s) for k, s in zip(keep, problem.shapes)]

@@ -603,6 +603,104 @@ def measure_batch(args, name, rank, world, local):
     return line
 
 
+# Time to SNR (the learned warm start): per benchmark survey, the network
+# family it is trained on, the training size, the survey, a held-out
+# validation survey of the same family (other seed) and the grid of
+# iterations at which the warm-started schedule may begin.
+TIME_TO_SNR = {
+    "vibroseis_4d": ("vibroseis", 30, 12, lambda S: S.vibroseis_4d(seed=1002),
+                     lambda S: S.vibroseis_4d(seed=4999), (140, 130, 120, 110, 100, 90, 75, 50)),
+    "two_volume_3d": ("gather_2d", 2000, 8, lambda S: S.two_volume_3d(),
+                      lambda S: S.two_volume_3d(seed=4998), (195, 190, 180, 160, 140, 120, 100)),
+}
+
+
+def timed(f):
+    import torch
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = f()
+    torch.cuda.synchronize()
+    return r, time.perf_counter() - t0
+
+
+def measure_time_to_snr(name):
+    """Wall time of one public-API solve on host data (agd_gpu_solve for the
+    plain method; agd_gpu_solve_learned - network estimate on the device,
+    warm model, the tail of the same threshold schedule - for the learned
+    start) until the deblended SNR against the known truth reaches the
+    plain method's own final SNR minus 0.1 dB.  The iteration at which the
+    learned schedule begins is the latest one of the grid that reaches the
+    plain method's SNR (-0.1 dB) on the validation survey; it is then used
+    unchanged on the benchmark survey.  Median of three calls each."""
+    import agdeblend_b200 as A
+    from agdeblend_b200 import synthetic as S
+    from agdeblend_b200 import warmstart as WS
+
+    family, n_train, epochs, make, make_val, grid = TIME_TO_SNR[name]
+    (net, losses), t_train = timed(lambda: WS.train(family, n_train, epochs=epochs))
+
+    def snr(out, sv):
+        return S.snr_db(out, sv.truth, sv.trace_types)
+
+    # the schedule's start, chosen on the validation survey
+    val = make_val(S)
+    p = A.Problem.from_survey(val)
+    target_val = snr(p.solve(val.data, val.initial_factor, val.n_its), val) - 0.1
+    k_pick, val_curve = grid[-1], {}
+    for k in grid:  # latest start first: fewest iterations
+        val_curve[k] = snr(WS.solve_learned(p, net, val.data, val.initial_factor, val.n_its, k),
+                           val)
+        if val_curve[k] >= target_val:
+            k_pick = k
+            break
+    p.close()
+
+    sv = make(S)
+    p = A.Problem.from_survey(sv)
+    p.solve(sv.data, sv.initial_factor, 2)  # warm-up: device arrays, graphs
+    WS.solve_learned(p, net, sv.data, sv.initial_factor, sv.n_its, sv.n_its)
+
+    def median_call(f):
+        runs = [timed(f) for _ in range(3)]
+        return runs[-1][0], float(np.median([r[1] for r in runs]))
+
+    plain, t_plain = median_call(lambda: p.solve(sv.data, sv.initial_factor, sv.n_its))
+    target = snr(plain, sv) - 0.1
+    learned, t_learned = median_call(
+        lambda: WS.solve_learned(p, net, sv.data, sv.initial_factor, sv.n_its, k_pick))
+    res = {"metric": "seconds to the plain method's deblended SNR - 0.1 dB (one solve, host "
+                     "data in and out)", "unit": "s", "higher_is_better": False,
+           "survey": name, "target_snr_db": target,
+           "plain_fp32": {"seconds": t_plain, "iterations": sv.n_its - 1,
+                          "snr_db": snr(plain, sv)},
+           "learned_fp32": {"seconds": t_learned, "iterations": sv.n_its - k_pick,
+                            "it_begin": k_pick, "snr_db": snr(learned, sv),
+                            "reached": snr(learned, sv) >= target},
+           "speedup_learned_fp32": t_plain / t_learned,
+           "network": {"family": family, "training": n_train, "epochs": epochs,
+                       "loss_first_last": [float(losses[0]), float(losses[-1])],
+                       "train_seconds": t_train},
+           "validation": {"target_snr_db": target_val,
+                          "snr_db_by_it_begin": {str(k): v for k, v in val_curve.items()}}}
+    if name == "vibroseis_4d":
+        # the precision variant: split-BF16 tensor-core space DFTs as well
+        n_tc = p.set_precision(1)
+        p.solve(sv.data, sv.initial_factor, 2)
+        lb, t_lb = median_call(
+            lambda: WS.solve_learned(p, net, sv.data, sv.initial_factor, sv.n_its, k_pick))
+        pb, t_pb = median_call(lambda: p.solve(sv.data, sv.initial_factor, sv.n_its))
+        res["learned_split_bf16"] = {"seconds": t_lb, "iterations": sv.n_its - k_pick,
+                                     "snr_db": snr(lb, sv), "reached": snr(lb, sv) >= target,
+                                     "tc_windows": n_tc}
+        res["plain_split_bf16"] = {"seconds": t_pb, "snr_db": snr(pb, sv)}
+        res["speedup_learned_split_bf16"] = t_plain / t_lb
+    p.close()
+    net.close()
+    return res
+
+
 SUMMARY_KEYS = ("metric", "value", "unit", "ms_per_step", "config", "clocks", "e2e",
                 "gpu_launches", "roofline", "cpu_baseline", "per_gather_loop")
 
@@ -622,6 +720,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1],
                     help="1: split-BF16 tensor-core space DFTs (agd_gpu_problem_set_precision)")
+    ap.add_argument("--no-time-to-snr", action="store_true",
+                    help="skip the learned warm-start time-to-SNR measurements")
+    ap.add_argument("--time-to-snr-only", action="store_true",
+                    help="only the time-to-SNR measurements (one JSON line)")
     ap.add_argument("--no-workloads", action="store_true",
                     help="only the headline workload (no vibroseis_4d / uneven_gathers entries)")
     ap.add_argument("--workload", default="two_volume_3d",
@@ -631,6 +733,9 @@ def main():
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         run_reference(args, rank, int(os.environ.get("WORLD_SIZE", "1")))
+        return
+    if args.time_to_snr_only:
+        print(json.dumps({n: measure_time_to_snr(n) for n in TIME_TO_SNR}), flush=True)
         return
     rank, world, local = dist_setup(args.gpus)
     try:
@@ -648,6 +753,8 @@ def main():
                 "uneven_gathers": workload_summary(
                     measure_batch(args, "uneven_gathers", rank, world, local)),
             }
+            if not args.no_time_to_snr:
+                line["time_to_snr"] = {n: measure_time_to_snr(n) for n in TIME_TO_SNR}
         if line is not None:
             print(json.dumps(line), flush=True)
     finally:

@@ -225,6 +225,35 @@ int agd_gpu_problem_set_precision(agd_gpu_problem *problem, int precision,
 int agd_nn_gemm_bf16(const void *A, const void *B, float *C, int M, int N, int K, int lda,
                      int ldb, int ldc, float alpha, float beta, void *stream);
 
+/* Warm start (no counterpart in the reference, whose solver starts from a
+ * zero model, src/model.c:1160-1185, and whose threshold schedule starts at
+ * the largest coefficient of the first adjoint, src/agdeblend.c:526-589).
+ * `estimate` is an estimate of the deblended data (patch layout as `data`).
+ * agd_gpu_warm_model writes the model x0 whose FK (and wavelet) operator
+ * reproduces the estimate on the live traces' samples (layout as
+ * agd_gpu_forward).  agd_gpu_solve_warm runs agd_gpu_solve's initial step
+ * and threshold schedule from the blended input `data`, replaces the model
+ * by the warm model of `estimate`, and runs iterations [it_begin, n_its) of
+ * that schedule (1 <= it_begin <= n_its): the thresholds start at the
+ * schedule's level for iteration it_begin instead of the largest
+ * coefficient.  `data` receives the deblended output. */
+int agd_gpu_warm_model(agd_gpu_problem *problem, AGD_TYPE const *const *estimate,
+                       AGD_TYPE *model);
+int agd_gpu_solve_warm(agd_gpu_problem *problem, AGD_TYPE initial_factor, int n_its,
+                       int it_begin, int print_freq, AGD_TYPE const *const *estimate,
+                       AGD_TYPE *const *data);
+
+typedef struct agd_nn agd_nn;
+
+/* agd_gpu_solve_warm with the network's estimate: `data` (blended input,
+ * receives the output) is cut on the device into 2-D images - every line of
+ * a patch along the space axis whose shot times change least (receiver
+ * gathers of consecutive shots) x the time samples - each normalised by its
+ * RMS, run through `net`, scaled back, and used as the estimate.  Float
+ * library only. */
+int agd_gpu_solve_learned(agd_gpu_problem *problem, agd_nn *net, AGD_TYPE initial_factor,
+                          int n_its, int it_begin, int print_freq, AGD_TYPE *const *data);
+
 /* The warm-start network: a 4-level 2-D convolutional encoder-decoder on
  * images of n x h x w samples (traces x time; h, w multiples of 8), base
  * channels c (32: 1,162,945 parameters), output = input + a learned
@@ -233,7 +262,6 @@ int agd_nn_gemm_bf16(const void *A, const void *B, float *C, int M, int N, int K
  * are host memory, [n][h][w] row-major float.  Parameter layout: per layer
  * (encoder, bottleneck, decoder order) the weights [cout][3][3][cin] then
  * the biases [cout]. */
-typedef struct agd_nn agd_nn;
 int agd_nn_create(int base_channels, unsigned seed, agd_nn **net);
 void agd_nn_destroy(agd_nn *net);
 long agd_nn_param_count(const agd_nn *net);

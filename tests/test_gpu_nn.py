@@ -4,9 +4,12 @@ feeds its tensor cores, and whose backpropagation is itself checked against
 finite differences): output, loss and every parameter gradient on small
 shapes; then a short training run lowers the loss.
 
-Tolerances: output and loss 1e-3 relative, gradient vector 2e-2 relative L2
-with cosine similarity above 0.999 (BF16 operands: a sum that lands on the
-other side of a BF16 rounding boundary moves a value by 2^-8)."""
+Tolerances: for base 4 and 8 channels (sums of at most 576 products) output,
+loss and gradient within 1e-5 relative: only the FP32 summation order
+differs.  For the full network (base 32, sums of up to 2304 products) a sum
+that lands on the other side of a BF16 rounding boundary moves a value by
+2^-8, and such moves compound over the 14 layers: output and loss within
+2e-2, gradient within 5e-2 relative L2 with cosine similarity above 0.999."""
 import numpy as np
 import pytest
 
@@ -29,14 +32,17 @@ def test_forward_and_gradients_match_oracle(base, n, h, w):
     t = (x + 0.5 * rng.standard_normal(x.shape)).astype(np.float32)
     ora = N.Net(base, p.astype(np.float64), bf16_like_gpu=True)
     loss_o, g_o = ora.loss_grad(x.astype(np.float64), t.astype(np.float64))
+    tol_out, tol_grad = (1e-5, 1e-5) if base <= 8 else (2e-2, 5e-2)
     y = net.forward(x)
-    assert rel_l2(y, ora.out) <= 1e-3
+    err_out = rel_l2(y, ora.out)
     loss, g = net.loss_grad(x, t)
-    assert abs(loss - loss_o) <= 1e-3 * loss_o
     err = rel_l2(g, g_o)
     cos = float(np.dot(g.astype(np.float64), g_o) / np.linalg.norm(g) / np.linalg.norm(g_o))
-    print(f"base {base}: gradient rel L2 {err:.2e}, cosine {cos:.6f}")
-    assert err <= 2e-2 and cos >= 0.999
+    print(f"base {base}: output rel L2 {err_out:.2e}, loss {loss:.6e} vs {loss_o:.6e}, "
+          f"gradient rel L2 {err:.2e}, cosine {cos:.6f}")
+    assert err_out <= tol_out
+    assert abs(loss - loss_o) <= tol_out * loss_o
+    assert err <= tol_grad and cos >= 0.999
     net.close()
 
 

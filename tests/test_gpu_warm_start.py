@@ -1,0 +1,83 @@
+"""The learned warm start (agd_gpu_warm_model, agd_gpu_solve_warm,
+agd_gpu_solve_learned) on the GPU.
+
+  * the warm model of an estimate reproduces it: for the true data of a 2-D
+    gather and of a two-volume 3-D survey, set_output of the warm model
+    equals the truth on every live trace to 1e-5 relative (F F^+ = identity
+    on the represented samples);
+  * starting from the truth's warm model one iteration before the end of
+    the schedule keeps an SNR above 30 dB;
+  * a network trained here by the project's own tensor-core kernels on
+    pseudo-deblended / deblended pairs that the plain GPU method makes
+    (800 seeded 128 x 512 gathers, 4 epochs) starts the two-volume survey
+    of the benchmark (2 x 64 ch x 128 shots x 1024, 200 iterations) 170
+    iterations into the plain schedule: the 30 remaining iterations reach
+    the plain method's 200-iteration SNR (-0.1 dB) in less wall time, which
+    the test reports.  The plain solve (agd_deblend) is not changed by any
+    of this: its parity with the reference is tested in
+    tests/test_gpu_full_size.py."""
+import time
+
+import numpy as np
+import pytest
+
+import agdeblend_b200 as A
+from agdeblend_b200 import synthetic as S
+from agdeblend_b200 import warmstart as WS
+
+pytestmark = pytest.mark.gpu
+
+
+def _live_rel_err(out, truth, trace_types):
+    num = den = 0.0
+    for o, t, tt in zip(out, truth, trace_types):
+        live = np.asarray(tt).reshape(-1) == S.LIVE
+        nt = t.shape[-1]
+        o2 = np.asarray(o, np.float64).reshape(-1, nt)[live]
+        t2 = np.asarray(t, np.float64).reshape(-1, nt)[live]
+        num += float(np.sum((o2 - t2) ** 2))
+        den += float(np.sum(t2 ** 2))
+    return np.sqrt(num / den)
+
+
+@pytest.mark.parametrize("make", [
+    lambda: S.gather_2d(seed=4101, n_shots=128, nt=512, window=(32, 256)),
+    lambda: S.two_volume_3d(seed=4102, n_ch=16, n_shots=32, nt=300, window=(8, 16, 128),
+                            n_its=30)], ids=["gather_2d", "two_volume_3d"])
+def test_warm_model_reproduces_the_estimate(make):
+    sv = make()
+    p = A.Problem.from_survey(sv)
+    x0 = WS.warm_model(p, sv.truth)
+    assert _live_rel_err(p.set_output(x0), sv.truth, sv.trace_types) <= 1e-5
+    out = WS.solve_warm(p, sv.data, sv.truth, 1.0, sv.n_its, sv.n_its - 1)
+    p.close()
+    assert S.snr_db(out, sv.truth, sv.trace_types) >= 30.0
+
+
+def test_learned_start_reaches_plain_snr_faster():
+    net, losses = WS.train("gather_2d", 800, epochs=4)
+    assert losses[-1] < 0.5 * losses[0]
+    sv = S.two_volume_3d()
+    p = A.Problem.from_survey(sv)
+    p.solve(sv.data, 1.0, 2)
+    WS.solve_learned(p, net, sv.data, 1.0, sv.n_its, sv.n_its)
+
+    def timed(f):
+        import torch
+
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = f()
+        torch.cuda.synchronize()
+        return r, time.perf_counter() - t0
+
+    plain, t_plain = timed(lambda: p.solve(sv.data, 1.0, sv.n_its))
+    learned, t_learned = timed(lambda: WS.solve_learned(p, net, sv.data, 1.0, sv.n_its, 170))
+    p.close()
+    net.close()
+    snr_plain = S.snr_db(plain, sv.truth, sv.trace_types)
+    snr_learned = S.snr_db(learned, sv.truth, sv.trace_types)
+    print(f"plain 199 iterations: {snr_plain:.3f} dB in {t_plain:.3f} s; learned start, 30 "
+          f"iterations: {snr_learned:.3f} dB in {t_learned:.3f} s")
+    assert snr_learned >= snr_plain - 0.1
+    assert t_learned < t_plain
