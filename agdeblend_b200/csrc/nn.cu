@@ -2,6 +2,7 @@
 // and their C entry points.  No counterpart in the reference, whose solver
 // always starts from a zero model (src/model.c:1160-1185).
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cstdio>
@@ -47,6 +48,9 @@ cudaError_t tc_gemm(const uint16_t *A, const uint16_t *B, float *C, int M, int N
                     const BiasActOut &act = BiasActOut{nullptr, nullptr, 0, 0, 0}) {
   if (M <= 0 || N <= 0) return cudaSuccess;
   if (conv.x != nullptr || act.y != nullptr) splits = 1;
+  if (N <= 32)
+    return launch_gemm<32>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, splits, conv, act, err,
+                           s);
   if (N <= 64)
     return launch_gemm<64>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, splits, conv, act, err,
                            s);
@@ -519,6 +523,7 @@ namespace nn {
 
 void estimate_images(agd_nn *handle, float *data, const std::vector<ImageGroup> &groups,
                      cudaStream_t stream) {
+  nvtxRangePushA("agd network estimate");
   Net &nt = *handle->net;
   // the network's stream follows the caller's and the caller's the network's
   cudaEvent_t ev = nullptr;
@@ -555,6 +560,7 @@ void estimate_images(agd_nn *handle, float *data, const std::vector<ImageGroup> 
   NCK(cudaStreamWaitEvent(stream, ev, 0));
   nt.check_errors();  // synchronises the network's stream
   cudaEventDestroy(ev);
+  nvtxRangePop();
 }
 
 }  // namespace nn

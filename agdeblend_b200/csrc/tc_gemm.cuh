@@ -76,30 +76,6 @@ struct BiasActOut {
   int n_real, ldy, relu;
 };
 
-template <int ROWS>
-__device__ __forceinline__ void tc_load_conv_tile(uint32_t sbase, const ConvGeom &g, int n_rows,
-                                                  int K, int r0, int k0) {
-  constexpr int kChunks = ROWS * (kTcBK / 8);
-  for (int q = threadIdx.x; q < kChunks; q += blockDim.x) {
-    const int row = q >> 3, c = q & 7;
-    const int p = r0 + row, k = k0 + 8 * c;
-    bool valid = p < n_rows && k < K;
-    const uint16_t *src = g.x;
-    if (valid) {
-      const int tap = k / g.cin, ci = k - tap * g.cin;
-      const int ky = tap / 3, kx = tap - 3 * ky;
-      const int xx = p % g.w, t = p / g.w;
-      const int yy = t % g.h, n = t / g.h;
-      const int sy = yy + ky - 1, sx = xx + kx - 1;
-      valid = sy >= 0 && sy < g.h && sx >= 0 && sx < g.w;
-      if (valid) src = g.x + ((long)(n * g.h + sy) * g.w + sx) * g.cs + ci;
-    }
-    const uint32_t dst = sbase + (uint32_t)(row >> 3) * kTcSbo + (uint32_t)c * kTcLbo +
-                         (uint32_t)(row & 7) * 16u;
-    cp_async16_zfill(dst, src, valid);
-  }
-}
-
 template <int BN>
 __global__ void __launch_bounds__(128) tc_gemm_bf16(const uint16_t *__restrict__ A,
                                                     const uint16_t *__restrict__ B,
@@ -135,11 +111,48 @@ __global__ void __launch_bounds__(128) tc_gemm_bf16(const uint16_t *__restrict__
   A += kz0;
   B += kz0;
   K = kz1 > kz0 ? kz1 - kz0 : 0;
+  // implicit convolution: thread t always loads k chunk t & 7 of the rows
+  // (t >> 3) + 16 i, i < 8 - their pixel coordinates are fixed for the tile
+  constexpr int kRowsPerThread = kTcBM * (kTcBK / 8) / 128;
+  long pix[kRowsPerThread];
+  int py[kRowsPerThread], px[kRowsPerThread];
+  if (conv.x != nullptr) {
+#pragma unroll
+    for (int i = 0; i < kRowsPerThread; ++i) {
+      const int p = m0 + (int)(threadIdx.x >> 3) + 16 * i;
+      const int xx = p % conv.w, t = p / conv.w;
+      const int yy = t % conv.h, n = t / conv.h;
+      py[i] = p < M ? yy : -(1 << 20);  // rows past M never pass the bounds test
+      px[i] = xx;
+      pix[i] = ((long)(n * conv.h + yy) * conv.w + xx) * conv.cs;
+    }
+  }
   auto load_a = [&](uint32_t sbase, int k0) {
-    if (conv.x != nullptr)
-      tc_load_conv_tile<kTcBM>(sbase, conv, M, K, m0, k0);
-    else
+    if (conv.x != nullptr) {
+      const int c = threadIdx.x & 7;
+      const int k = k0 + 8 * c;
+      int dy = 0, dx = 0;
+      long off = 0;
+      const bool kv = k < K;
+      if (kv) {
+        const int tap = k / conv.cin, ci = k - tap * conv.cin;
+        const int ky = tap / 3;
+        dy = ky - 1;
+        dx = tap - 3 * ky - 1;
+        off = ((long)dy * conv.w + dx) * conv.cs + ci;
+      }
+#pragma unroll
+      for (int i = 0; i < kRowsPerThread; ++i) {
+        const int row = (int)(threadIdx.x >> 3) + 16 * i;
+        const int sy = py[i] + dy, sx = px[i] + dx;
+        const bool valid = kv && (unsigned)sy < (unsigned)conv.h && (unsigned)sx < (unsigned)conv.w;
+        const uint32_t dst = sbase + (uint32_t)(row >> 3) * kTcSbo + (uint32_t)c * kTcLbo +
+                             (uint32_t)(row & 7) * 16u;
+        cp_async16_zfill(dst, valid ? conv.x + pix[i] + off : conv.x, valid);
+      }
+    } else {
       tc_load_tile<kTcBM>(sbase, A, M, K, lda, m0, k0);
+    }
   };
   const bool split = gridDim.z > 1;
   const int nk = (K + kTcBK - 1) / kTcBK;
