@@ -560,7 +560,41 @@ namespace {
 // Images for the network: every line of a patch along its trace axis (the
 // space axis along which the shot times change least, but change: receiver
 // gathers of consecutive shots) is one image of (traces x time samples).
-std::vector<agd::nn::ImageGroup> image_groups(const agd_gpu_problem &pb) {
+// Source axes of a patch: the space axes along which the shot times change,
+// by increasing mean |shot-time step| (the first: receiver gathers of
+// consecutive shots).  Lines along any of them see the blending noise of
+// other shots as incoherent.
+std::vector<int> source_axes(const agd_gpu_problem &pb, size_t p) {
+  const std::vector<int> &sh = pb.shapes[p];
+  const int D = (int)sh.size() - 1;
+  std::vector<long> stride(sh.size(), 1);
+  for (int d = (int)sh.size() - 2; d >= 0; --d) stride[d] = stride[d + 1] * sh[d + 1];
+  std::vector<std::pair<double, int>> found;
+  for (int d = 0; d < D; ++d) {
+    if (sh[d] < 2) continue;
+    const long st = stride[d] / sh[D];  // trace stride of axis d
+    double sum = 0;
+    long cnt = 0;
+    const long n_tr = (long)pb.shottimes[p].size();
+    for (long t = 0; t < n_tr; ++t)
+      if ((t / st) % sh[d] + 1 < sh[d]) {
+        sum += std::fabs((double)(pb.shottimes[p][t + st] - pb.shottimes[p][t]));
+        ++cnt;
+      }
+    const double m = cnt ? sum / cnt : 0;
+    if (m > 0) found.emplace_back(m, d);
+  }
+  std::sort(found.begin(), found.end());
+  std::vector<int> axes;
+  for (const auto &f : found) axes.push_back(f.second);
+  if (axes.empty()) axes.push_back(D - 1);
+  return axes;
+}
+
+// Images for the network: every line of each patch along its `which`-th
+// source axis (the first one where a patch has fewer) is one image of
+// (traces x time samples).
+std::vector<agd::nn::ImageGroup> image_groups(const agd_gpu_problem &pb, size_t which) {
   std::vector<agd::nn::ImageGroup> groups;
   const agd::EngineR &e = *pb.eng;
   for (size_t p = 0; p < pb.shapes.size(); ++p) {
@@ -568,26 +602,8 @@ std::vector<agd::nn::ImageGroup> image_groups(const agd_gpu_problem &pb) {
     const int D = (int)sh.size() - 1;
     std::vector<long> stride(sh.size(), 1);
     for (int d = (int)sh.size() - 2; d >= 0; --d) stride[d] = stride[d + 1] * sh[d + 1];
-    // mean |shot-time step| along each space axis (traces in C order)
-    int axis = D - 1;
-    double best = 0;
-    for (int d = 0; d < D; ++d) {
-      if (sh[d] < 2) continue;
-      const long st = stride[d] / sh[D];  // trace stride of axis d
-      double sum = 0;
-      long cnt = 0;
-      const long n_tr = (long)pb.shottimes[p].size();
-      for (long t = 0; t < n_tr; ++t)
-        if ((t / st) % sh[d] + 1 < sh[d]) {
-          sum += std::fabs((double)(pb.shottimes[p][t + st] - pb.shottimes[p][t]));
-          ++cnt;
-        }
-      const double m = cnt ? sum / cnt : 0;
-      if (m > 0 && (best == 0 || m < best)) {
-        best = m;
-        axis = d;
-      }
-    }
+    const std::vector<int> axes = source_axes(pb, p);
+    const int axis = axes[which < axes.size() ? which : 0];
     agd::nn::ImageGroup *g = nullptr;
     for (auto &x : groups)
       if (x.rows == sh[axis] && x.cols == sh[D] && x.row_stride == stride[axis]) g = &x;
@@ -613,6 +629,12 @@ std::vector<agd::nn::ImageGroup> image_groups(const agd_gpu_problem &pb) {
   return groups;
 }
 
+size_t max_source_axes(const agd_gpu_problem &pb) {
+  size_t n = 1;
+  for (size_t p = 0; p < pb.shapes.size(); ++p) n = std::max(n, source_axes(pb, p).size());
+  return n;
+}
+
 }  // namespace
 
 int agd_gpu_solve_learned(agd_gpu_problem *pb, agd_nn *net, AGD_TYPE initial_factor, int n_its,
@@ -628,15 +650,42 @@ int agd_gpu_solve_learned(agd_gpu_problem *pb, agd_nn *net, AGD_TYPE initial_fac
     throw std::runtime_error("the warm-start network serves the float library only");
 #else
     agd::EngineR &e = *pb->eng;
+    PhaseTimer timer;
     e.upload_data(data);
     pb->input_blend();
+    timer.mark("upload+blend");
     const double r0 = e.record_norm(e.rec_d.get());
     agd::EngineR::require_finite(r0, "the norm of the blended input data");
     e.start_schedule(initial_factor, n_its, std::max(1, n_its - 1));
-    // the pseudo-deblended input in data_dev becomes the network's estimate
-    agd::nn::estimate_images(net, e.data_dev.get(), image_groups(*pb), e.stream);
+    timer.mark("initial step");
+    // the pseudo-deblended input in data_dev becomes the network's estimate:
+    // the mean of its estimates from the lines along every source axis
+    const size_t n_axes = max_source_axes(*pb);
+    // (kept between calls: allocating half a gigabyte per call costs more
+    // than the estimate)
+    if (n_axes > 1 && e.est_aux.bytes() != (size_t)e.data_size * sizeof(float)) {
+      e.est_aux.alloc(e.data_size);
+      e.est_tmp.alloc(e.data_size);
+    }
+    if (n_axes > 1)
+      agd::CK(cudaMemcpyAsync(e.est_aux.get(), e.data_dev.get(), e.data_size * sizeof(float),
+                              cudaMemcpyDeviceToDevice, e.stream));
+    agd::nn::estimate_images(net, e.data_dev.get(), image_groups(*pb, 0), e.stream);
+    for (size_t a = 1; a < n_axes; ++a) {
+      agd::CK(cudaMemcpyAsync(e.est_tmp.get(), e.est_aux.get(), e.data_size * sizeof(float),
+                              cudaMemcpyDeviceToDevice, e.stream));
+      agd::nn::estimate_images(net, e.est_tmp.get(), image_groups(*pb, a), e.stream);
+      agd::mean_into<float><<<agd::EngineR::grid_for(e.data_size), agd::kThreads, 0,
+                              e.stream>>>(e.data_dev.get(), e.est_tmp.get(), e.data_size,
+                                          (float)a / (float)(a + 1));
+      agd::CK(cudaGetLastError());
+      agd::CK(cudaStreamSynchronize(e.stream));
+    }
+    timer.mark("estimate");
     e.warm_iterations(n_its, it_begin, print_freq);
+    timer.mark("warm model+its");
     e.download_data(data);
+    timer.mark("download");
 #endif
     return 0;
   });

@@ -2230,6 +2230,7 @@ class Engine {
   // with it (the wavelet operator is all-pass: its adjoint inverts it on
   // live traces).  No counterpart in the reference, which starts from zero.
   DevArray<R> inv_fold2;  // 1 / fold2 per patch data sample
+  DevArray<R> est_aux, est_tmp;  // the input and an estimate along another source axis
   // fold2 is at least 0.5^(D+1) (D space axes) on the samples the model
   // represents; with a source wavelet the last samples of a trace lie in the
   // tapered tail of the last time window, where fold2 falls towards 0: the

@@ -662,6 +662,14 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// running mean: acc = w acc + (1 - w) x
+template <typename R>
+__global__ void mean_into(R *acc, const R *x, long n, R w) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    acc[i] = w * acc[i] + ((R)1 - w) * x[i];
+}
+
 // x = 1 / max(x, floor) where x > 0 (else 0)
 template <typename R>
 __global__ void reciprocal_floor(R *x, long n, R floor) {

@@ -205,6 +205,9 @@ class Net {
   Buf<float> z, dcol, in_f, out_f, tgt_f, last_f;
   Buf<double> loss_d;
   Buf<int> err;
+  // images, their RMS and their offsets of estimate_images (grow only)
+  Buf<float> img_buf, rms_buf;
+  Buf<long> base_buf;
   cudaStream_t s = nullptr;
   long adam_t = 0;
   int cur_n = 0, cur_h = 0, cur_w = 0;
@@ -531,8 +534,8 @@ void estimate_images(agd_nn *handle, float *data, const std::vector<ImageGroup> 
   NCK(cudaEventRecord(ev, stream));
   NCK(cudaStreamWaitEvent(nt.s, ev, 0));
   const long max_pixels = 1L << 23;  // images per network pass
-  Buf<float> imgs, rms;
-  Buf<long> bases;
+  Buf<float> &imgs = nt.img_buf, &rms = nt.rms_buf;
+  Buf<long> &bases = nt.base_buf;
   for (const ImageGroup &g : groups) {
     if (g.base.empty()) continue;
     const int hp = pad8(g.rows), wp = pad8(g.cols);
