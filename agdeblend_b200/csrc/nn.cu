@@ -12,6 +12,37 @@
 
 namespace {
 
+// The persistent kernel: two CTAs per SM (at most one per output tile).
+template <int BN>
+cudaError_t launch_pipe(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K,
+                        int lda, int ldb, int ldc, float alpha, float beta,
+                        const agd::ConvGeom &conv, const agd::BiasActOut &act, int *err,
+                        cudaStream_t s) {
+  using L = agd::TcPipeSmem<BN>;
+  static int n_sms[64] = {};  // per device, per instantiation (attributes set)
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (n_sms[dev] == 0) {
+    e = cudaFuncSetAttribute(agd::tc_gemm_pipe<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             L::kBytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(agd::tc_gemm_pipe<BN>,
+                               cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    int n_sm = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    n_sms[dev] = std::max(1, n_sm);
+  }
+  const long tiles =
+      (long)((M + agd::kTcBM - 1) / agd::kTcBM) * (long)((N + BN - 1) / BN);
+  const int grid = (int)std::min<long>(tiles, (long)n_sms[dev] * L::kPerSm);
+  agd::tc_gemm_pipe<BN><<<grid, agd::kPipeThreads, L::kBytes, s>>>(
+      A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, conv, act, err);
+  return cudaGetLastError();
+}
+
 template <int BN>
 cudaError_t launch_gemm(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K,
                         int lda, int ldb, int ldc, float alpha, float beta, int splits,
@@ -27,6 +58,9 @@ cudaError_t launch_gemm(const uint16_t *A, const uint16_t *B, float *C, int M, i
   splits = std::max(1, std::min(splits, steps));
   const int k_split = (steps + splits - 1) / splits * agd::kTcBK;
   splits = (K + k_split - 1) / k_split;
+  const bool table_fits = conv.x == nullptr || steps * (agd::kTcBK / 8) <= agd::kPipeMaxChunks;
+  if (splits == 1 && K > 0 && table_fits) return launch_pipe<BN>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta,
+                                                   conv, act, err, s);
   const dim3 grid((M + agd::kTcBM - 1) / agd::kTcBM, (N + BN - 1) / BN, std::max(1, splits));
   agd::tc_gemm_bf16<BN><<<grid, 128, L::kBytes, s>>>(A, B, C, M, N, K, lda, ldb, ldc, alpha,
                                                       beta, k_split, conv, act, err);

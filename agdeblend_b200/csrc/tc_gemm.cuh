@@ -252,3 +252,261 @@ __global__ void __launch_bounds__(128) tc_gemm_bf16(const uint16_t *__restrict__
 }
 
 }  // namespace agd
+
+namespace agd {
+
+// ------------------------------------------------------------ persistent GEMM
+//
+// The same product (no split K) by persistent CTAs of 256 threads, two per
+// SM, that walk the output tiles blockIdx.x, blockIdx.x + gridDim.x, ...
+// (all M tiles of an N tile before the next N tile, so the B tile stays in
+// L2).  The K steps of every tile form one sequence per CTA, streamed
+// through S shared-memory stages by cp.async S - 1 steps ahead of the MMAs
+// (S = 4, or 3 for BN = 128 so that two CTAs fit an SM); the accumulator has
+// two TMEM buffers, so the epilogue of tile j - 1 runs while the tensor core
+// works on tile j and the copies for tile j + 1 are in flight.  Iteration g
+// of the sequence: wait for step g's copies, thread 0 issues its four MMAs
+// (and commits them to the stage's mbarrier, and at a tile's last step to
+// the accumulator's), then every thread waits for step g - 1's MMAs and
+// refills their stage with step g + S - 1.
+//
+// Copies: thread t fills k chunk (t >> 3) & 7 of rows (t & 7) + 8 (t >> 6)
+// + 32 i, so the eight threads of a shared-memory wavefront write the eight
+// rows of one core matrix (no bank conflicts) and a warp reads eight
+// consecutive rows x 64 bytes.  For implicit convolutions the tap of every
+// k chunk (its offset in the activations and its (dy, dx)) comes from a
+// table the CTA builds once, and the pixel coordinates of a thread's rows
+// are derived once per tile.  Needs K > 0 and, for convolutions,
+// K / 8 <= kPipeMaxChunks.
+constexpr int kPipeThreads = 256;
+constexpr int kPipeMaxChunks = 512;
+
+template <int BN>
+struct TcPipeSmem {
+  static constexpr int kStages = BN >= 128 ? 3 : 4;
+  static constexpr int kABytes = kTcBM * kTcBK * 2;
+  static constexpr int kBBytes = BN * kTcBK * 2;
+  static constexpr int kStage = kABytes + kBBytes;
+  static constexpr int kTab = kStages * kStage;             // int2 per k chunk
+  static constexpr int kBar = kTab + 8 * kPipeMaxChunks;    // stage, accumulator barriers
+  static constexpr int kBytes = kBar + 8 * (kStages + 2) + 16;
+  static constexpr uint32_t kCols = 2 * BN < 32 ? 32 : 2 * BN;  // power of two for BN 16..128
+  static constexpr int kPerSm = 2;
+  static_assert(kPerSm * (kBytes + 1024) <= 233472, "two CTAs per SM");
+};
+
+template <int BN>
+__global__ void __launch_bounds__(kPipeThreads, 2)
+    tc_gemm_pipe(const uint16_t *__restrict__ A, const uint16_t *__restrict__ B,
+                 float *__restrict__ C, int M, int N, int K, int lda, int ldb, int ldc,
+                 float alpha, float beta, ConvGeom conv, BiasActOut act, int *err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  using L = TcPipeSmem<BN>;
+  constexpr int S = L::kStages;
+  int2 *tab = reinterpret_cast<int2 *>(smem + L::kTab);
+  uint64_t *sbar = reinterpret_cast<uint64_t *>(smem + L::kBar);  // [S] stages
+  uint64_t *abar = sbar + S;                                       // [2] accumulators
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(abar + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nk = (K + kTcBK - 1) / kTcBK;
+  if (tid == 0) {
+    for (int i = 0; i < S + 2; ++i) umma::bar_init(&sbar[i], 1);
+    umma::bar_init_fence();
+  }
+  if (conv.x != nullptr) {
+    // k chunk j: tap (ky, kx), channel ci; .x the offset of (dy, dx, ci) in
+    // the activations, .y = (dy + 1) | (dx + 1) << 2, or -1 past K
+    for (int j = tid; j < nk * (kTcBK / 8); j += kPipeThreads) {
+      const int k = 8 * j;
+      int2 e = make_int2(0, -1);
+      if (k < K) {
+        const int tap = k / conv.cin, ci = k - tap * conv.cin;
+        const int ky = tap / 3, kx = tap - 3 * ky;
+        e.x = ((ky - 1) * conv.w + (kx - 1)) * conv.cs + ci;
+        e.y = ky | (kx << 2);
+      }
+      tab[j] = e;
+    }
+  }
+  if (warp == 0) umma::tmem_alloc(tslot, L::kCols);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tbase = *tslot;
+  const uint32_t s0 = umma::smem_u32(smem);
+  constexpr uint32_t idesc = umma::idesc_bf16(kTcBM, BN);
+  const int n_m = (M + kTcBM - 1) / kTcBM;
+  const int total = n_m * ((N + BN - 1) / BN);
+  const int n_local = (int)blockIdx.x < total ? (total - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int G = n_local * nk;
+  auto tile_of = [&](int lt, int &m0, int &n0) {
+    const int t = (int)blockIdx.x + lt * (int)gridDim.x;
+    const int nt = t / n_m;
+    m0 = (t - nt * n_m) * kTcBM;
+    n0 = nt * BN;
+  };
+  // this thread's copy slots
+  const int ck = (tid >> 3) & 7;                  // k chunk
+  const int rb = (tid & 7) + 8 * (tid >> 6);      // first row; rows rb + 32 i
+  const uint32_t slot = (uint32_t)(rb >> 3) * kTcSbo + (uint32_t)ck * kTcLbo + (uint32_t)(rb & 7) * 16u;
+  constexpr uint32_t kRowStep = 4 * kTcSbo;       // 32 rows
+  constexpr int kRowsA = kTcBM / 32, kRowsB = BN / 32 > 0 ? BN / 32 : 1;
+  // loader state: the step it copies next
+  int ld_lt = 0, ld_kt = 0, ld_st = 0, m0l = 0, n0l = 0;
+  long pix[kRowsA];
+  int py[kRowsA], px[kRowsA];
+  auto load_next = [&]() {
+    if (ld_lt < n_local) {
+      if (ld_kt == 0) {
+        tile_of(ld_lt, m0l, n0l);
+        if (conv.x != nullptr) {
+          int p = m0l + rb;
+          int x = p % conv.w, y = (p / conv.w) % conv.h;
+#pragma unroll
+          for (int i = 0; i < kRowsA; ++i) {
+            py[i] = p < M ? y : -(1 << 20);  // rows past M never pass the bounds test
+            px[i] = x;
+            pix[i] = (long)p * conv.cs;
+            p += 32;
+            x += 32;
+            while (x >= conv.w) {
+              x -= conv.w;
+              if (++y == conv.h) y = 0;
+            }
+          }
+        }
+      }
+      const uint32_t sa = s0 + (uint32_t)ld_st * L::kStage, sb = sa + L::kABytes;
+      const int k0 = ld_kt * kTcBK, k = k0 + 8 * ck;
+      if (conv.x != nullptr) {
+        const int2 e = tab[ld_kt * (kTcBK / 8) + ck];
+        const int dy = (e.y & 3) - 1, dx = ((e.y >> 2) & 3) - 1;
+#pragma unroll
+        for (int i = 0; i < kRowsA; ++i) {
+          const int sy = py[i] + dy, sx = px[i] + dx;
+          const bool valid =
+              e.y >= 0 && (unsigned)sy < (unsigned)conv.h && (unsigned)sx < (unsigned)conv.w;
+          cp_async16_zfill(sa + slot + i * kRowStep, valid ? conv.x + pix[i] + e.x : conv.x,
+                           valid);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < kRowsA; ++i) {
+          const int gr = m0l + rb + 32 * i;
+          const bool valid = gr < M && k < K;
+          cp_async16_zfill(sa + slot + i * kRowStep, valid ? A + (long)gr * lda + k : A, valid);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < kRowsB; ++i) {
+        const int gr = n0l + rb + 32 * i;
+        const bool valid = rb + 32 * i < BN && gr < N && k < K;
+        if (rb + 32 * i < BN)
+          cp_async16_zfill(sb + slot + i * kRowStep, valid ? B + (long)gr * ldb + k : B, valid);
+      }
+      ld_st = ld_st + 1 == S ? 0 : ld_st + 1;
+      if (++ld_kt == nk) {
+        ld_kt = 0;
+        ++ld_lt;
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  bool ok = true;
+  // epilogue: warp w reads TMEM lanes 32 (w % 4) .., columns of half w / 4
+  auto epilogue = [&](int lt) {
+    ok = umma::bar_wait(&abar[lt & 1], (lt >> 1) & 1) && ok;
+    ok = __syncthreads_and(ok);
+    umma::fence_after_sync();
+    if (!ok) return;
+    int m0, n0;
+    tile_of(lt, m0, n0);
+    const int row = m0 + 32 * (warp & 3) + lane;
+    const int c0 = (warp >> 2) * (BN / 2);
+    const uint32_t taddr = tbase + ((uint32_t)(32 * (warp & 3)) << 16) +
+                           (uint32_t)((lt & 1) * BN + c0);
+#pragma unroll 1
+    for (int cc = 0; cc < BN / 32; ++cc) {
+      float v[16];
+      umma::tmem_ld16(taddr + cc * 16, v);
+      if (row >= M) continue;
+      const int nb = n0 + c0 + cc * 16;
+      if (act.y != nullptr) {
+        uint32_t packed[8];
+#pragma unroll
+        for (int i = 0; i < 16; i += 2) {
+          const int n = nb + i;
+          float a = n < act.n_real ? v[i] + act.bias[n] : 0.f;
+          float b = n + 1 < act.n_real ? v[i + 1] + act.bias[n + 1] : 0.f;
+          if (act.relu) {
+            a = fmaxf(a, 0.f);
+            b = fmaxf(b, 0.f);
+          }
+          const __nv_bfloat162 h2 = __floats2bfloat162_rn(a, b);
+          packed[i / 2] = *reinterpret_cast<const uint32_t *>(&h2);
+        }
+        uint16_t *y = act.y + (long)row * act.ldy + nb;
+        if (nb + 16 <= N) {
+          reinterpret_cast<uint4 *>(y)[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+          reinterpret_cast<uint4 *>(y)[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            if (nb + i < N) y[i] = (uint16_t)(packed[i / 2] >> (16 * (i & 1)));
+        }
+      } else {
+        float *c = C + (long)row * ldc + nb;
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          if (nb + i < N) c[i] = alpha * v[i] + (beta != 0.f ? beta * c[i] : 0.f);
+      }
+    }
+    umma::fence_before_sync();  // TMEM reads done before the buffer is reused
+  };
+
+  for (int g = 0; g < S - 1; ++g) load_next();  // steps 0 .. S - 2 in flight
+  int lt = 0, kt = 0, st = 0, ph = 0;            // the step the MMAs take next
+  int pst = 0, pph = 0;                           // the previous step's stage, phase
+  for (int g = 0; g < G; ++g) {
+    asm volatile("cp.async.wait_group %0;" ::"n"(S - 2) : "memory");  // step g landed
+    umma::fence_async_smem();
+    ok = __syncthreads_and(ok);  // every thread takes the same branch
+    if (!ok) break;
+    if (tid == 0) {
+      umma::fence_after_sync();
+      const uint32_t sa = s0 + (uint32_t)st * L::kStage, sb = sa + L::kABytes;
+      const uint32_t d = tbase + (uint32_t)((lt & 1) * BN);
+#pragma unroll
+      for (int j = 0; j < kTcBK / 16; ++j) {
+        const uint64_t ad = umma::desc_kmajor(sa + 2 * j * kTcLbo, kTcLbo, kTcSbo);
+        const uint64_t bd = umma::desc_kmajor(sb + 2 * j * kTcLbo, kTcLbo, kTcSbo);
+        umma::mma_bf16(d, ad, bd, idesc, (kt > 0 || j > 0) ? 1u : 0u);
+      }
+      umma::commit(&sbar[st]);
+      if (kt == nk - 1) umma::commit(&abar[lt & 1]);
+    }
+    // step g - 1's MMAs done: its stage takes step g + S - 1
+    if (g >= 1) ok = umma::bar_wait(&sbar[pst], pph) && ok;
+    load_next();
+    if (kt == nk - 1 && lt >= 1) epilogue(lt - 1);
+    pst = st;
+    pph = ph;
+    if (++st == S) {
+      st = 0;
+      ph ^= 1;
+    }
+    if (++kt == nk) {
+      kt = 0;
+      ++lt;
+    }
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  ok = __syncthreads_and(ok);
+  if (ok && n_local > 0) epilogue(n_local - 1);
+  if (!ok && tid == 0) atomicExch(err, 1);
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_free(tbase, L::kCols);
+}
+
+}  // namespace agd

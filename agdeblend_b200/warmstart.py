@@ -117,13 +117,14 @@ def training_set(n_gathers: int = 2000, crops: int = 8, n_its: int = 100, seed: 
 
 
 def training_set_vibroseis(n_surveys: int = 40, crops: int = 1, n_its: int = 150,
-                           seed: int = TRAIN_SEED):
+                           seed: int = TRAIN_SEED, both_axes: bool = False):
     """(inputs, targets) of 32 x 256 windows of receiver gathers from seeded
     small vibroseis surveys (vibroseis_4d with seeds seed + i: 16 sY x 32 sX
     x 16 channels x 2048 samples, the 256-sample 8-80 Hz sweep, windows
     (16, 16, 16, 256)) deblended by the plain method on the GPU; every line
     along sX (32 shots x 2048 samples) gives `crops` windows, normalised by
-    the line's RMS."""
+    the line's RMS; with both_axes also every line along sY (16 shots,
+    zero-padded to 32 rows)."""
     from . import Problem
 
     rng = np.random.default_rng(seed + 100000)
@@ -136,6 +137,12 @@ def training_set_vibroseis(n_surveys: int = 40, crops: int = 1, n_its: int = 150
         p.close()
         x = np.moveaxis(sv.data[0], 1, 2).reshape(-1, 32, 2048)  # (sY, ch) lines along sX
         y = np.moveaxis(np.asarray(out[0], np.float32), 1, 2).reshape(-1, 32, 2048)
+        if both_axes:  # (sX, ch) lines along sY, padded to 32 rows
+            xs2 = np.moveaxis(sv.data[0], 0, 2).reshape(-1, 16, 2048)
+            ys2 = np.moveaxis(np.asarray(out[0], np.float32), 0, 2).reshape(-1, 16, 2048)
+            pad = ((0, 0), (0, 16), (0, 0))
+            x = np.concatenate([x, np.pad(xs2, pad)])
+            y = np.concatenate([y, np.pad(ys2, pad)])
         for xi, yi in zip(x, y):
             rms = float(np.sqrt(np.mean(xi.astype(np.float64) ** 2))) or 1.0
             for _ in range(crops):
@@ -149,9 +156,10 @@ def train(family: str = "gather_2d", n: int = 2000, epochs: int = 8, batch: int 
           lr: float = 1e-3, base_channels: int = 32, seed: int = 0):
     """A network trained on the plain method's own results: family
     "gather_2d" (n receiver gathers, training_set) or "vibroseis" (n small
-    surveys, training_set_vibroseis).  Returns (net, per-epoch mean loss)."""
+    surveys, lines along both source axes, training_set_vibroseis).
+    Returns (net, per-epoch mean loss)."""
     if family == "vibroseis":
-        x, t = training_set_vibroseis(n)
+        x, t = training_set_vibroseis(n, both_axes=True)
     else:
         x, t = training_set(n)
     net = WarmStartNet(base_channels, seed=seed)

@@ -247,10 +247,10 @@ typedef struct agd_nn agd_nn;
 
 /* agd_gpu_solve_warm with the network's estimate: `data` (blended input,
  * receives the output) is cut on the device into 2-D images - every line of
- * a patch along the space axis whose shot times change least (receiver
- * gathers of consecutive shots) x the time samples - each normalised by its
- * RMS, run through `net`, scaled back, and used as the estimate.  Float
- * library only. */
+ * a patch along a source axis (a space axis along which the shot times
+ * change: receiver gathers) x the time samples - each normalised by its
+ * RMS, run through `net` and scaled back; the estimate is the mean of the
+ * estimates from the lines along every source axis.  Float library only. */
 int agd_gpu_solve_learned(agd_gpu_problem *problem, agd_nn *net, AGD_TYPE initial_factor,
                           int n_its, int it_begin, int print_freq, AGD_TYPE *const *data);
 

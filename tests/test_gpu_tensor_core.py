@@ -1,7 +1,8 @@
 """The tcgen05 BF16 GEMM (agd_nn_gemm_bf16) against an FP32 product of the
 same BF16 operands (torch on the GPU): relative L2 error within 1e-5 (the
 tensor cores accumulate in FP32, in another order), on shapes with partial
-tiles in M, N and K, with alpha and beta, through the C-ABI."""
+tiles in M, N and K, with alpha and beta, through the C-ABI.  Products
+without split K run on the persistent kernel (tc_gemm_pipe)."""
 import ctypes
 
 import numpy as np
@@ -22,8 +23,12 @@ def _gemm():
     return fn
 
 
+# the last four have more output tiles than the GPU holds CTAs at once, so
+# the persistent CTAs walk several tiles (both TMEM accumulators, every
+# stage of the ring, one- and many-step K)
 @pytest.mark.parametrize("M,N,K", [(128, 64, 64), (200, 100, 72), (1000, 256, 520),
-                                   (37, 16, 8), (513, 129, 1024)])
+                                   (37, 16, 8), (513, 129, 1024), (76800, 32, 288),
+                                   (40000, 64, 576), (70001, 200, 136), (50000, 48, 8)])
 def test_tc_gemm_matches_fp32_product(M, N, K):
     torch = pytest.importorskip("torch")
     g = torch.Generator(device="cuda").manual_seed(M * 7 + N * 3 + K)
