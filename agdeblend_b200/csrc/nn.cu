@@ -43,6 +43,37 @@ cudaError_t launch_pipe(const uint16_t *A, const uint16_t *B, float *C, int M, i
   return cudaGetLastError();
 }
 
+// The halo-tile convolution: PER_SM CTAs per SM over the output tiles of
+// each of `groups` groups of BN output channels.
+template <int BN, int PER_SM>
+cudaError_t launch_halo(const uint16_t *B, float *C, int M, int N, int ldc, int groups,
+                        const agd::ConvGeom &conv, const agd::BiasActOut &act, int *err,
+                        cudaStream_t s) {
+  using L = agd::TcHaloSmem<PER_SM>;
+  static int n_sms[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (n_sms[dev] == 0) {
+    e = cudaFuncSetAttribute(agd::tc_conv_halo<BN, PER_SM>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(agd::tc_conv_halo<BN, PER_SM>,
+                               cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    int n_sm = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    n_sms[dev] = std::max(1, n_sm);
+  }
+  const int tiles = M / agd::kTcBM;
+  const int per_group = std::max(1, n_sms[dev] * PER_SM / groups);
+  const dim3 grid(std::min(tiles, per_group), groups);
+  agd::tc_conv_halo<BN, PER_SM><<<grid, agd::kPipeThreads, L::kBytes, s>>>(B, C, M, N, ldc, conv,
+                                                                           act, err);
+  return cudaGetLastError();
+}
+
 template <int BN>
 cudaError_t launch_gemm(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K,
                         int lda, int ldb, int ldc, float alpha, float beta, int splits,
@@ -70,6 +101,46 @@ cudaError_t launch_gemm(const uint16_t *A, const uint16_t *B, float *C, int M, i
 }  // namespace
 
 namespace agd {
+
+// How a 3 x 3 convolution (implicit GEMM geometry conv, N output channels,
+// weights N x K) runs on tc_conv_halo: channels a multiple of 32 without
+// padding, image rows a multiple of 128 pixels, and the weights of one
+// group of BN output channels in shared memory - two CTAs per SM when they
+// fit 36 KB, else one with up to 144 KB, in at most two groups of at least
+// 64 channels.  bn == 0: not eligible (the implicit GEMM runs it).
+struct HaloPlan {
+  int bn = 0, per_sm = 0, groups = 0;
+};
+
+HaloPlan halo_plan(const ConvGeom &conv, int N, int K) {
+  HaloPlan h;
+  if (conv.x == nullptr || conv.cin % 32 || conv.cs != conv.cin || conv.w % 128 ||
+      K != 9 * conv.cin || N <= 0)
+    return h;
+  const long row = 2L * K;  // bytes of one weight row
+  const int small = N <= 32 ? 32 : 64;
+  if (N <= 64 && small * row <= TcHaloSmem<2>::kMaxB) return HaloPlan{small, 2, 1};
+  for (int bn : {128, 64}) {
+    const int groups = (N + bn - 1) / bn;
+    if (bn * row <= TcHaloSmem<1>::kMaxB && groups <= 2 && (bn == 64 || N > 64))
+      return HaloPlan{bn, 1, groups};
+  }
+  return h;
+}
+
+// Y = conv3x3(X) on tc_conv_halo with a plan from halo_plan: the epilogue
+// act, or FP32 into C (row stride ldc) when act.y is null.
+cudaError_t tc_conv(const uint16_t *B, float *C, long M, int N, int ldc, const ConvGeom &conv,
+                    const HaloPlan &h, const BiasActOut &act, int *err, cudaStream_t s) {
+  if (M <= 0) return cudaSuccess;
+  if (M % kTcBM || M > INT32_MAX || h.bn == 0) return cudaErrorInvalidValue;
+  const int m = (int)M;
+  if (h.per_sm == 2)
+    return h.bn == 32 ? launch_halo<32, 2>(B, C, m, N, ldc, 1, conv, act, err, s)
+                      : launch_halo<64, 2>(B, C, m, N, ldc, 1, conv, act, err, s);
+  return h.bn == 128 ? launch_halo<128, 1>(B, C, m, N, ldc, h.groups, conv, act, err, s)
+                     : launch_halo<64, 1>(B, C, m, N, ldc, h.groups, conv, act, err, s);
+}
 
 // C = alpha A B^T + beta C on the tensor cores (see tc_gemm.cuh for the
 // operand rules); err receives 1 if an MMA wait gave up.
@@ -118,6 +189,42 @@ extern "C" int agd_nn_gemm_bf16(const void *A, const void *B, float *C, int M, i
   if (err) cudaFree(err);
   if (e != cudaSuccess || h_err) {
     std::fprintf(stderr, "ERROR: agd_nn_gemm_bf16: %s\n",
+                 e != cudaSuccess ? cudaGetErrorString(e) : "tensor-core wait timed out");
+    return 1;
+  }
+  return 0;
+}
+
+extern "C" int agd_nn_conv3x3_bf16(const void *x, int n, int h, int w, int cin,
+                                   const void *weights, int cout, float *y, void *stream) {
+  const long P = (long)n * h * w;
+  if (x == nullptr || weights == nullptr || y == nullptr || n <= 0 || h <= 0 || w <= 0 ||
+      cin <= 0 || cin % 8 || cout <= 0 || P > INT32_MAX || 9L * cin > INT32_MAX ||
+      (reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(weights)) % 16) {
+    std::fprintf(stderr,
+                 "ERROR: agd_nn_conv3x3_bf16: need positive sizes, cin a multiple of 8 and "
+                 "16-byte aligned x, weights\n");
+    return 1;
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const agd::ConvGeom geom{static_cast<const uint16_t *>(x), n, h, w, cin, cin};
+  const agd::BiasActOut none{nullptr, nullptr, 0, 0, 0};
+  const auto *wts = static_cast<const uint16_t *>(weights);
+  int *err = nullptr;
+  cudaError_t e = cudaMalloc(&err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), s);
+  if (e == cudaSuccess)
+    e = agd::halo_plan(geom, cout, 9 * cin).bn > 0
+            ? agd::tc_conv(wts, y, P, cout, cout, geom, agd::halo_plan(geom, cout, 9 * cin),
+                           none, err, s)
+            : agd::tc_gemm(nullptr, wts, y, (int)P, cout, 9 * cin, 9 * cin, 9 * cin, cout, 1.f,
+                           0.f, err, s, 1, geom);
+  int h_err = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (err) cudaFree(err);
+  if (e != cudaSuccess || h_err) {
+    std::fprintf(stderr, "ERROR: agd_nn_conv3x3_bf16: %s\n",
                  e != cudaSuccess ? cudaGetErrorString(e) : "tensor-core wait timed out");
     return 1;
   }
@@ -406,6 +513,14 @@ class Net {
                                                  L.cout_s, L.relu};
     const uint16_t *A = nullptr;
     ConvGeom geom{X.v.get(), cur_n, H, Wd, L.cin, X.Cs};  // implicit GEMM
+    if (L.cin == 1 && L.in == 0 && !keep_f32 && L.cout_s <= 64) {
+      // the first layer, from the FP32 input images
+      conv_first<<<grid_of(P), kNnThreads, 0, s>>>(in_f.get(), cur_n, H, Wd, w.get() + L.w_off,
+                                                   w.get() + L.b_off, L.cout, L.cout_s, L.relu,
+                                                   reinterpret_cast<uint4 *>(Y.v.get()));
+      NCK(cudaGetLastError());
+      return;
+    }
     if (L.cin % 8 != 0) {
       im2col3x3<<<grid_of(P * L.kp), kNnThreads, 0, s>>>(X.v.get(), cur_n, H, Wd, L.cin, X.Cs,
                                                          L.kp, col.get());
@@ -413,8 +528,14 @@ class Net {
       A = col.get();
       geom.x = nullptr;
     }
-    NCK(tc_gemm(A, wp[&L - layers.data()].get(), z.get(), (int)P, L.cout_s, L.kp, L.kp, L.kp,
-                L.cout_s, 1.f, 0.f, err.get(), s, 1, geom, act));
+    const HaloPlan hp = A == nullptr ? halo_plan(geom, L.cout_s, L.kp) : HaloPlan{};
+    if (hp.bn > 0) {
+      NCK(tc_conv(wp[&L - layers.data()].get(), z.get(), P, L.cout_s, L.cout_s, geom, hp, act,
+                  err.get(), s));
+    } else {
+      NCK(tc_gemm(A, wp[&L - layers.data()].get(), z.get(), (int)P, L.cout_s, L.kp, L.kp, L.kp,
+                  L.cout_s, 1.f, 0.f, err.get(), s, 1, geom, act));
+    }
     if (keep_f32) {
       bias_act<<<grid_of(P * L.cout_s), kNnThreads, 0, s>>>(
           z.get(), w.get() + L.b_off, P, L.cout, L.cout_s, L.relu, Y.v.get(), last_f.get());
@@ -426,22 +547,50 @@ class Net {
   void forward(const float *in_dev) {
     const long P0 = pixels(0);
     NCK(cudaMemcpyAsync(in_f.get(), in_dev, P0 * sizeof(float), cudaMemcpyDeviceToDevice, s));
-    load_input<<<grid_of(P0 * t[0].Cs), kNnThreads, 0, s>>>(in_f.get(), P0, t[0].Cs,
-                                                             t[0].v.get());
+    if (t[0].Cs == 8) {
+      load_input_v<<<grid_of(P0), kNnThreads, 0, s>>>(in_f.get(), P0,
+                                                      reinterpret_cast<uint4 *>(t[0].v.get()));
+    } else {
+      load_input<<<grid_of(P0 * t[0].Cs), kNnThreads, 0, s>>>(in_f.get(), P0, t[0].Cs,
+                                                               t[0].v.get());
+    }
     NCK(cudaGetLastError());
+    // row-wise 16-byte kernels where the channel stride is 8 times a power of two
+    auto c8_shift = [](int cs) {
+      int sh = 0;
+      while ((8 << sh) < cs) ++sh;
+      return (8 << sh) == cs ? sh : -1;
+    };
+    auto row_grid = [](long rows) {
+      return (unsigned)std::max<long>(1, std::min<long>(rows, 148L * 8));
+    };
     for (const Op &op : ops) {
       if (op.kind == kConv) {
         conv_forward(layers[op.a], op.a + 1 == (int)layers.size());
       } else if (op.kind == kPool) {
         const Tensor &X = t[op.a];
-        avgpool2<<<grid_of(pixels(X.level + 1) * X.Cs), kNnThreads, 0, s>>>(
-            X.v.get(), cur_n, cur_h >> X.level, cur_w >> X.level, X.Cs, t[op.out].v.get());
+        const int sh = c8_shift(X.Cs), H = cur_h >> X.level, Wd = cur_w >> X.level;
+        if (sh >= 0) {
+          avgpool2_v<<<row_grid((long)cur_n * (H / 2)), kNnThreads, 0, s>>>(
+              reinterpret_cast<const uint4 *>(X.v.get()), cur_n, H, Wd, sh,
+              reinterpret_cast<uint4 *>(t[op.out].v.get()));
+        } else {
+          avgpool2<<<grid_of(pixels(X.level + 1) * X.Cs), kNnThreads, 0, s>>>(
+              X.v.get(), cur_n, H, Wd, X.Cs, t[op.out].v.get());
+        }
         NCK(cudaGetLastError());
       } else {
         const Tensor &S = t[op.b];
-        upsample2_add<<<grid_of(pixels(S.level) * S.Cs), kNnThreads, 0, s>>>(
-            t[op.a].v.get(), S.v.get(), cur_n, cur_h >> S.level, cur_w >> S.level, S.Cs,
-            t[op.out].v.get());
+        const int sh = c8_shift(S.Cs), H = cur_h >> S.level, Wd = cur_w >> S.level;
+        if (sh >= 0) {
+          upsample2_add_v<<<row_grid((long)cur_n * H), kNnThreads, 0, s>>>(
+              reinterpret_cast<const uint4 *>(t[op.a].v.get()),
+              reinterpret_cast<const uint4 *>(S.v.get()), cur_n, H, Wd, sh,
+              reinterpret_cast<uint4 *>(t[op.out].v.get()));
+        } else {
+          upsample2_add<<<grid_of(pixels(S.level) * S.Cs), kNnThreads, 0, s>>>(
+              t[op.a].v.get(), S.v.get(), cur_n, H, Wd, S.Cs, t[op.out].v.get());
+        }
         NCK(cudaGetLastError());
       }
     }

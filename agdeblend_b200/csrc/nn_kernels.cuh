@@ -370,5 +370,129 @@ __global__ void scatter_images(const float *__restrict__ est, const long *__rest
   }
 }
 
+// ------------------------------------------------ 16-byte forms (inference)
+//
+// Eight BF16 channels per thread and one row of pixels per block iteration,
+// so that the index arithmetic (divisions by H and W) happens once per row,
+// not per element.  Channel strides are powers of two times 8 (c8s = log2 of
+// the 16-byte chunks per pixel).
+
+__device__ __forceinline__ void unpack8(uint4 v, float (&f)[8]) {
+  const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    f[2 * i] = __uint_as_float(w[i] << 16);
+    f[2 * i + 1] = __uint_as_float(w[i] & 0xFFFF0000u);
+  }
+}
+
+__device__ __forceinline__ uint4 pack8(const float (&f)[8]) {
+  uint32_t w[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const __nv_bfloat162 h2 = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
+    w[i] = *reinterpret_cast<const uint32_t *>(&h2);
+  }
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// y = nearest 2x upsampling of low (N, H/2, W/2) + skip (N, H, W)
+__global__ void upsample2_add_v(const uint4 *__restrict__ low, const uint4 *__restrict__ skip,
+                                int N, int H, int W, int c8s, uint4 *__restrict__ y) {
+  const int C8 = 1 << c8s, per_row = W << c8s;
+  const long rows = (long)N * H;
+  for (long r = blockIdx.x; r < rows; r += gridDim.x) {
+    const long n = r / H;
+    const int yy = (int)(r - n * H);
+    const uint4 *lrow = low + ((n * (H / 2) + yy / 2) * (W / 2) << c8s);
+    const uint4 *srow = skip + (r * W << c8s);
+    uint4 *yrow = y + (r * W << c8s);
+    for (int e = threadIdx.x; e < per_row; e += blockDim.x) {
+      float a[8], b[8];
+      unpack8(lrow[((e >> c8s) >> 1 << c8s) + (e & (C8 - 1))], a);
+      unpack8(srow[e], b);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] += b[i];
+      yrow[e] = pack8(a);
+    }
+  }
+}
+
+// y (N, H/2, W/2) = 2 x 2 average of x (N, H, W)
+__global__ void avgpool2_v(const uint4 *__restrict__ x, int N, int H, int W, int c8s,
+                           uint4 *__restrict__ y) {
+  const int C8 = 1 << c8s, Ho = H / 2, Wo = W / 2, per_row = Wo << c8s;
+  const long rows = (long)N * Ho;
+  for (long r = blockIdx.x; r < rows; r += gridDim.x) {
+    const long n = r / Ho;
+    const int yo = (int)(r - n * Ho);
+    const uint4 *r0 = x + ((n * H + 2 * yo) * W << c8s);
+    const uint4 *r1 = r0 + ((long)W << c8s);
+    uint4 *yrow = y + (r * Wo << c8s);
+    for (int e = threadIdx.x; e < per_row; e += blockDim.x) {
+      const int xo = e >> c8s, c = e & (C8 - 1);
+      const int i0 = (2 * xo << c8s) + c, i1 = i0 + C8;
+      float a[8], b[8], c2[8], d[8];
+      unpack8(r0[i0], a);
+      unpack8(r0[i1], b);
+      unpack8(r1[i0], c2);
+      unpack8(r1[i1], d);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] = 0.25f * (a[i] + b[i] + c2[i] + d[i]);
+      yrow[e] = pack8(a);
+    }
+  }
+}
+
+// First layer (one input channel): y[p][co] = bf16(act(bias[co] + sum over
+// the 3 x 3 neighbourhood of bf16(x) * bf16(w[co][tap]))) for co < cout,
+// zero for cout <= co < cout_s (a multiple of 8, at most 64), on the CUDA
+// cores: 9 products per output do not pay for an im2col copy.  One thread
+// per pixel; products exact in FP32 (BF16 operands), FP32 sums.
+__global__ void conv_first(const float *__restrict__ x, int N, int H, int W,
+                           const float *__restrict__ w, const float *__restrict__ bias, int cout,
+                           int cout_s, int relu, uint4 *__restrict__ y) {
+  __shared__ float ws[9 * 64], bs[64];
+  for (int i = threadIdx.x; i < 9 * cout_s; i += blockDim.x) {
+    const int co = i / 9, tap = i - 9 * co;
+    ws[tap * 64 + co] = co < cout ? from_bf16(to_bf16(w[co * 9 + tap])) : 0.f;
+  }
+  for (int i = threadIdx.x; i < cout_s; i += blockDim.x) bs[i] = i < cout ? bias[i] : 0.f;
+  __syncthreads();
+  const long P = (long)N * H * W;
+  const int c8 = cout_s / 8;
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < P;
+       p += (long)gridDim.x * blockDim.x) {
+    const long r = p / W;
+    const int xx = (int)(p - r * W), yy = (int)(r % H);
+    float v[9];
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+      const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+      const bool in = (unsigned)(yy + dy) < (unsigned)H && (unsigned)(xx + dx) < (unsigned)W;
+      v[tap] = in ? from_bf16(to_bf16(x[p + (long)dy * W + dx])) : 0.f;
+    }
+    for (int c = 0; c < c8; ++c) {
+      float o[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        float acc = 0.f;
+#pragma unroll
+        for (int tap = 0; tap < 9; ++tap) acc = fmaf(v[tap], ws[tap * 64 + 8 * c + i], acc);
+        acc += bs[8 * c + i];
+        o[i] = (relu && acc < 0.f) || 8 * c + i >= cout ? 0.f : acc;
+      }
+      y[p * c8 + c] = pack8(o);
+    }
+  }
+}
+
+// x (P) -> channel 0 of y (P x 8 BF16, the other channels zero)
+__global__ void load_input_v(const float *__restrict__ x, long P, uint4 *__restrict__ y) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < P;
+       p += (long)gridDim.x * blockDim.x)
+    y[p] = make_uint4((uint32_t)to_bf16(x[p]), 0u, 0u, 0u);
+}
+
 }  // namespace nn
 }  // namespace agd

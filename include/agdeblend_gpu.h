@@ -225,6 +225,17 @@ int agd_gpu_problem_set_precision(agd_gpu_problem *problem, int precision,
 int agd_nn_gemm_bf16(const void *A, const void *B, float *C, int M, int N, int K, int lda,
                      int ldb, int ldc, float alpha, float beta, void *stream);
 
+/* The network's 3 x 3 convolution (padding 1, no bias) on the tensor cores:
+ * y[n][h][w][cout] (FP32) = sum over (ky, kx, ci) of
+ * x[n][h + ky - 1][w + kx - 1][ci] * weights[cout][ky][kx][ci], x and weights
+ * BF16 device arrays (NHWC, cin a multiple of 8, 16-byte aligned), FP32
+ * accumulation.  Layers with cin a multiple of 32 and w a multiple of 128
+ * whose weights fit shared memory in at most two groups of output channels
+ * run on the halo-tile kernel, the others on the implicit GEMM.  Returns
+ * after it is done. */
+int agd_nn_conv3x3_bf16(const void *x, int n, int h, int w, int cin, const void *weights,
+                        int cout, float *y, void *stream);
+
 /* Warm start (no counterpart in the reference, whose solver starts from a
  * zero model, src/model.c:1160-1185, and whose threshold schedule starts at
  * the largest coefficient of the first adjoint, src/agdeblend.c:526-589).

@@ -49,3 +49,42 @@ def test_tc_gemm_rejects_misaligned_k():
     c = torch.zeros(16, 16, device="cuda")
     assert _gemm()(a.data_ptr(), a.data_ptr(), c.data_ptr(), 16, 16, 12, 12, 12, 16, 1.0, 0.0,
                    None) == 1
+
+
+def _conv():
+    lib = A.load_library(np.float32)
+    fn = lib.agd_nn_conv3x3_bf16
+    fn.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 4 + [ctypes.c_void_p, ctypes.c_int,
+                                                            ctypes.c_void_p, ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    return fn
+
+
+# (n, h, w, cin, cout): the halo-tile kernel (w a multiple of 128, cin a
+# multiple of 32) with two CTAs per SM - one image row, one-row images, 2
+# channel blocks, 8 and 64 output channels, weights at the 36 KB limit, more
+# tiles than resident CTAs - and with one CTA per SM - 64 and 128 channels in
+# one group, 128 and 96 (a partial second group) in two; the implicit GEMM
+# for the rest (w = 64, 256 output channels, 2304-long weight rows, cin = 8)
+@pytest.mark.parametrize("n,h,w,cin,cout", [(2, 5, 256, 32, 32), (3, 1, 128, 64, 8),
+                                            (1, 4, 384, 32, 64), (2, 3, 128, 64, 32),
+                                            (4, 32, 1024, 32, 32), (1, 3, 256, 64, 64),
+                                            (1, 3, 128, 64, 128), (2, 2, 128, 128, 128),
+                                            (1, 2, 128, 128, 96), (8, 16, 512, 64, 64),
+                                            (2, 6, 64, 32, 32), (1, 2, 128, 128, 256),
+                                            (1, 2, 128, 256, 128), (2, 4, 256, 8, 16)])
+def test_conv3x3_matches_float64(n, h, w, cin, cout):
+    """agd_nn_conv3x3_bf16 against a float64 convolution of the same BF16
+    values: relative L2 within 1e-5 (FP32 accumulation)."""
+    torch = pytest.importorskip("torch")
+    g = torch.Generator().manual_seed(n * 1000 + h * 100 + w + cin + cout)
+    x = torch.randn(n, h, w, cin, generator=g).to(torch.bfloat16)
+    wt = torch.randn(cout, 3, 3, cin, generator=g).to(torch.bfloat16)
+    want = torch.nn.functional.conv2d(x.double().permute(0, 3, 1, 2),
+                                      wt.double().permute(0, 3, 1, 2), padding=1)
+    want = want.permute(0, 2, 3, 1).numpy()
+    xd, wd = x.cuda(), wt.cuda()
+    y = torch.full((n, h, w, cout), float("nan"), device="cuda")
+    torch.cuda.synchronize()
+    assert _conv()(xd.data_ptr(), n, h, w, cin, wd.data_ptr(), cout, y.data_ptr(), None) == 0
+    assert rel_l2(y.cpu().numpy().astype(np.float64), want) <= 1e-5
