@@ -1,6 +1,7 @@
 // Learned warm start: the tensor-core building blocks (BF16 GEMM on tcgen05)
 // and their C entry points.  No counterpart in the reference, whose solver
 // always starts from a zero model (src/model.c:1160-1185).
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 
@@ -43,6 +44,39 @@ cudaError_t launch_pipe(const uint16_t *A, const uint16_t *B, float *C, int M, i
   return cudaGetLastError();
 }
 
+// cuTensorMapEncodeTiled, from the driver through the runtime (no link
+// against libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// Tensor map of NHWC BF16 activations (channel stride cs) for the halo
+// loads: box 8 channels x kHaloPix pixels x 3 rows x 1 image, zero fill
+// outside the tensor.
+cudaError_t halo_tensor_map(const agd::ConvGeom &conv, CUtensorMap *map) {
+  static EncodeTiledFn encode = nullptr;
+  if (encode == nullptr) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    const cudaError_t e =
+        cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || fn == nullptr)
+      return cudaErrorNotSupported;
+    encode = reinterpret_cast<EncodeTiledFn>(fn);
+  }
+  const cuuint64_t cs = (cuuint64_t)conv.cs, w = (cuuint64_t)conv.w, h = (cuuint64_t)conv.h;
+  const cuuint64_t dims[4] = {cs, w, h, (cuuint64_t)conv.n};
+  const cuuint64_t strides[3] = {2 * cs, 2 * cs * w, 2 * cs * w * h};  // bytes
+  const cuuint32_t box[4] = {8, agd::kHaloPix, 3, 1};
+  const cuuint32_t unit[4] = {1, 1, 1, 1};
+  const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4,
+                            const_cast<uint16_t *>(conv.x), dims, strides, box, unit,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 // The halo-tile convolution: PER_SM CTAs per SM over the output tiles of
 // each of `groups` groups of BN output channels.
 template <int BN, int PER_SM>
@@ -66,11 +100,14 @@ cudaError_t launch_halo(const uint16_t *B, float *C, int M, int N, int ldc, int 
     if (e != cudaSuccess) return e;
     n_sms[dev] = std::max(1, n_sm);
   }
+  CUtensorMap xmap;
+  e = halo_tensor_map(conv, &xmap);
+  if (e != cudaSuccess) return e;
   const int tiles = M / agd::kTcBM;
   const int per_group = std::max(1, n_sms[dev] * PER_SM / groups);
   const dim3 grid(std::min(tiles, per_group), groups);
-  agd::tc_conv_halo<BN, PER_SM><<<grid, agd::kPipeThreads, L::kBytes, s>>>(B, C, M, N, ldc, conv,
-                                                                           act, err);
+  agd::tc_conv_halo<BN, PER_SM><<<grid, agd::kHaloThreads, L::kBytes, s>>>(xmap, B, C, M, N, ldc,
+                                                                           conv, act, err);
   return cudaGetLastError();
 }
 

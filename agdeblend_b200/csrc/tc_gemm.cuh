@@ -17,6 +17,8 @@
 
 #include <cstdint>
 
+#include <cuda.h>
+
 #include "umma.cuh"
 
 namespace agd {
@@ -518,53 +520,85 @@ namespace agd {
 // layer (B, N x 9 cin, k = tap * cin + ci) held in shared memory for the
 // life of the CTA: blockIdx.y selects the group of BN output channels.  An
 // output tile is 128 consecutive pixels of one image row (w a multiple of
-// 128); for each block of 32 input channels the CTA copies the tile's halo
-// - 3 rows x 130 pixels x 32 channels, zero outside the image - once, and
-// the nine taps read it through shifted shared-memory descriptors: tap
-// (ky, kx) of chunk c starts at plane (c, ky), pixel kx, with 8 pixels (16
-// bytes each) per core matrix.  So each input value crosses L2 about 3
-// times per layer and channel group instead of 9 (the implicit-GEMM
-// loader), and B once per CTA.  Persistent CTAs (PER_SM per SM: two with
-// at most 36 KB of B, one with up to 144 KB), a 3-stage halo ring,
-// double-buffered TMEM accumulators and the epilogues of tc_gemm_pipe.
-constexpr int kHaloPix = 130;                       // pixels of a halo row
-constexpr int kHaloPlane = 3 * kHaloPix * 16;       // bytes of one chunk's 3 rows
+// 128); for each block of 32 input channels the tile's halo - 3 rows x 130
+// pixels of each 8-channel chunk, zero outside the image - arrives by four
+// TMA box loads (box 8 channels x 130 pixels x 3 rows of the NHWC tensor
+// map, corner at (channel, x0 - 1, y - 1, image); the tensor map's bounds
+// give the zero padding), one plane per chunk, and the nine taps read it
+// through shifted shared-memory descriptors: tap (ky, kx) of chunk c starts
+// at plane c, row ky, pixel kx, with 8 pixels (16 bytes each) per core
+// matrix.  So each input value crosses L2 about 3 times per layer and
+// channel group instead of 9 (the implicit-GEMM loader), and B once per
+// CTA.  Persistent CTAs (PER_SM per SM: two with at most 36 KB of B, one
+// with up to 144 KB) walk the tiles.
+//
+// Roles, linked only by mbarriers: lane 0 of warp 8 issues the TMA loads of
+// step g + 2 into the 3-stage ring (after the MMAs of step g - 1 released
+// it: `empty`) and then the 18 MMAs of step g (after its loads landed:
+// `full`; at a tile's first step also after the epilogue of the tile that
+// last used the accumulator: `acc_empty`), committed to `empty` (and at a
+// tile's last step to `acc_full`).  Warps 0-7 run the epilogues (TMEM ->
+// bias, ReLU, BF16 or FP32 -> global) and arrive on `acc_empty`.  Two TMEM
+// accumulators, so the tensor core runs tile j while the epilogue of tile
+// j - 1 drains.  Every wait is bounded; a timeout sets *err.
+constexpr int kHaloPix = 130;                       // pixels of a halo row (the TMA box)
+constexpr int kHaloBox = 3 * kHaloPix * 16;         // bytes of one chunk's box
+constexpr int kHaloPlane = 6528;                    // plane stride: the box, 128-byte aligned
 constexpr int kHaloStage = 4 * kHaloPlane;          // 32 channels
 constexpr int kHaloStages = 3;
+constexpr int kHaloThreads = kPipeThreads + 32;     // 8 epilogue warps + the control warp
+static_assert(kHaloPlane % 128 == 0 && kHaloPlane >= kHaloBox, "TMA destinations");
 
 template <int PER_SM>
 struct TcHaloSmem {
   static constexpr int kMaxB = PER_SM == 2 ? 36864 : 147456;  // bytes of B (BN x K bf16)
   static constexpr int kB = kHaloStages * kHaloStage;
-  static constexpr int kBar = kB + kMaxB;
-  static constexpr int kBytes = kBar + 8 * (kHaloStages + 2) + 16;
+  static constexpr int kBias = kB + kMaxB;                     // BN floats
+  static constexpr int kBar = kBias + (PER_SM == 2 ? 256 : 512);
+  static constexpr int kBytes = kBar + 8 * (2 * kHaloStages + 4) + 16;
   static_assert(PER_SM * (kBytes + 1024) <= 233472, "CTAs per SM");
 };
 
 template <int BN, int PER_SM>
-__global__ void __launch_bounds__(kPipeThreads, PER_SM)
-    tc_conv_halo(const uint16_t *__restrict__ B, float *__restrict__ C, int M, int N, int ldc,
-                 ConvGeom conv, BiasActOut act, int *err) {
+__global__ void __launch_bounds__(kHaloThreads, PER_SM)
+    tc_conv_halo(const __grid_constant__ CUtensorMap xmap, const uint16_t *__restrict__ B,
+                 float *__restrict__ C, int M, int N, int ldc, ConvGeom conv, BiasActOut act,
+                 int *err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   using L = TcHaloSmem<PER_SM>;
   constexpr int S = kHaloStages;
-  uint64_t *sbar = reinterpret_cast<uint64_t *>(smem + L::kBar);
-  uint64_t *abar = sbar + S;
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(abar + 2);
+  constexpr int P = kPipeThreads;  // epilogue threads
+  static_assert(BN * 4 <= L::kBar - L::kBias, "bias buffer");
+  float *bias_s = reinterpret_cast<float *>(smem + L::kBias);
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + L::kBar);
+  uint64_t *empty = full + S;
+  uint64_t *acc_full = empty + S;
+  uint64_t *acc_empty = acc_full + 2;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(acc_empty + 2);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int K = 9 * conv.cin;           // B row length (cin == cs, a multiple of 32)
   const int nkb = conv.cin / 32;        // channel blocks per tile
   const uint32_t s0 = umma::smem_u32(smem);
   const uint32_t sB = s0 + L::kB;
-  constexpr uint32_t kBSboUnit = 128;   // B: [row group][k chunk][8 rows][16 B]
-  const uint32_t b_sbo = (uint32_t)(K / 8) * kBSboUnit;
+  const uint32_t b_sbo = (uint32_t)(K / 8) * 128u;  // B: [row group][k chunk][8 rows][16 B]
+  const int n0 = (int)blockIdx.y * BN;
+  if ((s0 & 127u) != 0) {  // TMA destinations must be 128-byte aligned
+    if (tid == 0) atomicExch(err, 1);
+    return;
+  }
   if (tid == 0) {
-    for (int i = 0; i < S + 2; ++i) umma::bar_init(&sbar[i], 1);
+    for (int i = 0; i < S; ++i) {
+      umma::bar_init(&full[i], 1);
+      umma::bar_init(&empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      umma::bar_init(&acc_full[i], 1);
+      umma::bar_init(&acc_empty[i], P);
+    }
     umma::bar_init_fence();
   }
-  // this CTA's weight rows, once: rows >= N zero
-  const int n0 = (int)blockIdx.y * BN;
-  for (int q = tid; q < BN * (K / 8); q += kPipeThreads) {
+  // this CTA's weight rows (rows >= N zero) and biases, once
+  for (int q = tid; q < BN * (K / 8); q += kHaloThreads) {
     const int row = q / (K / 8), c = q - row * (K / 8);
     const bool valid = n0 + row < N;
     cp_async16_zfill(sB + (uint32_t)(row >> 3) * b_sbo + (uint32_t)c * 128u +
@@ -572,144 +606,145 @@ __global__ void __launch_bounds__(kPipeThreads, PER_SM)
                      valid ? B + (long)(n0 + row) * K + 8 * c : B, valid);
   }
   asm volatile("cp.async.commit_group;" ::: "memory");
+  if (tid < BN)
+    bias_s[tid] = act.bias != nullptr && n0 + tid < act.n_real ? act.bias[n0 + tid] : 0.f;
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  umma::fence_async_smem();
   if (warp == 0) umma::tmem_alloc(tslot, 2 * BN);
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tbase = *tslot;
-  constexpr uint32_t idesc = umma::idesc_bf16(kTcBM, BN);
   const int total = M / kTcBM;
-  const int n_local = (int)blockIdx.x < total ? (total - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int n_local =
+      (int)blockIdx.x < total ? (total - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   const int G = n_local * nkb;
-  // loader: the step it copies next
-  int ld_lt = 0, ld_kb = 0, ld_st = 0;
-  long ld_row = 0;  // pixel index of the tile's first pixel
-  int ld_y = 0, ld_x0 = 0;
-  auto load_next = [&]() {
-    if (ld_lt < n_local) {
-      if (ld_kb == 0) {
-        const long p0 = (long)((int)blockIdx.x + ld_lt * (int)gridDim.x) * kTcBM;
-        ld_row = p0;
-        ld_x0 = (int)(p0 % conv.w);
-        ld_y = (int)((p0 / conv.w) % conv.h);
-      }
-      const uint32_t st = s0 + (uint32_t)ld_st * kHaloStage;
-      // q -> pixel j = 8 (rest % 17) + (q & 7), chunk (q >> 3) & 3, row rest / 17
-      for (int q = tid; q < 51 * 32; q += kPipeThreads) {
-        const int rest = q >> 5;
-        const int r = rest / 17, j = 8 * (rest - 17 * r) + (q & 7), c = (q >> 3) & 3;
-        if (j >= kHaloPix) continue;
-        const int yy = ld_y + r - 1, xx = ld_x0 + j - 1;
-        const bool valid = (unsigned)yy < (unsigned)conv.h && (unsigned)xx < (unsigned)conv.w;
-        const long pix = ld_row + (long)(r - 1) * conv.w + (j - 1);
-        cp_async16_zfill(st + (uint32_t)((c * 3 + r) * kHaloPix + j) * 16u,
-                         valid ? conv.x + pix * conv.cs + 32 * ld_kb + 8 * c : conv.x, valid);
-      }
-      ld_st = ld_st + 1 == S ? 0 : ld_st + 1;
-      if (++ld_kb == nkb) {
-        ld_kb = 0;
-        ++ld_lt;
-      }
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-  };
   bool ok = true;
-  auto epilogue = [&](int lt) {
-    ok = umma::bar_wait(&abar[lt & 1], (lt >> 1) & 1) && ok;
-    ok = __syncthreads_and(ok);
-    umma::fence_after_sync();
-    if (!ok) return;
-    const int m0 = ((int)blockIdx.x + lt * (int)gridDim.x) * kTcBM;
-    const int row = m0 + 32 * (warp & 3) + lane;
-    const int c0 = (warp >> 2) * (BN / 2);
-    const uint32_t taddr = tbase + ((uint32_t)(32 * (warp & 3)) << 16) +
-                           (uint32_t)((lt & 1) * BN + c0);
-#pragma unroll 1
-    for (int cc = 0; cc < BN / 32; ++cc) {
-      float v[16];
-      umma::tmem_ld16(taddr + cc * 16, v);
-      const int nb = n0 + c0 + cc * 16;
-      if (nb >= N) continue;
-      if (act.y != nullptr) {
-        uint32_t packed[8];
-#pragma unroll
-        for (int i = 0; i < 16; i += 2) {
-          const int n = nb + i;
-          float a = n < act.n_real ? v[i] + act.bias[n] : 0.f;
-          float b = n + 1 < act.n_real ? v[i + 1] + act.bias[n + 1] : 0.f;
-          if (act.relu) {
-            a = fmaxf(a, 0.f);
-            b = fmaxf(b, 0.f);
-          }
-          const __nv_bfloat162 h2 = __floats2bfloat162_rn(a, b);
-          packed[i / 2] = *reinterpret_cast<const uint32_t *>(&h2);
+
+  if (warp == P / 32) {
+    // ------------------------------------------------- TMA loads and MMAs
+    if (lane == 0) {
+      constexpr uint32_t idesc = umma::idesc_bf16(kTcBM, BN);
+      const uint32_t tap_chunks = (uint32_t)(conv.cin / 8);
+      const long hw = (long)conv.h * conv.w;
+      int ld_lt = 0, ld_kb = 0, ld_n = 0, ld_y = 0, ld_x0 = 0, issued = 0, consumed = 0;
+      auto load = [&](int g) {  // step g (in order) into stage g % S
+        const int st = g % S;
+        if (g >= S) ok = umma::bar_wait(&empty[st], ((g / S) - 1) & 1) && ok;
+        if (!ok) return;
+        if (ld_kb == 0) {
+          const long p0 = (long)((int)blockIdx.x + ld_lt * (int)gridDim.x) * kTcBM;
+          ld_n = (int)(p0 / hw);
+          const long r = p0 - (long)ld_n * hw;
+          ld_y = (int)(r / conv.w);
+          ld_x0 = (int)(r - (long)ld_y * conv.w);
         }
-        uint16_t *y = act.y + (long)row * act.ldy + nb;
-        if (nb + 16 <= N) {
-          reinterpret_cast<uint4 *>(y)[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
-          reinterpret_cast<uint4 *>(y)[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+        umma::bar_arrive_expect_tx(&full[st], 4 * kHaloBox);
+        const uint32_t dst = s0 + (uint32_t)st * kHaloStage;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          umma::tma_load_4d(dst + (uint32_t)c * kHaloPlane, &xmap, 32 * ld_kb + 8 * c, ld_x0 - 1,
+                            ld_y - 1, ld_n, &full[st]);
+        issued = g + 1;
+        if (++ld_kb == nkb) {
+          ld_kb = 0;
+          ++ld_lt;
+        }
+      };
+      for (int g = 0; g < S - 1 && g < G; ++g) load(g);
+      int lt = 0, kb = 0, st = 0, ph = 0;
+      for (int g = 0; g < G && ok; ++g) {
+        if (g + S - 1 < G) load(g + S - 1);
+        // the epilogue of tile lt - 2 has read this accumulator
+        if (ok && kb == 0 && lt >= 2)
+          ok = umma::bar_wait(&acc_empty[lt & 1], ((lt >> 1) - 1) & 1);
+        if (ok) ok = umma::bar_wait(&full[st], ph);
+        if (!ok) break;
+        consumed = g + 1;
+        umma::fence_after_sync();
+        // descriptors as base + start offset (16-byte units; shared-memory
+        // addresses stay below 2^18, so the 14-bit start field cannot carry)
+        const uint64_t a0 = umma::desc_kmajor(s0 + (uint32_t)st * kHaloStage, kHaloPlane, 128u);
+        const uint64_t b0 = umma::desc_kmajor(sB, 128u, b_sbo) + (uint64_t)(4 * kb) * 8u;
+        const uint32_t d = tbase + (uint32_t)((lt & 1) * BN);
+#pragma unroll
+        for (int tap = 0; tap < 9; ++tap) {
+          const int ky = tap / 3, kx = tap - 3 * ky;
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const uint64_t ad =
+                a0 + (uint64_t)((2 * q * kHaloPlane + (ky * kHaloPix + kx) * 16) >> 4);
+            const uint64_t bd = b0 + (uint64_t)(tap * tap_chunks + 2 * q) * 8u;
+            umma::mma_bf16(d, ad, bd, idesc, (kb > 0 || tap > 0 || q > 0) ? 1u : 0u);
+          }
+        }
+        umma::commit(&empty[st]);
+        if (kb == nkb - 1) umma::commit(&acc_full[lt & 1]);
+        if (++st == S) {
+          st = 0;
+          ph ^= 1;
+        }
+        if (++kb == nkb) {
+          kb = 0;
+          ++lt;
+        }
+      }
+      // after an error: loads still in flight land before the CTA's shared
+      // memory goes away (bounded waits)
+      for (int g = consumed; g < issued; ++g) umma::bar_wait(&full[g % S], (g / S) & 1);
+    }
+  } else {
+    // -------------------------------------------------------- epilogues
+    for (int lt = 0; lt < n_local && ok; ++lt) {
+      ok = umma::bar_wait(&acc_full[lt & 1], (lt >> 1) & 1);
+      if (!ok) break;
+      umma::fence_after_sync();
+      const int row = ((int)blockIdx.x + lt * (int)gridDim.x) * kTcBM + 32 * (warp & 3) + lane;
+      const int c0 = (warp >> 2) * (BN / 2);
+      const uint32_t taddr = tbase + ((uint32_t)(32 * (warp & 3)) << 16) +
+                             (uint32_t)((lt & 1) * BN + c0);
+#pragma unroll 1
+      for (int cc = 0; cc < BN / 32; ++cc) {
+        float v[16];
+        umma::tmem_ld16(taddr + cc * 16, v);
+        const int nl = c0 + cc * 16, nb = n0 + nl;
+        if (nb >= N) continue;
+        if (act.y != nullptr) {
+          uint32_t packed[8];
+#pragma unroll
+          for (int i = 0; i < 16; i += 2) {
+            float a = nb + i < act.n_real ? v[i] + bias_s[nl + i] : 0.f;
+            float b = nb + i + 1 < act.n_real ? v[i + 1] + bias_s[nl + i + 1] : 0.f;
+            if (act.relu) {
+              a = fmaxf(a, 0.f);
+              b = fmaxf(b, 0.f);
+            }
+            const __nv_bfloat162 h2 = __floats2bfloat162_rn(a, b);
+            packed[i / 2] = *reinterpret_cast<const uint32_t *>(&h2);
+          }
+          uint16_t *y = act.y + (long)row * act.ldy + nb;
+          if (nb + 16 <= N) {
+            reinterpret_cast<uint4 *>(y)[0] =
+                make_uint4(packed[0], packed[1], packed[2], packed[3]);
+            reinterpret_cast<uint4 *>(y)[1] =
+                make_uint4(packed[4], packed[5], packed[6], packed[7]);
+          } else {
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+              if (nb + i < N) y[i] = (uint16_t)(packed[i / 2] >> (16 * (i & 1)));
+          }
         } else {
+          float *c = C + (long)row * ldc + nb;
 #pragma unroll
           for (int i = 0; i < 16; ++i)
-            if (nb + i < N) y[i] = (uint16_t)(packed[i / 2] >> (16 * (i & 1)));
-        }
-      } else {
-        float *c = C + (long)row * ldc + nb;
-#pragma unroll
-        for (int i = 0; i < 16; ++i)
-          if (nb + i < N) c[i] = v[i];
-      }
-    }
-    umma::fence_before_sync();
-  };
-
-  for (int g = 0; g < S - 1; ++g) load_next();
-  int lt = 0, kb = 0, st = 0, ph = 0, pst = 0, pph = 0;
-  for (int g = 0; g < G; ++g) {
-    // step g landed (and, at g = 0, B: the oldest group)
-    asm volatile("cp.async.wait_group %0;" ::"n"(S - 2) : "memory");
-    umma::fence_async_smem();
-    ok = __syncthreads_and(ok);
-    if (!ok) break;
-    if (tid == 0) {
-      umma::fence_after_sync();
-      // descriptors as base + start offset (16-byte units; shared-memory
-      // addresses stay below 2^18, so the 14-bit start field cannot carry)
-      const uint64_t a0 = umma::desc_kmajor(s0 + (uint32_t)st * kHaloStage, kHaloPlane, 128u);
-      const uint64_t b0 = umma::desc_kmajor(sB, 128u, b_sbo) + (uint64_t)(4 * kb) * 8u;
-      const uint32_t tap_chunks = (uint32_t)(conv.cin / 8);
-      const uint32_t d = tbase + (uint32_t)((lt & 1) * BN);
-#pragma unroll
-      for (int tap = 0; tap < 9; ++tap) {
-        const int ky = tap / 3, kx = tap - 3 * ky;
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const uint64_t ad = a0 + (uint64_t)((2 * q * 3 + ky) * kHaloPix + kx);
-          const uint64_t bd = b0 + (uint64_t)(tap * tap_chunks + 2 * q) * 8u;
-          umma::mma_bf16(d, ad, bd, idesc, (kb > 0 || tap > 0 || q > 0) ? 1u : 0u);
+            if (nb + i < N) c[i] = v[i];
         }
       }
-      umma::commit(&sbar[st]);
-      if (kb == nkb - 1) umma::commit(&abar[lt & 1]);
-    }
-    if (g >= 1) ok = umma::bar_wait(&sbar[pst], pph) && ok;
-    load_next();
-    if (kb == nkb - 1 && lt >= 1) epilogue(lt - 1);
-    pst = st;
-    pph = ph;
-    if (++st == S) {
-      st = 0;
-      ph ^= 1;
-    }
-    if (++kb == nkb) {
-      kb = 0;
-      ++lt;
+      umma::fence_before_sync();  // TMEM reads done before the MMAs reuse the buffer
+      umma::bar_arrive(&acc_empty[lt & 1]);
     }
   }
-  asm volatile("cp.async.wait_group 0;" ::: "memory");
-  ok = __syncthreads_and(ok);
-  if (ok && n_local > 0) epilogue(n_local - 1);
-  if (!ok && tid == 0) atomicExch(err, 1);
+  if (!ok) atomicExch(err, 1);
   umma::fence_before_sync();
   __syncthreads();
   if (warp == 0) umma::tmem_free(tbase, 2 * BN);

@@ -82,6 +82,38 @@ __device__ __forceinline__ void bar_init_fence() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// One arrival on the mbarrier (release at CTA scope).
+__device__ __forceinline__ void bar_arrive(uint64_t *bar) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+// Arrival that also expects `bytes` of asynchronous (TMA) transfers on the
+// mbarrier before its phase can complete.
+__device__ __forceinline__ void bar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(
+          smem_u32(bar)),
+      "r"(bytes)
+      : "memory");
+}
+
+// Tiled TMA load of a 4-D box at coordinates (c0 innermost .. c3) of the
+// tensor map into shared memory (128-byte aligned), completing `bytes` on
+// the mbarrier.  c0 times the element size must be a multiple of 16 bytes;
+// the other coordinates may lie outside the tensor (zero fill).  No
+// multicast.
+__device__ __forceinline__ void tma_load_4d(uint32_t sdst, const void *tmap, int c0, int c1,
+                                            int c2, int c3, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(sdst),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+      "r"(smem_u32(bar))
+      : "memory");
+}
+
 // Waits for the completion of the mbarrier phase of the given parity; false
 // if it did not complete within the limits above.
 __device__ __forceinline__ bool bar_wait(uint64_t *bar, unsigned parity) {
