@@ -279,10 +279,13 @@ extern "C" int agd_nn_conv3x3_bf16(const void *x, int n, int h, int w, int cin,
 //        conv(2c,c) | up + skip | conv(c,c) conv(c,1, linear)
 //   output = input + last conv (the network predicts a correction)
 // 3 x 3 convolutions with padding 1 and ReLU, 2 x 2 average pooling, nearest
-// 2x upsampling, additive skips.  Each convolution is an im2col copy and a
-// BF16 tensor-core GEMM with FP32 accumulation; the backward pass computes
-// weight gradients as split-K GEMMs over the pixels and input gradients as
-// GEMMs followed by the transpose of im2col.  Parameters: per layer the
+// 2x upsampling, additive skips.  Forward convolutions run on the tensor
+// cores with FP32 accumulation and the bias / ReLU / BF16 store in the
+// epilogue: the halo-tile kernel where halo_plan allows it, else the
+// implicit GEMM; the first layer (one input channel) on the CUDA cores.  The
+// backward pass computes weight gradients as split-K GEMMs over the pixels
+// and input gradients as GEMMs followed by the transpose of im2col.
+// Parameters: per layer the
 // weights [cout][ky][kx][cin] then the biases [cout], FP32 masters updated
 // by Adam, BF16 copies for the GEMMs.
 #include <cmath>

@@ -620,10 +620,10 @@ def _schedules(lengths, counts):
 TIME_TO_SNR = {
     "vibroseis_4d": ("vibroseis", 30, 12, lambda S: S.vibroseis_4d(seed=1002),
                      lambda S: S.vibroseis_4d(seed=4999),
-                     _schedules((150, 100, 60), (10, 20, 30, 40, 50, 60, 75, 100))),
+                     _schedules((150, 100, 80, 60), (10, 20, 30, 40, 45, 50, 55, 60, 75, 100))),
     "two_volume_3d": ("gather_2d", 2000, 8, lambda S: S.two_volume_3d(),
                       lambda S: S.two_volume_3d(seed=4998),
-                      _schedules((200, 100, 60), (5, 10, 20, 30, 40, 60, 80, 100))),
+                      _schedules((200, 100, 60), (5, 10, 20, 25, 30, 40, 60, 80, 100))),
 }
 
 
@@ -725,6 +725,48 @@ def workload_summary(line):
     return {k: line[k] for k in SUMMARY_KEYS if k in line}
 
 
+# multiply-adds per level-0 pixel of the warm-start network with base c
+# channels: 3 x 3 convolutions, level l on 4^-l of the pixels
+def network_macs_per_pixel(c: int = 32) -> int:
+    levels = [(1 * c + c * c + c * c + c * 1),
+              (c * 2 * c + 4 * c * c + 4 * c * c + 2 * c * c),
+              (2 * c * 4 * c + 16 * c * c + 16 * c * c + 4 * c * 2 * c),
+              (4 * c * 8 * c + 8 * c * 4 * c)]
+    return 9 * sum(m // 4 ** lv for lv, m in enumerate(levels))
+
+
+def measure_network(steps: int = 5, warmup: int = 3, n: int = 64, h: int = 64, w: int = 2048):
+    """Forward passes of the warm-start network (base 32) on seeded images
+    through agd_nn_forward (host arrays in and out): pixels/s and the
+    convolutions' TFLOP/s.  The default shape is one network pass of the
+    vibroseis survey's estimate: 64 receiver lines of 64 shots x 2048
+    samples (8.4 M pixels)."""
+    import time
+
+    import torch
+
+    from agdeblend_b200.nn import WarmStartNet
+
+    net = WarmStartNet(32, seed=0)
+    x = np.random.default_rng(7).standard_normal((n, h, w)).astype(np.float32)
+    for _ in range(warmup):
+        net.forward(x)
+    times = []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        net.forward(x)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    net.close()
+    s = float(np.median(times))
+    px = n * h * w
+    return {"metric": "warm-start network forward, images in and out through host memory",
+            "images": [n, h, w], "ms": 1e3 * s, "pixels_per_s": px / s,
+            "conv_tflops": 2.0 * network_macs_per_pixel(32) * px / s / 1e12,
+            "macs_per_pixel": network_macs_per_pixel(32)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -740,6 +782,8 @@ def main():
                     help="skip the learned warm-start time-to-SNR measurements")
     ap.add_argument("--time-to-snr-only", action="store_true",
                     help="only the time-to-SNR measurements (one JSON line)")
+    ap.add_argument("--network-only", action="store_true",
+                    help="only the warm-start network's forward throughput (one JSON line)")
     ap.add_argument("--no-workloads", action="store_true",
                     help="only the headline workload (no vibroseis_4d / uneven_gathers entries)")
     ap.add_argument("--workload", default="two_volume_3d",
@@ -749,6 +793,9 @@ def main():
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         run_reference(args, rank, int(os.environ.get("WORLD_SIZE", "1")))
+        return
+    if args.network_only:
+        print(json.dumps(measure_network()), flush=True)
         return
     if args.time_to_snr_only:
         print(json.dumps({n: measure_time_to_snr(n) for n in TIME_TO_SNR}), flush=True)
