@@ -110,7 +110,7 @@ def _n_dims(volumes, data):
 
 
 def _deblend_args(volumes, window_shapes, coords, shottimes, channels, trace_types, data,
-                  wavelet_idxs=None, wavelets=None, dtype=None):
+                  wavelet_idxs=None, wavelets=None, dtype=None, in_place=False):
     """Checks and converts the arguments of ``deblend`` (the reference
     wrapper's, wrappers/python/agdeblend/agdeblend.py:71-146)."""
     dtype = _dtype_of(data) if dtype is None else np.dtype(dtype)
@@ -134,25 +134,30 @@ def _deblend_args(volumes, window_shapes, coords, shottimes, channels, trace_typ
     shapes = [list(np.asarray(d).shape) for d in data]
     return capi.DeblendArgs(volumes, _n_dims(volumes, data), window_shapes, coords, shapes,
                             shottimes, channels, trace_types, data, wavelet_lengths,
-                            wavelet_idxs, wavelets, dtype=dtype)
+                            wavelet_idxs, wavelets, dtype=dtype, in_place=in_place)
 
 
 def deblend(volumes, window_shapes, coords, shottimes, channels, trace_types, initial_factor,
-            n_its, print_freq, data, wavelet_idxs=None, wavelets=None, comm=None):
+            n_its, print_freq, data, wavelet_idxs=None, wavelets=None, comm=None,
+            overwrite_input=False):
     """Deblends seismic data; same arguments and result as the reference's
-    ``agdeblend.deblend`` (serial form: ``comm`` must be None)."""
+    ``agdeblend.deblend`` (serial form: ``comm`` must be None).  The input
+    patches are left intact unless ``overwrite_input`` (an addition): then
+    patches that are C-contiguous writable arrays of the data type are
+    overwritten with the result and returned, with no copy, as the
+    reference's wrapper does."""
     if comm is not None:
         raise RuntimeError("MPI communicators are not supported: the problem runs on one GPU")
     dtype = _dtype_of(data)
     lib = load_library(dtype)
     args = _deblend_args(volumes, window_shapes, coords, shottimes, channels, trace_types, data,
-                         wavelet_idxs, wavelets, dtype)
+                         wavelet_idxs, wavelets, dtype, in_place=overwrite_input)
     fn = lib.agd_deblend
     if capi.call_deblend(fn, args, initial_factor, n_its, print_freq):
         raise RuntimeError("Error in call to agd_deblend")
-    # args.data are this call's own copies of the input, overwritten with the
-    # result: returned as they are (a second copy would cost a full pass
-    # over the data)
+    # args.data (this call's own copies of the input, or the input itself
+    # with overwrite_input) hold the result: returned as they are (a second
+    # copy would cost a full pass over the data)
     return args.data
 
 
@@ -331,9 +336,16 @@ class Problem:
         self._check(self.lib.agd_gpu_adjoint(self.h, self._p(r), self._p(out)), "adjoint")
         return out
 
-    def _data_ptrs(self, data, writable=False):
-        arrs = [np.array(d, self.dtype, copy=True, order="C") if writable
-                else np.ascontiguousarray(d, self.dtype) for d in data]
+    def _data_ptrs(self, data, writable=False, in_place=False):
+        """Pointer array of patches; writable: arrays the call may overwrite -
+        copies of the input, or with in_place the input patches themselves
+        where they are C-contiguous writable arrays of the data type."""
+        if writable and in_place:
+            arrs = [np.require(d, self.dtype, ["C", "A", "W"]) for d in data]
+        elif writable:
+            arrs = [capi.private_copy(d, self.dtype) for d in data]
+        else:
+            arrs = [np.ascontiguousarray(d, self.dtype) for d in data]
         return capi._ptrs(arrs, self.dtype, capi.real_ctype(self.dtype), writable=writable)
 
     def blend_input(self, data) -> np.ndarray:
@@ -349,8 +361,12 @@ class Problem:
         self._check(self.lib.agd_gpu_set_output(self.h, self._p(m), ptrs), "set_output")
         return outs
 
-    def solve(self, data, initial_factor: float, n_its: int, print_freq: int = 0) -> list:
-        ptrs, keep = self._data_ptrs(data, writable=True)
+    def solve(self, data, initial_factor: float, n_its: int, print_freq: int = 0,
+              overwrite_input: bool = False) -> list:
+        """agd_gpu_solve: the deblended patches (with overwrite_input, written
+        over the input patches where they are C-contiguous writable arrays
+        of the data type, as deblend(..., overwrite_input=True))."""
+        ptrs, keep = self._data_ptrs(data, writable=True, in_place=overwrite_input)
         self._check(self.lib.agd_gpu_solve(self.h, initial_factor, n_its, print_freq, ptrs),
                     "solve")
         return [k.reshape(s) for k, s in zip(keep, self.shapes)]

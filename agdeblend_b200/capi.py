@@ -103,7 +103,7 @@ class DeblendArgs:
 
     def __init__(self, volumes, n_dims, window_shapes, coords, shapes, shottimes,
                  channels, trace_types, data=None, wavelet_lengths=None,
-                 wavelet_idxs=None, wavelets=None, dtype=np.float32):
+                 wavelet_idxs=None, wavelets=None, dtype=np.float32, in_place=False):
         self.dtype = np.dtype(dtype)
         rc = real_ctype(dtype)
         self.n_patches = len(volumes)
@@ -130,10 +130,16 @@ class DeblendArgs:
             self.wavelets_p = None
         self.data = None
         if data is not None:
-            self.set_data(data)
+            self.set_data(data, in_place)
 
-    def set_data(self, data):
-        self.data = [private_copy(d, self.dtype) for d in data]
+    def set_data(self, data, in_place=False):
+        """in_place: arrays that are already C-contiguous, aligned, writable
+        ``dtype`` arrays are used as they are (the call overwrites them, as
+        the reference's own wrapper does); others are copied."""
+        if in_place:
+            self.data = [np.require(d, self.dtype, ["C", "A", "W"]) for d in data]
+        else:
+            self.data = [private_copy(d, self.dtype) for d in data]
         self.data_p, _ = _ptrs(self.data, self.dtype, real_ctype(self.dtype), writable=True)
 
     def problem_args(self):

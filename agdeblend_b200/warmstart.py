@@ -208,10 +208,11 @@ def warm_model(problem, estimate_patches) -> np.ndarray:
 
 
 def solve_learned(problem, net: WarmStartNet, data, initial_factor: float, n_its: int,
-                  it_begin: int, print_freq: int = 0):
+                  it_begin: int, print_freq: int = 0, overwrite_input: bool = False):
     """agd_gpu_solve_learned: the network's estimate of the deblended data
     (computed on the device from the uploaded input) as the warm start,
-    then iterations [it_begin, n_its) of the plain schedule."""
+    then iterations [it_begin, n_its) of the plain schedule.  The input is
+    left intact unless overwrite_input (as Problem.solve)."""
     lib = problem.lib
     _bind_warm(lib, problem.dtype)
     if not getattr(lib, "_agd_learned_bound", False):
@@ -220,7 +221,7 @@ def solve_learned(problem, net: WarmStartNet, data, initial_factor: float, n_its
                                               c_int, POINTER(POINTER(rc))]
         lib.agd_gpu_solve_learned.restype = c_int
         lib._agd_learned_bound = True
-    ptrs, keep = problem._data_ptrs(data, writable=True)
+    ptrs, keep = problem._data_ptrs(data, writable=True, in_place=overwrite_input)
     if lib.agd_gpu_solve_learned(problem.h, net.h, initial_factor, n_its, it_begin, print_freq,
                                  ptrs):
         raise RuntimeError("agd_gpu_solve_learned failed")

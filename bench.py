@@ -364,31 +364,34 @@ def measure_single(args, name, rank, world, local, cpu_its):
     wavelet_kw = {}
     if sv.wavelets is not None:
         wavelet_kw = dict(wavelet_idxs=sv.wavelet_idxs, wavelets=sv.wavelets)
-    def public_call(n_its):
+    def public_call(n_its, data):
         """The public API on host data: agd_deblend, or for a precision
-        mode the extension calls (plan, set the mode, solve, release)."""
+        mode the extension calls (plan, set the mode, solve, release); the
+        page-locked input is overwritten with the result."""
         if not args.precision:
             return A.deblend(sv.volumes, sv.window_shapes, sv.coords, sv.shottimes,
-                             sv.channels, sv.trace_types, sv.initial_factor, n_its, 0, sv.data,
-                             **wavelet_kw)
+                             sv.channels, sv.trace_types, sv.initial_factor, n_its, 0, data,
+                             overwrite_input=True, **wavelet_kw)
         p = A.Problem.from_survey(sv)
         p.set_precision(args.precision)
-        res = p.solve(sv.data, sv.initial_factor, n_its)
+        res = p.solve(data, sv.initial_factor, n_its, overwrite_input=True)
         p.close()
         return res
 
     if not args.no_e2e:
+        pinned = PinnedInput(sv.data)
         # one untimed call first: the first call in a process also pays the
         # one-time mapping of fresh device memory
-        public_call(2)
+        public_call(2, pinned.fresh())
         # three timed calls, the median counts (one call is a single sample of
         # host-side set-up time)
         calls = []
         for _ in range(3):
+            bufs = pinned.fresh()  # the caller's input, outside the timed region
             torch.cuda.synchronize()
             barrier(world)
             t0 = time.perf_counter()
-            out = public_call(sv.n_its)
+            out = public_call(sv.n_its, bufs)
             torch.cuda.synchronize()
             calls.append(barrier_max(world, time.perf_counter() - t0))
         e2e_s = float(np.median(calls))
@@ -463,7 +466,9 @@ def measure_single(args, name, rank, world, local, cpu_its):
                 "e2e": {"value": e2e_value, "unit": UNIT,
                         "h2d_bytes_per_step": data_bytes / sv.n_its,
                         "d2h_bytes_per_step": data_bytes / sv.n_its,
-                        "call_s": e2e_s, "n_its": sv.n_its, "snr_db": snr},
+                        "call_s": e2e_s, "n_its": sv.n_its, "snr_db": snr,
+                        "input": "page-locked host arrays, overwritten with the result "
+                                 "(overwrite_input=True), refilled outside the timed region"},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
                 "ms_forward_half": ms_fwd, "ms_adjoint_half": ms_adj}
         if args.precision:
@@ -605,6 +610,24 @@ def measure_batch(args, name, rank, world, local):
     return line
 
 
+class PinnedInput:
+    """Page-locked host copies of a survey's patches: the input buffers of
+    the end-to-end calls, refilled from the survey before each call (outside
+    the timed region) because the calls overwrite them with the result."""
+
+    def __init__(self, data):
+        import torch
+
+        self.src = data
+        self.bufs = [torch.empty(d.shape, dtype=torch.from_numpy(d[:0]).dtype,
+                                 pin_memory=True).numpy() for d in data]
+
+    def fresh(self):
+        for b, d in zip(self.bufs, self.src):
+            np.copyto(b, d)
+        return self.bufs
+
+
 # Time to SNR (the learned warm start): per benchmark survey, the network
 # family it is trained on, the training size and epochs, the survey, a
 # held-out validation survey of the same family (other seed) and the
@@ -675,17 +698,26 @@ def measure_time_to_snr(name):
 
     sv = make(S)
     p = A.Problem.from_survey(sv)
-    p.solve(sv.data, sv.initial_factor, 2)  # warm-up: device arrays, graphs
-    WS.solve_learned(p, net, sv.data, sv.initial_factor, n_pick, n_pick)
+    pinned = PinnedInput(sv.data)
+    p.solve(pinned.fresh(), sv.initial_factor, 2, overwrite_input=True)  # device arrays, graphs
+    WS.solve_learned(p, net, pinned.fresh(), sv.initial_factor, n_pick, n_pick,
+                     overwrite_input=True)
 
     def median_call(f):
-        runs = [timed(f) for _ in range(3)]
-        return runs[-1][0], float(np.median([r[1] for r in runs]))
+        """Three calls on a fresh page-locked copy of the input each (the
+        copy outside the timed region); the call overwrites it."""
+        runs = []
+        for _ in range(3):
+            bufs = pinned.fresh()
+            runs.append(timed(lambda: f(bufs)))
+        return [np.array(o) for o in runs[-1][0]], float(np.median([r[1] for r in runs]))
 
-    plain, t_plain = median_call(lambda: p.solve(sv.data, sv.initial_factor, sv.n_its))
+    plain, t_plain = median_call(
+        lambda d: p.solve(d, sv.initial_factor, sv.n_its, overwrite_input=True))
     target = snr(plain, sv) - 0.1
     learned, t_learned = median_call(
-        lambda: WS.solve_learned(p, net, sv.data, sv.initial_factor, n_pick, k_pick))
+        lambda d: WS.solve_learned(p, net, d, sv.initial_factor, n_pick, k_pick,
+                                   overwrite_input=True))
     res = {"metric": "seconds to the plain method's deblended SNR - 0.1 dB (one solve, host "
                      "data in and out)", "unit": "s", "higher_is_better": False,
            "survey": name, "target_snr_db": target,
@@ -703,10 +735,12 @@ def measure_time_to_snr(name):
     if name == "vibroseis_4d":
         # the precision variant: split-BF16 tensor-core space DFTs as well
         n_tc = p.set_precision(1)
-        p.solve(sv.data, sv.initial_factor, 2)
+        p.solve(pinned.fresh(), sv.initial_factor, 2, overwrite_input=True)
         lb, t_lb = median_call(
-            lambda: WS.solve_learned(p, net, sv.data, sv.initial_factor, n_pick, k_pick))
-        pb, t_pb = median_call(lambda: p.solve(sv.data, sv.initial_factor, sv.n_its))
+            lambda d: WS.solve_learned(p, net, d, sv.initial_factor, n_pick, k_pick,
+                                       overwrite_input=True))
+        pb, t_pb = median_call(
+            lambda d: p.solve(d, sv.initial_factor, sv.n_its, overwrite_input=True))
         res["learned_split_bf16"] = {"seconds": t_lb, "iterations": n_pick - k_pick,
                                      "snr_db": snr(lb, sv), "reached": bool(snr(lb, sv) >= target),
                                      "tc_windows": n_tc}

@@ -180,3 +180,17 @@ def test_print_freq_residuals_match_reference(name, capfd):
     assert np.array_equal(its, ref[f"{name}_its"])
     want = ref[f"{name}_residual"]
     assert np.all(np.abs(vals - want) <= 1e-3 * np.abs(want) + 1e-6)
+
+
+def test_overwrite_input_writes_the_result_in_place():
+    """deblend(..., overwrite_input=True) returns the caller's own arrays,
+    holding the same result as the default call (which leaves them intact)."""
+    sv = S.gather_2d(seed=77, n_its=20)
+    out = _deblend(sv, 20)
+    before = [d.copy() for d in sv.data]
+    assert all(np.array_equal(a, b) for a, b in zip(sv.data, before))
+    buf = [d.copy() for d in sv.data]
+    res = A.deblend(sv.volumes, sv.window_shapes, sv.coords, sv.shottimes, sv.channels,
+                    sv.trace_types, sv.initial_factor, 20, 0, buf, overwrite_input=True)
+    assert np.shares_memory(res[0], buf[0])
+    assert np.array_equal(res[0], out[0])
