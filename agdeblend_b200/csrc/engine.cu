@@ -591,10 +591,13 @@ std::vector<int> source_axes(const agd_gpu_problem &pb, size_t p) {
   return axes;
 }
 
-// Images for the network: every line of each patch along its `which`-th
-// source axis (the first one where a patch has fewer) is one image of
-// (traces x time samples).
-std::vector<agd::nn::ImageGroup> image_groups(const agd_gpu_problem &pb, size_t which) {
+// Lines along source axis `which` of every patch (the first one where a
+// patch has fewer), grouped by shape; with in_ch = 2 k + 1 > 1 input
+// channels, each image also gets the lines at offsets -1, +1, ..., -k, +k
+// (clamped at the patch edge) along the patch's next source axis, or itself
+// where the patch has one source axis.
+std::vector<agd::nn::ImageGroup> image_groups(const agd_gpu_problem &pb, size_t which,
+                                              int in_ch) {
   std::vector<agd::nn::ImageGroup> groups;
   const agd::EngineR &e = *pb.eng;
   for (size_t p = 0; p < pb.shapes.size(); ++p) {
@@ -603,7 +606,9 @@ std::vector<agd::nn::ImageGroup> image_groups(const agd_gpu_problem &pb, size_t 
     std::vector<long> stride(sh.size(), 1);
     for (int d = (int)sh.size() - 2; d >= 0; --d) stride[d] = stride[d + 1] * sh[d + 1];
     const std::vector<int> axes = source_axes(pb, p);
-    const int axis = axes[which < axes.size() ? which : 0];
+    const size_t ai = which < axes.size() ? which : 0;
+    const int axis = axes[ai];
+    const int nbr_axis = axes.size() > 1 ? axes[(ai + 1) % axes.size()] : -1;
     agd::nn::ImageGroup *g = nullptr;
     for (auto &x : groups)
       if (x.rows == sh[axis] && x.cols == sh[D] && x.row_stride == stride[axis]) g = &x;
@@ -618,12 +623,25 @@ std::vector<agd::nn::ImageGroup> image_groups(const agd_gpu_problem &pb, size_t 
     const long n_img = stride[0] * sh[0] / ((long)sh[axis] * sh[D]);
     for (long i = 0; i < n_img; ++i) {
       long rem = i, off = 0;
+      int j = 0;  // index along the neighbour axis
       for (int d = D - 1; d >= 0; --d) {
         if (d == axis) continue;
-        off += (rem % sh[d]) * stride[d];
+        const int idx = (int)(rem % sh[d]);
+        if (d == nbr_axis) j = idx;
+        off += idx * stride[d];
         rem /= sh[d];
       }
-      g->base.push_back(e.patch_off[p] + off);
+      const long b = e.patch_off[p] + off;
+      g->base.push_back(b);
+      for (int c = 1; c < in_ch; ++c) {
+        if (nbr_axis < 0) {
+          g->nbr.push_back(b);
+          continue;
+        }
+        const int o = (c + 1) / 2 * (c % 2 ? -1 : 1);  // -1, +1, -2, +2, ...
+        const int jn = std::min(std::max(j + o, 0), sh[nbr_axis] - 1);
+        g->nbr.push_back(b + (long)(jn - j) * stride[nbr_axis]);
+      }
     }
   }
   return groups;
@@ -661,20 +679,25 @@ int agd_gpu_solve_learned(agd_gpu_problem *pb, agd_nn *net, AGD_TYPE initial_fac
     // the pseudo-deblended input in data_dev becomes the network's estimate:
     // the mean of its estimates from the lines along every source axis
     const size_t n_axes = max_source_axes(*pb);
-    // (kept between calls: allocating half a gigabyte per call costs more
-    // than the estimate)
-    if (n_axes > 1 && e.est_aux.bytes() != (size_t)e.data_size * sizeof(float)) {
+    const int in_ch = agd::nn::input_channels(net);
+    // the input is read from an untouched copy when the estimate is written
+    // over it while other images still read it (neighbour channels, more
+    // axes); kept between calls: allocating half a gigabyte per call costs
+    // more than the estimate
+    const bool copy = n_axes > 1 || in_ch > 1;
+    if (copy && e.est_aux.bytes() != (size_t)e.data_size * sizeof(float))
       e.est_aux.alloc(e.data_size);
+    if (n_axes > 1 && e.est_tmp.bytes() != (size_t)e.data_size * sizeof(float))
       e.est_tmp.alloc(e.data_size);
-    }
-    if (n_axes > 1)
+    if (copy)
       agd::CK(cudaMemcpyAsync(e.est_aux.get(), e.data_dev.get(), e.data_size * sizeof(float),
                               cudaMemcpyDeviceToDevice, e.stream));
-    agd::nn::estimate_images(net, e.data_dev.get(), image_groups(*pb, 0), e.stream);
+    const float *src = copy ? e.est_aux.get() : e.data_dev.get();
+    agd::nn::estimate_images(net, src, e.data_dev.get(), image_groups(*pb, 0, in_ch), e.stream);
     for (size_t a = 1; a < n_axes; ++a) {
-      agd::CK(cudaMemcpyAsync(e.est_tmp.get(), e.est_aux.get(), e.data_size * sizeof(float),
-                              cudaMemcpyDeviceToDevice, e.stream));
-      agd::nn::estimate_images(net, e.est_tmp.get(), image_groups(*pb, a), e.stream);
+      // every sample of est_tmp is written (each trace lies on one line)
+      agd::nn::estimate_images(net, src, e.est_tmp.get(), image_groups(*pb, a, in_ch),
+                               e.stream);
       agd::mean_into<float><<<agd::EngineR::grid_for(e.data_size), agd::kThreads, 0,
                               e.stream>>>(e.data_dev.get(), e.est_tmp.get(), e.data_size,
                                           (float)a / (float)(a + 1));

@@ -127,8 +127,8 @@ cudaError_t launch_gemm(const uint16_t *A, const uint16_t *B, float *C, int M, i
   const int k_split = (steps + splits - 1) / splits * agd::kTcBK;
   splits = (K + k_split - 1) / k_split;
   const bool table_fits = conv.x == nullptr || steps * (agd::kTcBK / 8) <= agd::kPipeMaxChunks;
-  if (splits == 1 && K > 0 && table_fits) return launch_pipe<BN>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta,
-                                                   conv, act, err, s);
+  if (splits == 1 && K > 0 && table_fits)
+    return launch_pipe<BN>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, conv, act, err, s);
   const dim3 grid((M + agd::kTcBM - 1) / agd::kTcBM, (N + BN - 1) / BN, std::max(1, splits));
   agd::tc_gemm_bf16<BN><<<grid, 128, L::kBytes, s>>>(A, B, C, M, N, K, lda, ldb, ldc, alpha,
                                                       beta, k_split, conv, act, err);
@@ -373,6 +373,7 @@ class Net {
   };
 
   int base;
+  int in_ch = 1;  // input channels: the line and in_ch - 1 neighbouring lines
   long n_params = 0;
   std::vector<Layer> layers;
   std::vector<Op> ops;
@@ -386,14 +387,14 @@ class Net {
   Buf<float> z, dcol, in_f, out_f, tgt_f, last_f;
   Buf<double> loss_d;
   Buf<int> err;
-  // images, their RMS and their offsets of estimate_images (grow only)
-  Buf<float> img_buf, rms_buf;
-  Buf<long> base_buf;
+  // image RMS values, image and neighbour offsets of estimate_images (grow only)
+  Buf<float> rms_buf;
+  Buf<long> base_buf, nbr_buf;
   cudaStream_t s = nullptr;
   long adam_t = 0;
   int cur_n = 0, cur_h = 0, cur_w = 0;
 
-  explicit Net(int base_c, unsigned seed) : base(base_c) {
+  Net(int base_c, unsigned seed, int in_channels = 1) : base(base_c), in_ch(in_channels) {
     NCK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     const int c = base;
     auto tensor = [&](int level, int C) {
@@ -432,7 +433,7 @@ class Net {
       ops.push_back(Op{kUpAdd, low, skip, o});
       return o;
     };
-    const int x0 = tensor(0, 1);
+    const int x0 = tensor(0, in_ch);
     const int s1 = conv(conv(x0, c, 1), c, 1);
     const int s2 = conv(conv(pool(s1), 2 * c, 1), 2 * c, 1);
     const int s3 = conv(conv(pool(s2), 4 * c, 1), 4 * c, 1);
@@ -526,7 +527,7 @@ class Net {
       dzT.ensure(z_max);
     }
     const long P0 = pixels(0);
-    in_f.ensure(P0);
+    in_f.ensure((size_t)P0 * in_ch);
     out_f.ensure(P0);
     tgt_f.ensure(P0);
     last_f.ensure((size_t)P0 * t.back().Cs);
@@ -553,10 +554,11 @@ class Net {
                                                  L.cout_s, L.relu};
     const uint16_t *A = nullptr;
     ConvGeom geom{X.v.get(), cur_n, H, Wd, L.cin, X.Cs};  // implicit GEMM
-    if (L.cin == 1 && L.in == 0 && !keep_f32 && L.cout_s <= 64) {
+    if (L.in == 0 && L.cin == in_ch && in_ch <= kFirstMaxIn && !keep_f32 && L.cout_s <= 64) {
       // the first layer, from the FP32 input images
-      conv_first<<<grid_of(P), kNnThreads, 0, s>>>(in_f.get(), cur_n, H, Wd, w.get() + L.w_off,
-                                                   w.get() + L.b_off, L.cout, L.cout_s, L.relu,
+      conv_first<<<grid_of(P), kNnThreads, 0, s>>>(in_f.get(), in_ch, cur_n, H, Wd,
+                                                   w.get() + L.w_off, w.get() + L.b_off, L.cout,
+                                                   L.cout_s, L.relu,
                                                    reinterpret_cast<uint4 *>(Y.v.get()));
       NCK(cudaGetLastError());
       return;
@@ -583,15 +585,18 @@ class Net {
     }
   }
 
-  // n images (device fp32 [n][h][w]) -> out_f = input + network correction
+  // n images (device fp32 [n][h][w][in_ch]; in_f itself or copied there) ->
+  // out_f = channel 0 + network correction
   void forward(const float *in_dev) {
     const long P0 = pixels(0);
-    NCK(cudaMemcpyAsync(in_f.get(), in_dev, P0 * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    if (in_dev != in_f.get())
+      NCK(cudaMemcpyAsync(in_f.get(), in_dev, (size_t)P0 * in_ch * sizeof(float),
+                          cudaMemcpyDeviceToDevice, s));
     if (t[0].Cs == 8) {
-      load_input_v<<<grid_of(P0), kNnThreads, 0, s>>>(in_f.get(), P0,
+      load_input_v<<<grid_of(P0), kNnThreads, 0, s>>>(in_f.get(), in_ch, P0,
                                                       reinterpret_cast<uint4 *>(t[0].v.get()));
     } else {
-      load_input<<<grid_of(P0 * t[0].Cs), kNnThreads, 0, s>>>(in_f.get(), P0, t[0].Cs,
+      load_input<<<grid_of(P0 * t[0].Cs), kNnThreads, 0, s>>>(in_f.get(), in_ch, P0, t[0].Cs,
                                                                t[0].v.get());
     }
     NCK(cudaGetLastError());
@@ -634,8 +639,8 @@ class Net {
         NCK(cudaGetLastError());
       }
     }
-    residual_out<<<grid_of(P0), kNnThreads, 0, s>>>(in_f.get(), last_f.get(), P0, t.back().Cs,
-                                                     out_f.get());
+    residual_out<<<grid_of(P0), kNnThreads, 0, s>>>(in_f.get(), in_ch, last_f.get(), P0,
+                                                     t.back().Cs, out_f.get());
     NCK(cudaGetLastError());
   }
 
@@ -747,8 +752,10 @@ struct agd_nn {
 namespace agd {
 namespace nn {
 
-void estimate_images(agd_nn *handle, float *data, const std::vector<ImageGroup> &groups,
-                     cudaStream_t stream) {
+int input_channels(const agd_nn *handle) { return handle->net->in_ch; }
+
+void estimate_images(agd_nn *handle, const float *src, float *dst,
+                     const std::vector<ImageGroup> &groups, cudaStream_t stream) {
   nvtxRangePushA("agd network estimate");
   Net &nt = *handle->net;
   // the network's stream follows the caller's and the caller's the network's
@@ -757,28 +764,37 @@ void estimate_images(agd_nn *handle, float *data, const std::vector<ImageGroup> 
   NCK(cudaEventRecord(ev, stream));
   NCK(cudaStreamWaitEvent(nt.s, ev, 0));
   const long max_pixels = 1L << 23;  // images per network pass
-  Buf<float> &imgs = nt.img_buf, &rms = nt.rms_buf;
-  Buf<long> &bases = nt.base_buf;
+  Buf<float> &rms = nt.rms_buf;
+  Buf<long> &bases = nt.base_buf, &nbrs = nt.nbr_buf;
+  const int k = nt.in_ch;
   for (const ImageGroup &g : groups) {
     if (g.base.empty()) continue;
+    if (k > 1 && g.nbr.size() != g.base.size() * (k - 1))
+      throw NnError("image group without the neighbour lines of every input channel");
     const int hp = pad8(g.rows), wp = pad8(g.cols);
     const long per = (long)hp * wp;
     const int chunk = (int)std::max<long>(1, std::min<long>((long)g.base.size(),
                                                             max_pixels / per));
-    imgs.ensure((size_t)chunk * per);
     rms.ensure(chunk);
     bases.ensure(g.base.size());
     NCK(cudaMemcpyAsync(bases.get(), g.base.data(), g.base.size() * sizeof(long),
                         cudaMemcpyHostToDevice, nt.s));
+    if (k > 1) {
+      nbrs.ensure(g.nbr.size());
+      NCK(cudaMemcpyAsync(nbrs.get(), g.nbr.data(), g.nbr.size() * sizeof(long),
+                          cudaMemcpyHostToDevice, nt.s));
+    }
     for (size_t i0 = 0; i0 < g.base.size(); i0 += chunk) {
       const int n = (int)std::min<size_t>(chunk, g.base.size() - i0);
-      gather_images<<<n, kNnThreads, 0, nt.s>>>(data, bases.get() + i0, g.rows, g.cols,
-                                                 g.row_stride, hp, wp, imgs.get(), rms.get());
+      nt.shape(n, hp, wp, false);  // the images go straight into the network's input
+      gather_images<<<n, kNnThreads, 0, nt.s>>>(src, bases.get() + i0,
+                                                 k > 1 ? nbrs.get() + i0 * (k - 1) : nullptr, k,
+                                                 g.rows, g.cols, g.row_stride, hp, wp,
+                                                 nt.in_f.get(), rms.get());
       NCK(cudaGetLastError());
-      nt.shape(n, hp, wp, false);
-      nt.forward(imgs.get());
+      nt.forward(nt.in_f.get());
       scatter_images<<<n, kNnThreads, 0, nt.s>>>(nt.out_f.get(), bases.get() + i0, g.rows,
-                                                  g.cols, g.row_stride, hp, wp, rms.get(), data);
+                                                  g.cols, g.row_stride, hp, wp, rms.get(), dst);
       NCK(cudaGetLastError());
     }
   }
@@ -808,16 +824,24 @@ int nn_guarded(const char *name, F &&f) {
 
 extern "C" {
 
-int agd_nn_create(int base_channels, unsigned seed, agd_nn **net) {
-  if (net == nullptr || base_channels < 1 || base_channels > 256) return 1;
+int agd_nn_create_channels(int base_channels, int in_channels, unsigned seed, agd_nn **net) {
+  if (net == nullptr || base_channels < 1 || base_channels > 256 || in_channels < 1 ||
+      in_channels > 8)
+    return 1;
   *net = nullptr;
   return nn_guarded("agd_nn_create", [&] {
     auto h = std::make_unique<agd_nn>();
-    h->net = std::make_unique<agd::nn::Net>(base_channels, seed);
+    h->net = std::make_unique<agd::nn::Net>(base_channels, seed, in_channels);
     *net = h.release();
     return 0;
   });
 }
+
+int agd_nn_create(int base_channels, unsigned seed, agd_nn **net) {
+  return agd_nn_create_channels(base_channels, 1, seed, net);
+}
+
+int agd_nn_input_channels(const agd_nn *net) { return net ? net->net->in_ch : -1; }
 
 void agd_nn_destroy(agd_nn *net) { delete net; }
 
@@ -852,9 +876,9 @@ int agd_nn_forward(agd_nn *net, const float *input, int n, int h, int w, float *
     agd::nn::Net &nt = *net->net;
     nt.shape(n, h, w, false);
     const long P0 = (long)n * h * w;
-    agd::nn::NCK(cudaMemcpyAsync(nt.tgt_f.get(), input, P0 * sizeof(float),
+    agd::nn::NCK(cudaMemcpyAsync(nt.in_f.get(), input, (size_t)P0 * nt.in_ch * sizeof(float),
                                  cudaMemcpyHostToDevice, nt.s));
-    nt.forward(nt.tgt_f.get());
+    nt.forward(nt.in_f.get());
     agd::nn::NCK(cudaMemcpyAsync(output, nt.out_f.get(), P0 * sizeof(float),
                                  cudaMemcpyDeviceToHost, nt.s));
     nt.check_errors();
@@ -869,9 +893,9 @@ int agd_nn_loss_grad(agd_nn *net, const float *input, const float *target, int n
     agd::nn::Net &nt = *net->net;
     nt.shape(n, h, w);
     const long P0 = (long)n * h * w;
-    agd::nn::NCK(cudaMemcpyAsync(nt.tgt_f.get(), input, P0 * sizeof(float),
+    agd::nn::NCK(cudaMemcpyAsync(nt.in_f.get(), input, (size_t)P0 * nt.in_ch * sizeof(float),
                                  cudaMemcpyHostToDevice, nt.s));
-    nt.forward(nt.tgt_f.get());
+    nt.forward(nt.in_f.get());
     agd::nn::NCK(cudaMemcpyAsync(nt.tgt_f.get(), target, P0 * sizeof(float),
                                  cudaMemcpyHostToDevice, nt.s));
     nt.backward();
@@ -892,14 +916,13 @@ int agd_nn_train(agd_nn *net, const float *inputs, const float *targets, long n_
   return nn_guarded("agd_nn_train", [&] {
     agd::nn::Net &nt = *net->net;
     nt.shape(batch, h, w);
-    const long hw = (long)h * w;
-    agd::nn::Buf<float> din, dtg, dbatch;
+    const long hw = (long)h * w, hwc = hw * nt.in_ch;  // values per target, per input
+    agd::nn::Buf<float> din, dtg;
     agd::nn::Buf<int> didx;
-    din.ensure((size_t)n_samples * hw);
+    din.ensure((size_t)n_samples * hwc);
     dtg.ensure((size_t)n_samples * hw);
-    dbatch.ensure((size_t)batch * hw);
     didx.ensure(batch);
-    agd::nn::NCK(cudaMemcpyAsync(din.get(), inputs, n_samples * hw * sizeof(float),
+    agd::nn::NCK(cudaMemcpyAsync(din.get(), inputs, n_samples * hwc * sizeof(float),
                                  cudaMemcpyHostToDevice, nt.s));
     agd::nn::NCK(cudaMemcpyAsync(dtg.get(), targets, n_samples * hw * sizeof(float),
                                  cudaMemcpyHostToDevice, nt.s));
@@ -913,9 +936,10 @@ int agd_nn_train(agd_nn *net, const float *inputs, const float *targets, long n_
       for (long st = 0; st < steps; ++st) {
         agd::nn::NCK(cudaMemcpyAsync(didx.get(), perm.data() + st * batch, batch * sizeof(int),
                                      cudaMemcpyHostToDevice, nt.s));
-        agd::nn::gather_samples<<<agd::nn::grid_of(batch * hw), agd::nn::kNnThreads, 0,
-                                       nt.s>>>(din.get(), didx.get(), batch, hw, dbatch.get());
-        nt.forward(dbatch.get());
+        agd::nn::gather_samples<<<agd::nn::grid_of(batch * hwc), agd::nn::kNnThreads, 0,
+                                       nt.s>>>(din.get(), didx.get(), batch, hwc,
+                                               nt.in_f.get());
+        nt.forward(nt.in_f.get());
         agd::nn::gather_samples<<<agd::nn::grid_of(batch * hw), agd::nn::kNnThreads, 0,
                                        nt.s>>>(dtg.get(), didx.get(), batch, hw,
                                                nt.tgt_f.get());

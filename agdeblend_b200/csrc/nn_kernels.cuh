@@ -220,11 +220,11 @@ __global__ void upsample2_backward(const float *__restrict__ dy, int N, int H, i
 }
 
 // out = in + r (the residual output, channel 0 of a Cs-strided tensor)
-__global__ void residual_out(const float *__restrict__ in, const float *__restrict__ r, long P,
-                             int Cs, float *__restrict__ out) {
+__global__ void residual_out(const float *__restrict__ in, int in_ch, const float *__restrict__ r,
+                             long P, int Cs, float *__restrict__ out) {
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < P;
        p += (long)gridDim.x * blockDim.x)
-    out[p] = in[p] + r[p * Cs];
+    out[p] = in[p * in_ch] + r[p * Cs];
 }
 
 // Mean squared error over P values and its gradient with respect to the
@@ -297,13 +297,13 @@ __global__ void unpack_grad(const float *__restrict__ dwp, int cout, int k9, int
 }
 
 // input images (fp32 [n][h][w]) into the first tensor (BF16, channel 0)
-__global__ void load_input(const float *__restrict__ x, long P, int Cs,
+__global__ void load_input(const float *__restrict__ x, int in_ch, long P, int Cs,
                                   uint16_t *__restrict__ y) {
   const long total = P * Cs;
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (long)gridDim.x * blockDim.x) {
     const int c = (int)(i % Cs);
-    y[i] = c == 0 ? to_bf16(x[i / Cs]) : (uint16_t)0;
+    y[i] = c < in_ch ? to_bf16(x[i / Cs * in_ch + c]) : (uint16_t)0;
   }
 }
 
@@ -325,22 +325,27 @@ __global__ void axpy1(const float *__restrict__ x, long n, float *__restrict__ y
 }
 
 
-// Images of an ImageGroup (nn_api.hpp) gathered into [n][hp][wp] (zero
-// padding), and their RMS over the real rows x cols samples: one block per
-// image; the image is divided by its RMS (1 for a zero image) and the RMS
+// Images of an ImageGroup (nn_api.hpp) gathered into [n][hp][wp][in_ch]
+// (zero padding; channel c > 0 from the start nbr[i (in_ch - 1) + c - 1]),
+// and the RMS of channel 0 over its real rows x cols samples: one block per
+// image; the image is divided by that RMS (1 for a zero image), which is
 // kept for scatter_images.
 __global__ void gather_images(const float *__restrict__ data, const long *__restrict__ base,
-                              int rows, int cols, long row_stride, int hp, int wp,
-                              float *__restrict__ out, float *__restrict__ rms) {
+                              const long *__restrict__ nbr, int in_ch, int rows, int cols,
+                              long row_stride, int hp, int wp, float *__restrict__ out,
+                              float *__restrict__ rms) {
   const int i = blockIdx.x;
-  const float *src = data + base[i];
-  float *dst = out + (long)i * hp * wp;
+  const long n_px = (long)hp * wp;
+  float *dst = out + (long)i * n_px * in_ch;
   float s = 0.f;
-  for (long e = threadIdx.x; e < (long)hp * wp; e += blockDim.x) {
-    const int r = (int)(e / wp), c = (int)(e - (long)r * wp);
-    const float v = (r < rows && c < cols) ? src[(long)r * row_stride + c] : 0.f;
-    dst[e] = v;
-    s += v * v;
+  for (int ch = 0; ch < in_ch; ++ch) {
+    const float *src = data + (ch == 0 ? base[i] : nbr[(long)i * (in_ch - 1) + ch - 1]);
+    for (long e = threadIdx.x; e < n_px; e += blockDim.x) {
+      const int r = (int)(e / wp), c = (int)(e - (long)r * wp);
+      const float v = (r < rows && c < cols) ? src[(long)r * row_stride + c] : 0.f;
+      dst[e * in_ch + ch] = v;
+      if (ch == 0) s += v * v;
+    }
   }
   __shared__ float red[kNnThreads];
   red[threadIdx.x] = s;
@@ -352,7 +357,7 @@ __global__ void gather_images(const float *__restrict__ data, const long *__rest
   const float rm = sqrtf(red[0] / (float)((long)rows * cols));
   const float r = rm > 0.f ? rm : 1.f;
   const float inv = 1.f / r;
-  for (long e = threadIdx.x; e < (long)hp * wp; e += blockDim.x) dst[e] *= inv;
+  for (long e = threadIdx.x; e < n_px * in_ch; e += blockDim.x) dst[e] *= inv;
   if (threadIdx.x == 0) rms[i] = r;
 }
 
@@ -444,18 +449,22 @@ __global__ void avgpool2_v(const uint4 *__restrict__ x, int N, int H, int W, int
   }
 }
 
-// First layer (one input channel): y[p][co] = bf16(act(bias[co] + sum over
-// the 3 x 3 neighbourhood of bf16(x) * bf16(w[co][tap]))) for co < cout,
-// zero for cout <= co < cout_s (a multiple of 8, at most 64), on the CUDA
-// cores: 9 products per output do not pay for an im2col copy.  One thread
-// per pixel; products exact in FP32 (BF16 operands), FP32 sums.
-__global__ void conv_first(const float *__restrict__ x, int N, int H, int W,
+// First layer (in_ch <= kFirstMaxIn input channels, interleaved per pixel):
+// y[p][co] = bf16(act(bias[co] + sum over the 3 x 3 neighbourhood and the
+// channels of bf16(x) * bf16(w[co][ky][kx][ci]))) for co < cout, zero for
+// cout <= co < cout_s (a multiple of 8, at most 64), on the CUDA cores: 9
+// in_ch products per output do not pay for an im2col copy.  One thread per
+// pixel; products exact in FP32 (BF16 operands), FP32 sums.
+constexpr int kFirstMaxIn = 4;
+
+__global__ void conv_first(const float *__restrict__ x, int in_ch, int N, int H, int W,
                            const float *__restrict__ w, const float *__restrict__ bias, int cout,
                            int cout_s, int relu, uint4 *__restrict__ y) {
-  __shared__ float ws[9 * 64], bs[64];
-  for (int i = threadIdx.x; i < 9 * cout_s; i += blockDim.x) {
-    const int co = i / 9, tap = i - 9 * co;
-    ws[tap * 64 + co] = co < cout ? from_bf16(to_bf16(w[co * 9 + tap])) : 0.f;
+  __shared__ float ws[9 * kFirstMaxIn * 64], bs[64];
+  const int K = 9 * in_ch;  // k = (ky * 3 + kx) * in_ch + ci, as the weight layout
+  for (int i = threadIdx.x; i < K * cout_s; i += blockDim.x) {
+    const int co = i / K, k = i - K * co;
+    ws[k * 64 + co] = co < cout ? from_bf16(to_bf16(w[co * K + k])) : 0.f;
   }
   for (int i = threadIdx.x; i < cout_s; i += blockDim.x) bs[i] = i < cout ? bias[i] : 0.f;
   __syncthreads();
@@ -465,12 +474,15 @@ __global__ void conv_first(const float *__restrict__ x, int N, int H, int W,
        p += (long)gridDim.x * blockDim.x) {
     const long r = p / W;
     const int xx = (int)(p - r * W), yy = (int)(r % H);
-    float v[9];
+    float v[9 * kFirstMaxIn];
 #pragma unroll
     for (int tap = 0; tap < 9; ++tap) {
       const int dy = tap / 3 - 1, dx = tap % 3 - 1;
       const bool in = (unsigned)(yy + dy) < (unsigned)H && (unsigned)(xx + dx) < (unsigned)W;
-      v[tap] = in ? from_bf16(to_bf16(x[p + (long)dy * W + dx])) : 0.f;
+      const float *src = x + (p + (long)dy * W + dx) * in_ch;
+#pragma unroll
+      for (int ci = 0; ci < kFirstMaxIn; ++ci)
+        v[tap * kFirstMaxIn + ci] = in && ci < in_ch ? from_bf16(to_bf16(src[ci])) : 0.f;
     }
     for (int c = 0; c < c8; ++c) {
       float o[8];
@@ -478,7 +490,11 @@ __global__ void conv_first(const float *__restrict__ x, int N, int H, int W,
       for (int i = 0; i < 8; ++i) {
         float acc = 0.f;
 #pragma unroll
-        for (int tap = 0; tap < 9; ++tap) acc = fmaf(v[tap], ws[tap * 64 + 8 * c + i], acc);
+        for (int tap = 0; tap < 9; ++tap)
+#pragma unroll
+          for (int ci = 0; ci < kFirstMaxIn; ++ci)
+            if (ci < in_ch)
+              acc = fmaf(v[tap * kFirstMaxIn + ci], ws[(tap * in_ch + ci) * 64 + 8 * c + i], acc);
         acc += bs[8 * c + i];
         o[i] = (relu && acc < 0.f) || 8 * c + i >= cout ? 0.f : acc;
       }
@@ -487,11 +503,16 @@ __global__ void conv_first(const float *__restrict__ x, int N, int H, int W,
   }
 }
 
-// x (P) -> channel 0 of y (P x 8 BF16, the other channels zero)
-__global__ void load_input_v(const float *__restrict__ x, long P, uint4 *__restrict__ y) {
+// x (P x in_ch, in_ch <= 8) -> channels 0 .. in_ch - 1 of y (P x 8 BF16, the
+// other channels zero)
+__global__ void load_input_v(const float *__restrict__ x, int in_ch, long P,
+                             uint4 *__restrict__ y) {
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < P;
-       p += (long)gridDim.x * blockDim.x)
-    y[p] = make_uint4((uint32_t)to_bf16(x[p]), 0u, 0u, 0u);
+       p += (long)gridDim.x * blockDim.x) {
+    uint32_t w[4] = {0u, 0u, 0u, 0u};
+    for (int c = 0; c < in_ch; ++c) w[c >> 1] |= (uint32_t)to_bf16(x[p * in_ch + c]) << (16 * (c & 1));
+    y[p] = make_uint4(w[0], w[1], w[2], w[3]);
+  }
 }
 
 }  // namespace nn

@@ -261,19 +261,26 @@ typedef struct agd_nn agd_nn;
  * a patch along a source axis (a space axis along which the shot times
  * change: receiver gathers) x the time samples - each normalised by its
  * RMS, run through `net` and scaled back; the estimate is the mean of the
- * estimates from the lines along every source axis.  Float library only. */
+ * estimates from the lines along every source axis.  A network with 3
+ * input channels also receives the two neighbouring lines along the next
+ * source axis (clamped at the patch edge; the line itself where the patch
+ * has one source axis).  Float library only. */
 int agd_gpu_solve_learned(agd_gpu_problem *problem, agd_nn *net, AGD_TYPE initial_factor,
                           int n_its, int it_begin, int print_freq, AGD_TYPE *const *data);
 
 /* The warm-start network: a 4-level 2-D convolutional encoder-decoder on
  * images of n x h x w samples (traces x time; h, w multiples of 8), base
- * channels c (32: 1,162,945 parameters), output = input + a learned
- * correction.  Convolutions run as BF16 tensor-core GEMMs with FP32
- * accumulation, forward and backward; FP32 master parameters, Adam.  Arrays
- * are host memory, [n][h][w] row-major float.  Parameter layout: per layer
- * (encoder, bottleneck, decoder order) the weights [cout][3][3][cin] then
- * the biases [cout]. */
+ * channels c (32: 1,162,945 parameters with one input channel), output =
+ * input channel 0 + a learned correction.  Convolutions run as BF16
+ * tensor-core GEMMs with FP32 accumulation, forward and backward; FP32
+ * master parameters, Adam.  Arrays are host memory, row-major float: inputs
+ * [n][h][w][in_channels], outputs and targets [n][h][w].  Parameter layout:
+ * per layer (encoder, bottleneck, decoder order) the weights
+ * [cout][3][3][cin] then the biases [cout].  agd_nn_create: one input
+ * channel; agd_nn_create_channels: 1 to 8. */
 int agd_nn_create(int base_channels, unsigned seed, agd_nn **net);
+int agd_nn_create_channels(int base_channels, int in_channels, unsigned seed, agd_nn **net);
+int agd_nn_input_channels(const agd_nn *net);
 void agd_nn_destroy(agd_nn *net);
 long agd_nn_param_count(const agd_nn *net);
 int agd_nn_get_params(const agd_nn *net, float *params);

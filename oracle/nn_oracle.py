@@ -25,10 +25,11 @@ def bf16(x):
     return (u.astype(np.uint32) << 16).view(np.float32).astype(np.float64)
 
 
-def architecture(c):
+def architecture(c, in_ch=1):
     """Layers (cin, cout, relu) in parameter order and the op list:
-    ("conv", layer, in, out) | ("pool", in, out) | ("up", low, skip, out)."""
-    layers, ops, chans = [], [], [1]
+    ("conv", layer, in, out) | ("pool", in, out) | ("up", low, skip, out);
+    in_ch input channels."""
+    layers, ops, chans = [], [], [in_ch]
 
     def tensor(ch):
         chans.append(ch)
@@ -60,8 +61,8 @@ def architecture(c):
     return layers, ops
 
 
-def param_count(c):
-    return sum(9 * ci * co + co for ci, co, _ in architecture(c)[0])
+def param_count(c, in_ch=1):
+    return sum(9 * ci * co + co for ci, co, _ in architecture(c, in_ch)[0])
 
 
 def _split(params, layers):
@@ -112,17 +113,22 @@ def _down_sum(d):
 
 
 class Net:
-    def __init__(self, base, params, bf16_like_gpu=True):
-        self.layers, self.ops = architecture(base)
+    def __init__(self, base, params, bf16_like_gpu=True, in_ch=1):
+        self.in_ch = in_ch
+        self.layers, self.ops = architecture(base, in_ch)
         self.params = np.asarray(params, np.float64)
         self.q = bf16 if bf16_like_gpu else (lambda a: np.asarray(a, np.float64))
         self.wb = _split(self.params, self.layers)
 
     def forward(self, x):
-        """x (n, h, w) -> network output (n, h, w); keeps what backward needs."""
+        """x (n, h, w), or (n, h, w, in_ch) -> network output (n, h, w) =
+        channel 0 + the last convolution; keeps what backward needs."""
         q = self.q
-        n, h, w = x.shape
-        t = {0: q(x[..., None])}
+        x = np.asarray(x, np.float64)
+        if x.ndim == 3:
+            x = x[..., None]
+        assert x.shape[3] == self.in_ch
+        t = {0: q(x)}
         self.cols = {}
         last = None
         for op in self.ops:
@@ -144,8 +150,8 @@ class Net:
             else:
                 t[op[3]] = q(_up(t[op[1]]) + t[op[2]])
         self.t = t
-        self.x = np.asarray(x, np.float64)
-        self.out = self.x + last[..., 0]
+        self.x = x
+        self.out = self.x[..., 0] + last[..., 0]
         return self.out
 
     def loss_grad(self, x, target):
@@ -186,11 +192,11 @@ class Net:
         return loss, np.concatenate(flat)
 
 
-def init_params(base, seed=0):
+def init_params(base, seed=0, in_ch=1):
     """A float64 parameter vector of the layout above (He-normal weights,
     small random biases)."""
     rng = np.random.default_rng(seed)
-    layers, _ = architecture(base)
+    layers, _ = architecture(base, in_ch)
     out = []
     for ci, co, _ in layers:
         out.append(rng.standard_normal(9 * ci * co) * np.sqrt(2.0 / (9 * ci)))

@@ -9,7 +9,11 @@ loss and gradient within 1e-5 relative: only the FP32 summation order
 differs.  For the full network (base 32, sums of up to 2304 products) a sum
 that lands on the other side of a BF16 rounding boundary moves a value by
 2^-8, and such moves compound over the 14 layers: output and loss within
-2e-2, gradient within 5e-2 relative L2 with cosine similarity above 0.999."""
+2e-2, gradient within 5e-2 relative L2 with cosine similarity above 0.999.
+The base-8 network with three input channels takes the second tolerance
+too: one of its first-layer sums (27 products, FP32 on the CUDA cores)
+crosses such a boundary on this input (output 7.9e-4, gradient 1.5e-3 from
+the oracle, cosine 0.999999)."""
 import numpy as np
 import pytest
 
@@ -20,19 +24,26 @@ from conftest import rel_l2
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("base,n,h,w", [(4, 2, 16, 32), (8, 3, 8, 64), (32, 2, 32, 256)])
-def test_forward_and_gradients_match_oracle(base, n, h, w):
-    net = WarmStartNet(base, seed=base)
-    assert net.n_params == N.param_count(base)
+# (base, n, h, w, input channels): one channel, and three (a line and its
+# two neighbours, as the vibroseis warm start feeds them)
+@pytest.mark.parametrize("base,n,h,w,in_ch", [(4, 2, 16, 32, 1), (8, 3, 8, 64, 1),
+                                              (32, 2, 32, 256, 1), (4, 2, 16, 32, 3),
+                                              (8, 2, 8, 64, 3)])
+def test_forward_and_gradients_match_oracle(base, n, h, w, in_ch):
+    net = WarmStartNet(base, seed=base, in_channels=in_ch)
+    assert net.n_params == N.param_count(base, in_ch)
     rng = np.random.default_rng(base + n)
     # non-trivial weights everywhere (the network's own last layer starts small)
-    p = N.init_params(base, seed=3).astype(np.float32)
+    p = N.init_params(base, seed=3, in_ch=in_ch).astype(np.float32)
     net.set_params(p)
-    x = rng.standard_normal((n, h, w)).astype(np.float32)
-    t = (x + 0.5 * rng.standard_normal(x.shape)).astype(np.float32)
-    ora = N.Net(base, p.astype(np.float64), bf16_like_gpu=True)
+    shape = (n, h, w) if in_ch == 1 else (n, h, w, in_ch)
+    x = rng.standard_normal(shape).astype(np.float32)
+    x0 = x if in_ch == 1 else x[..., 0]
+    t = (x0 + 0.5 * rng.standard_normal(x0.shape)).astype(np.float32)
+    ora = N.Net(base, p.astype(np.float64), bf16_like_gpu=True, in_ch=in_ch)
     loss_o, g_o = ora.loss_grad(x.astype(np.float64), t.astype(np.float64))
-    tol_out, tol_grad = (1e-5, 1e-5) if base <= 8 else (2e-2, 5e-2)
+    exact = base <= 8 and (in_ch == 1 or base == 4)
+    tol_out, tol_grad = (1e-5, 1e-5) if exact else (2e-2, 5e-2)
     y = net.forward(x)
     err_out = rel_l2(y, ora.out)
     loss, g = net.loss_grad(x, t)
