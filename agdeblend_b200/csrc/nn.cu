@@ -115,7 +115,7 @@ template <int BN>
 cudaError_t launch_gemm(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K,
                         int lda, int ldb, int ldc, float alpha, float beta, int splits,
                         const agd::ConvGeom &conv, const agd::BiasActOut &act, int *err,
-                        cudaStream_t s) {
+                        cudaStream_t s, float *ws, size_t ws_elems) {
   using L = agd::TcGemmSmem<BN>;
   // per function and device; cheap enough to set on every launch
   const cudaError_t e = cudaFuncSetAttribute(
@@ -130,8 +130,18 @@ cudaError_t launch_gemm(const uint16_t *A, const uint16_t *B, float *C, int M, i
   if (splits == 1 && K > 0 && table_fits)
     return launch_pipe<BN>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, conv, act, err, s);
   const dim3 grid((M + agd::kTcBM - 1) / agd::kTcBM, (N + BN - 1) / BN, std::max(1, splits));
+  const long slice = (long)M * ldc;
+  if (splits > 1 && ws != nullptr && (size_t)splits * slice <= ws_elems) {
+    // partial products in the workspace, summed in a fixed order
+    agd::tc_gemm_bf16<BN><<<grid, 128, L::kBytes, s>>>(A, B, ws, M, N, K, lda, ldb, ldc, alpha,
+                                                        0.f, k_split, slice, conv, act, err);
+    const long total = (long)M * N;
+    const unsigned g = (unsigned)std::max<long>(1, std::min<long>((total + 255) / 256, 148L * 8));
+    agd::split_reduce<<<g, 256, 0, s>>>(ws, splits, slice, M, N, ldc, C, beta);
+    return cudaGetLastError();
+  }
   agd::tc_gemm_bf16<BN><<<grid, 128, L::kBytes, s>>>(A, B, C, M, N, K, lda, ldb, ldc, alpha,
-                                                      beta, k_split, conv, act, err);
+                                                      beta, k_split, 0L, conv, act, err);
   return cudaGetLastError();
 }
 
@@ -181,23 +191,26 @@ cudaError_t tc_conv(const uint16_t *B, float *C, long M, int N, int ldc, const C
 
 // C = alpha A B^T + beta C on the tensor cores (see tc_gemm.cuh for the
 // operand rules); err receives 1 if an MMA wait gave up.
-// With splits > 1 the K range is cut into slices whose partial products are
-// added into C with atomics: C must hold beta C already (beta is ignored).
+// With splits > 1 the K range is cut into slices: with a workspace of at
+// least (splits actually used) x M x ldc floats their partial products are
+// summed in a fixed order (deterministic), else added into C with atomics
+// (C must then hold beta C already; beta is ignored).
 cudaError_t tc_gemm(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K,
                     int lda, int ldb, int ldc, float alpha, float beta, int *err,
                     cudaStream_t s, int splits = 1,
                     const ConvGeom &conv = ConvGeom{nullptr, 0, 0, 0, 0, 0},
-                    const BiasActOut &act = BiasActOut{nullptr, nullptr, 0, 0, 0}) {
+                    const BiasActOut &act = BiasActOut{nullptr, nullptr, 0, 0, 0},
+                    float *ws = nullptr, size_t ws_elems = 0) {
   if (M <= 0 || N <= 0) return cudaSuccess;
   if (conv.x != nullptr || act.y != nullptr) splits = 1;
   if (N <= 32)
     return launch_gemm<32>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, splits, conv, act, err,
-                           s);
+                           s, ws, ws_elems);
   if (N <= 64)
     return launch_gemm<64>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, splits, conv, act, err,
-                           s);
+                           s, ws, ws_elems);
   return launch_gemm<128>(A, B, C, M, N, K, lda, ldb, ldc, alpha, beta, splits, conv, act, err,
-                          s);
+                          s, ws, ws_elems);
 }
 
 }  // namespace agd
@@ -382,6 +395,7 @@ class Net {
   Buf<float> w, grad, m, v;
   std::vector<Buf<uint16_t>> wp, wpt;  // per layer: [cout_s][kp], [kp][cout_s] BF16
   Buf<float> dwp;                      // weight-gradient GEMM output
+  Buf<float> split_ws;                 // its split-K partial products
   // scratch
   Buf<uint16_t> col, colT, dz, dzT;
   Buf<float> z, dcol, in_f, out_f, tgt_f, last_f;
@@ -537,8 +551,10 @@ class Net {
             long ldb, int ldc, float beta, int splits = 1) {
     if (M > INT32_MAX || K > INT32_MAX || lda > INT32_MAX || ldb > INT32_MAX)
       throw NnError("GEMM too large");
+    if (splits > 1) split_ws.ensure((size_t)splits * M * ldc);  // deterministic split K
     NCK(tc_gemm(A, B, C, (int)M, N, (int)K, (int)lda, (int)ldb, ldc, 1.f, beta, err.get(), s,
-                splits));
+                splits, ConvGeom{nullptr, 0, 0, 0, 0, 0}, BiasActOut{nullptr, nullptr, 0, 0, 0},
+                split_ws.get(), split_ws.n));
   }
 
   void conv_forward(const Layer &L, bool keep_f32) {

@@ -4,8 +4,11 @@
 // multiples of 8, 16-byte aligned rows), K a multiple of 8; C row-major FP32.
 //
 // Split K (gridDim.z > 1): CTA z sums k in [z * k_split, (z + 1) * k_split)
-// and adds alpha times its partial tile into C with atomics (C holds beta C
-// beforehand; the caller scales or zeroes it).
+// and either stores alpha times its partial tile into the slice C + z *
+// split_stride (split_stride > 0; split_reduce then sums the slices in a
+// fixed order, so the result does not depend on the CTAs' timing) or adds
+// it into C with atomics (C holds beta C beforehand; the caller scales or
+// zeroes it).
 //
 // One CTA of 128 threads computes a 128 x BN tile: K is walked in 64-wide
 // steps through two shared-memory stages filled by 16-byte cp.async copies
@@ -83,7 +86,8 @@ __global__ void __launch_bounds__(128) tc_gemm_bf16(const uint16_t *__restrict__
                                                     const uint16_t *__restrict__ B,
                                                     float *__restrict__ C, int M, int N, int K,
                                                     int lda, int ldb, int ldc, float alpha,
-                                                    float beta, int k_split, ConvGeom conv,
+                                                    float beta, int k_split, long split_stride,
+                                                    ConvGeom conv,
                                                     BiasActOut act, int *err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   using L = TcGemmSmem<BN>;
@@ -236,7 +240,12 @@ __global__ void __launch_bounds__(128) tc_gemm_bf16(const uint16_t *__restrict__
         }
       } else if (row < M) {
         float *c = C + (long)row * ldc + n0 + cc * 16;
-        if (split) {
+        if (split && split_stride > 0) {
+          float *cz = c + (long)blockIdx.z * split_stride;
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            if (n0 + cc * 16 + i < N) cz[i] = alpha * v[i];  // v is 0 for an empty slice
+        } else if (split) {
 #pragma unroll
           for (int i = 0; i < 16; ++i)
             if (n0 + cc * 16 + i < N && nk > 0) atomicAdd(c + i, alpha * v[i]);
@@ -251,6 +260,21 @@ __global__ void __launch_bounds__(128) tc_gemm_bf16(const uint16_t *__restrict__
   umma::fence_before_sync();
   __syncthreads();
   if (warp == 0) umma::tmem_free(tbase, kCols);
+}
+
+// C[r][c] = beta C[r][c] + sum over z < splits (in order) of the slices
+// ws[z * slice + r * ldc + c], r < M, c < N.
+__global__ void split_reduce(const float *__restrict__ ws, int splits, long slice, int M, int N,
+                             int ldc, float *__restrict__ C, float beta) {
+  const long total = (long)M * N;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / N), c = (int)(i - (long)r * N);
+    const long o = (long)r * ldc + c;
+    float s = beta != 0.f ? beta * C[o] : 0.f;
+    for (int z = 0; z < splits; ++z) s += ws[z * slice + o];
+    C[o] = s;
+  }
 }
 
 }  // namespace agd

@@ -184,14 +184,23 @@ def training_set_vibroseis(n_surveys: int = 40, crops: int = 1, n_its: int = 150
 
 
 def train(family: str = "gather_2d", n: int = 2000, epochs: int = 8, batch: int = 32,
-          lr: float = 1e-3, base_channels: int = 32, seed: int = 0):
+          lr: float | None = None, base_channels: int = 32, seed: int = 0,
+          cosine: bool | None = None):
     """A network trained on the plain method's own results: family
     "gather_2d" (n receiver gathers, training_set, one input channel) or
     "vibroseis" (n small surveys, lines along sX with their two neighbours
     along sY as channels 1 and 2, training_set_vibroseis; the neighbours
     raise the estimate of held-out surveys by about 0.9 dB, adding the lines
-    along sY as further samples lowered it).
+    along sY as further samples lowered it).  Adam; with cosine the learning
+    rate of epoch e is lr (1 + cos(pi e / epochs)) / 2 (one agd_nn_train
+    call per epoch, the optimiser state carried over).  Defaults, chosen on
+    held-out surveys: lr 1e-3 with the cosine decay for "gather_2d", a
+    constant 5e-4 for "vibroseis".
     Returns (net, per-epoch mean loss)."""
+    if lr is None:
+        lr = 5e-4 if family == "vibroseis" else 1e-3
+    if cosine is None:
+        cosine = family != "vibroseis"
     in_ch = 1
     if family == "vibroseis":
         x, t = training_set_vibroseis(n, neighbours=1)
@@ -199,7 +208,12 @@ def train(family: str = "gather_2d", n: int = 2000, epochs: int = 8, batch: int 
     else:
         x, t = training_set(n)
     net = WarmStartNet(base_channels, seed=seed, in_channels=in_ch)
-    losses = net.train(x, t, batch=batch, epochs=epochs, lr=lr, seed=seed)
+    if not cosine:
+        return net, net.train(x, t, batch=batch, epochs=epochs, lr=lr, seed=seed)
+    losses = np.zeros(epochs)
+    for e in range(epochs):
+        rate = lr * 0.5 * (1.0 + np.cos(np.pi * e / epochs))
+        losses[e] = net.train(x, t, batch=batch, epochs=1, lr=float(rate), seed=seed + e)[0]
     return net, losses
 
 

@@ -629,7 +629,11 @@ class PinnedInput:
 
 
 # Time to SNR (the learned warm start): per benchmark survey, the network
-# family it is trained on, the training size and epochs, the survey, a
+# family it is trained on, the training size and epochs, the learning
+# rate and whether it follows a cosine decay (chosen on the validation
+# surveys: the decay helps the 2-D gathers; the vibroseis lines, 30 small
+# surveys, do best with a constant 5e-4 - longer or faster training fits
+# them closer and warm-starts the held-out survey worse), the survey, a
 # held-out validation survey of the same family (other seed) and the
 # warm-started schedules to try on it: (schedule length n, first
 # iteration k), run as iterations [k, n) of the n-iteration schedule.  The
@@ -641,10 +645,11 @@ def _schedules(lengths, counts):
 
 
 TIME_TO_SNR = {
-    "vibroseis_4d": ("vibroseis", 30, 12, lambda S: S.vibroseis_4d(seed=1002),
+    "vibroseis_4d": ("vibroseis", 30, 12, 5e-4, False, lambda S: S.vibroseis_4d(seed=1002),
                      lambda S: S.vibroseis_4d(seed=4999),
-                     _schedules((150, 100, 80, 60), (10, 20, 30, 40, 45, 50, 55, 60, 75, 100))),
-    "two_volume_3d": ("gather_2d", 2000, 8, lambda S: S.two_volume_3d(),
+                     _schedules((150, 100, 80, 60, 50, 40),
+                                (10, 20, 25, 30, 35, 40, 45, 50, 55, 60, 75, 100))),
+    "two_volume_3d": ("gather_2d", 2000, 8, 1e-3, True, lambda S: S.two_volume_3d(),
                       lambda S: S.two_volume_3d(seed=4998),
                       _schedules((200, 100, 60), (5, 10, 20, 25, 30, 40, 60, 80, 100))),
 }
@@ -674,8 +679,9 @@ def measure_time_to_snr(name):
     from agdeblend_b200 import synthetic as S
     from agdeblend_b200 import warmstart as WS
 
-    family, n_train, epochs, make, make_val, grid = TIME_TO_SNR[name]
-    (net, losses), t_train = timed(lambda: WS.train(family, n_train, epochs=epochs))
+    family, n_train, epochs, lr, cosine, make, make_val, grid = TIME_TO_SNR[name]
+    (net, losses), t_train = timed(lambda: WS.train(family, n_train, epochs=epochs, lr=lr,
+                                                    cosine=cosine))
 
     def snr(out, sv):
         return S.snr_db(out, sv.truth, sv.trace_types)
@@ -728,6 +734,7 @@ def measure_time_to_snr(name):
                             "reached": bool(snr(learned, sv) >= target)},
            "speedup_learned_fp32": t_plain / t_learned,
            "network": {"family": family, "training": n_train, "epochs": epochs,
+                       "lr": lr, "cosine_lr": cosine, "input_channels": net.in_channels,
                        "loss_first_last": [float(losses[0]), float(losses[-1])],
                        "train_seconds": t_train},
            "validation": {"target_snr_db": target_val,

@@ -69,3 +69,19 @@ def test_training_lowers_the_loss():
     losses = net.train(noisy, clean, batch=16, epochs=30, lr=2e-3)
     assert losses[-1] < 0.3 * losses[0]
     net.close()
+
+
+def test_training_is_deterministic():
+    """Two trainings from the same seed on the same data end with identical
+    parameters: the split-K weight gradients sum their partial products in
+    a fixed order (no atomics)."""
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal((64, 16, 64, 3)).astype(np.float32)
+    t = (x[..., 0] + 0.3 * rng.standard_normal((64, 16, 64))).astype(np.float32)
+    params = []
+    for _ in range(2):
+        net = WarmStartNet(8, seed=2, in_channels=3)
+        net.train(x, t, batch=16, epochs=2, lr=1e-3, seed=4)
+        params.append(net.params())
+        net.close()
+    assert np.array_equal(params[0], params[1])
