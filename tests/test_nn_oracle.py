@@ -38,3 +38,21 @@ def test_backprop_matches_finite_differences(in_ch):
         l2 = N.Net(base, p2, False, in_ch).loss_grad(x, target)[0]
         fd = (l1 - l2) / (2 * h)
         assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd)) + 1e-8, (i, fd, g[i])
+
+
+def test_neighbour_lines_channel_order():
+    """warmstart.neighbour_lines: channel 0 the line itself, then the lines at
+    offsets -1, +1 (clamped at the edges) along the neighbour axis - the
+    order agd_gpu_solve_learned gathers on the device."""
+    from agdeblend_b200.warmstart import neighbour_lines
+
+    v = np.arange(3 * 4 * 2 * 5, dtype=np.float32).reshape(3, 4, 2, 5)  # (sY, sX, ch, t)
+    x = neighbour_lines(v, 1, 0, 1)  # lines along sX, neighbours along sY
+    assert x.shape == (3 * 2, 4, 5, 3)
+    lines = np.moveaxis(v, 1, 2).reshape(-1, 4, 5)
+    for sy in range(3):
+        for ch in range(2):
+            i = sy * 2 + ch
+            assert np.array_equal(x[i, ..., 0], lines[i])
+            assert np.array_equal(x[i, ..., 1], lines[max(sy - 1, 0) * 2 + ch])
+            assert np.array_equal(x[i, ..., 2], lines[min(sy + 1, 2) * 2 + ch])
