@@ -591,11 +591,14 @@ std::vector<int> source_axes(const agd_gpu_problem &pb, size_t p) {
   return axes;
 }
 
-// Lines along source axis `which` of every patch (the first one where a
-// patch has fewer), grouped by shape; with in_ch = 2 k + 1 > 1 input
-// channels, each image also gets the lines at offsets -1, +1, ..., -k, +k
-// (clamped at the patch edge) along the patch's next source axis, or itself
-// where the patch has one source axis.
+// Lines along source axis `which` of every patch (source axes in order of
+// their shot-time step, smallest first; the first one where a patch has
+// fewer), grouped by shape.  A network with in_ch = 2 k + 1 > 1 input
+// channels gets the lines along each patch's slowest source axis instead
+// (`which` ignored), each with the lines at offsets -1, +1, ..., -k, +k
+// (clamped at the patch edge) along the next faster source axis - the shots
+// fired just before and after - or itself where the patch has one source
+// axis.
 std::vector<agd::nn::ImageGroup> image_groups(const agd_gpu_problem &pb, size_t which,
                                               int in_ch) {
   std::vector<agd::nn::ImageGroup> groups;
@@ -606,9 +609,9 @@ std::vector<agd::nn::ImageGroup> image_groups(const agd_gpu_problem &pb, size_t 
     std::vector<long> stride(sh.size(), 1);
     for (int d = (int)sh.size() - 2; d >= 0; --d) stride[d] = stride[d + 1] * sh[d + 1];
     const std::vector<int> axes = source_axes(pb, p);
-    const size_t ai = which < axes.size() ? which : 0;
+    const size_t ai = in_ch > 1 ? axes.size() - 1 : (which < axes.size() ? which : 0);
     const int axis = axes[ai];
-    const int nbr_axis = axes.size() > 1 ? axes[(ai + 1) % axes.size()] : -1;
+    const int nbr_axis = in_ch > 1 && ai > 0 ? axes[ai - 1] : -1;
     agd::nn::ImageGroup *g = nullptr;
     for (auto &x : groups)
       if (x.rows == sh[axis] && x.cols == sh[D] && x.row_stride == stride[axis]) g = &x;
@@ -677,9 +680,11 @@ int agd_gpu_solve_learned(agd_gpu_problem *pb, agd_nn *net, AGD_TYPE initial_fac
     e.start_schedule(initial_factor, n_its, std::max(1, n_its - 1));
     timer.mark("initial step");
     // the pseudo-deblended input in data_dev becomes the network's estimate:
-    // the mean of its estimates from the lines along every source axis
-    const size_t n_axes = max_source_axes(*pb);
+    // the mean of its estimates from the lines along every source axis, or
+    // for a multi-channel network its estimate from the lines along the
+    // slowest source axis with their neighbours
     const int in_ch = agd::nn::input_channels(net);
+    const size_t n_axes = in_ch > 1 ? 1 : max_source_axes(*pb);
     // the input is read from an untouched copy when the estimate is written
     // over it while other images still read it (neighbour channels, more
     // axes); kept between calls: allocating half a gigabyte per call costs

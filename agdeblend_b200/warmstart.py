@@ -141,24 +141,28 @@ def training_set_vibroseis(n_surveys: int = 40, crops: int = 1, n_its: int = 150
     (16, 16, 16, 256)) deblended by the plain method on the GPU; every line
     along sX (32 shots x 2048 samples) gives `crops` windows, normalised by
     the line's RMS; with both_axes also every line along sY (16 shots,
-    zero-padded to 32 rows).  neighbours = k > 0: inputs
-    [n][32][256][2 k + 1] with the lines at sY offsets -1, +1, ..., -k, +k
-    as channels 1 .. 2 k (neighbour_lines)."""
+    zero-padded to 32 rows).  neighbours = k > 0: the surveys are 32 sY x
+    16 sX instead, and the images are the lines along sY (the slow source
+    axis, 32 shots) with the lines at sX offsets -1, +1, ..., -k, +k (the
+    shots fired just before and after) as channels 1 .. 2 k: inputs
+    [n][32][256][2 k + 1] (neighbour_lines), as agd_gpu_solve_learned feeds
+    a multi-channel network."""
     from . import Problem
 
     if neighbours and both_axes:
-        raise ValueError("neighbour channels are built for the lines along sX only")
+        raise ValueError("neighbour channels are built for the lines along sY only")
     rng = np.random.default_rng(seed + 100000)
     xs, ts = [], []
     for i in range(n_surveys):
-        sv = S.vibroseis_4d(seed=seed + i, n_sy=16, n_sx=32, n_ch=16, nt=2048,
+        n_sy, n_sx = (32, 16) if neighbours else (16, 32)
+        sv = S.vibroseis_4d(seed=seed + i, n_sy=n_sy, n_sx=n_sx, n_ch=16, nt=2048,
                             window=(16, 16, 16, 256), n_its=n_its)
         p = Problem.from_survey(sv)
         out = p.solve(sv.data, 1.0, n_its)
         p.close()
-        if neighbours:  # (sY, ch) lines along sX, neighbours along sY
-            xc = neighbour_lines(sv.data[0], 1, 0, neighbours)
-            y = neighbour_lines(out[0], 1, 0, 0)[..., 0]
+        if neighbours:  # (sX, ch) lines along sY, neighbours along sX
+            xc = neighbour_lines(sv.data[0], 0, 1, neighbours)
+            y = neighbour_lines(out[0], 0, 1, 0)[..., 0]
             for xi, yi in zip(xc, y):
                 rms = float(np.sqrt(np.mean(xi[..., 0].astype(np.float64) ** 2))) or 1.0
                 for _ in range(crops):
@@ -188,10 +192,10 @@ def train(family: str = "gather_2d", n: int = 2000, epochs: int = 8, batch: int 
           cosine: bool | None = None):
     """A network trained on the plain method's own results: family
     "gather_2d" (n receiver gathers, training_set, one input channel) or
-    "vibroseis" (n small surveys, lines along sX with their two neighbours
-    along sY as channels 1 and 2, training_set_vibroseis; the neighbours
-    raise the estimate of held-out surveys by about 0.9 dB, adding the lines
-    along sY as further samples lowered it).  Adam; with cosine the learning
+    "vibroseis" (n small surveys, lines along sY with their two neighbours
+    along sX as channels 1 and 2, training_set_vibroseis: on held-out
+    surveys this warm-starts better than lines along sX, with or without
+    neighbours along sY, and than the mean of both axes).  Adam; with cosine the learning
     rate of epoch e is lr (1 + cos(pi e / epochs)) / 2 (one agd_nn_train
     call per epoch, the optimiser state carried over).  Defaults, chosen on
     held-out surveys: lr 1e-3 with the cosine decay for "gather_2d", a

@@ -262,9 +262,11 @@ typedef struct agd_nn agd_nn;
  * change: receiver gathers) x the time samples - each normalised by its
  * RMS, run through `net` and scaled back; the estimate is the mean of the
  * estimates from the lines along every source axis.  A network with 3
- * input channels also receives the two neighbouring lines along the next
- * source axis (clamped at the patch edge; the line itself where the patch
- * has one source axis).  Float library only. */
+ * input channels instead gets the lines along the slowest source axis (the
+ * largest shot-time step), each with its two neighbouring lines along the
+ * next faster source axis as channels 1 and 2 (clamped at the patch edge;
+ * the line itself where the patch has one source axis).  Float library
+ * only. */
 int agd_gpu_solve_learned(agd_gpu_problem *problem, agd_nn *net, AGD_TYPE initial_factor,
                           int n_its, int it_begin, int print_freq, AGD_TYPE *const *data);
 

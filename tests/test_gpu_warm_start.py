@@ -85,29 +85,26 @@ def test_learned_start_reaches_plain_snr_faster():
 
 
 def _host_estimate(net, v, k):
-    """The estimate agd_gpu_solve_learned computes on the device, made on the
-    host: for each source axis of the vibroseis volume v (sX, then sY) its
-    lines with their neighbours along the other one (neighbour_lines),
-    normalised by each line's RMS, run through net, scaled back; the mean
-    of the two."""
-    outs = []
-    for line_axis, nbr_axis in ((1, 0), (0, 1)):
-        x = WS.neighbour_lines(v, line_axis, nbr_axis, k)
-        rms = np.sqrt(np.mean(x[..., 0].astype(np.float64) ** 2, axis=(1, 2)))
-        rms[rms == 0] = 1.0
-        est = net.forward((x / rms[:, None, None, None]).astype(np.float32))
-        est = est * rms[:, None, None]
-        a = np.moveaxis(v, line_axis, -2)
-        outs.append(np.moveaxis(est.reshape(a.shape), -2, line_axis))
-    return [(0.5 * (outs[0] + outs[1])).astype(np.float32)]
+    """The estimate agd_gpu_solve_learned computes on the device for a
+    multi-channel network, made on the host: the lines along the slow
+    source axis of the vibroseis volume v (sY) with their neighbours along
+    sX (neighbour_lines), normalised by each line's RMS, run through net,
+    scaled back."""
+    x = WS.neighbour_lines(v, 0, 1, k)
+    rms = np.sqrt(np.mean(x[..., 0].astype(np.float64) ** 2, axis=(1, 2)))
+    rms[rms == 0] = 1.0
+    est = net.forward((x / rms[:, None, None, None]).astype(np.float32))
+    est = est * rms[:, None, None]
+    a = np.moveaxis(v, 0, -2)
+    return [np.moveaxis(est.reshape(a.shape), -2, 0).astype(np.float32)]
 
 
 def test_learned_estimate_with_neighbour_channels_matches_host():
     """A network with three input channels: agd_gpu_solve_learned's device
-    estimate (lines along both source axes, each with its two neighbours
-    along the other axis, clamped at the edges) gives the same warm start as
+    estimate (the lines along the slow source axis sY, each with its two
+    neighbours along sX, clamped at the edges) gives the same warm start as
     the estimate built on the host and passed to agd_gpu_solve_warm."""
-    sv = S.vibroseis_4d(seed=4200, n_sy=16, n_sx=32, n_ch=16, nt=2048,
+    sv = S.vibroseis_4d(seed=4200, n_sy=32, n_sx=16, n_ch=16, nt=2048,
                         window=(16, 16, 16, 256), n_its=20)
     net = WarmStartNet(8, seed=5, in_channels=3)
     p = A.Problem.from_survey(sv)
