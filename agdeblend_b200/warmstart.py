@@ -27,19 +27,21 @@ from .nn import WarmStartNet
 TRAIN_SEED = 4000
 
 
-def trace_axis(shape, shottimes) -> int:
-    """The space axis of a patch along which shot times change least (but
-    change): its lines are receiver gathers of consecutive shots, where the
-    blending noise is incoherent."""
+def source_axes(shape, shottimes) -> list:
+    """Space axes of a patch along which shot times change, in order of
+    their mean shot-time step between neighbouring traces, smallest first
+    (the last space axis if none changes): the axes, and their order, of
+    the receiver-gather lines agd_gpu_solve_learned cuts on the device."""
     st = np.asarray(shottimes, np.float64).reshape(shape[:-1])
-    best, best_d = len(shape) - 2, np.inf
+    found = []
     for ax in range(len(shape) - 1):
         if shape[ax] < 2:
             continue
         d = float(np.mean(np.abs(np.diff(st, axis=ax))))
-        if 0 < d < best_d:
-            best, best_d = ax, d
-    return best
+        if d > 0:
+            found.append((d, ax))
+    found.sort()
+    return [ax for _, ax in found] or [len(shape) - 2]
 
 
 def to_images(patch, axis):
@@ -60,16 +62,21 @@ def _pad8(n):
 
 
 def infer(net: WarmStartNet, images, max_pixels: int = 1 << 23):
-    """Network estimate of each image, RMS-normalised in and out; sides
-    zero-padded to multiples of 8."""
+    """Network estimate of each image ([n][h][w], or [n][h][w][c] with the
+    image in channel 0 and its neighbours after it), normalised in and out
+    by the RMS of channel 0; sides zero-padded to multiples of 8."""
     imgs = np.asarray(images, np.float32)
-    n, h, w = imgs.shape
-    rms = np.sqrt(np.mean(imgs.astype(np.float64) ** 2, axis=(1, 2)))
+    if imgs.ndim == 3:
+        imgs = imgs[..., None]
+    n, h, w, c = imgs.shape
+    rms = np.sqrt(np.mean(imgs[..., 0].astype(np.float64) ** 2, axis=(1, 2)))
     rms[rms == 0] = 1.0
     hp, wp = _pad8(h), _pad8(w)
-    x = np.zeros((n, hp, wp), np.float32)
-    x[:, :h, :w] = imgs / rms[:, None, None]
-    out = np.empty_like(x)
+    x = np.zeros((n, hp, wp, c), np.float32)
+    x[:, :h, :w] = imgs / rms[:, None, None, None]
+    if c == 1:
+        x = x[..., 0]
+    out = np.empty((n, hp, wp), np.float32)
     step = max(1, max_pixels // (hp * wp))
     for i in range(0, n, step):
         out[i: i + step] = net.forward(x[i: i + step])
@@ -77,12 +84,30 @@ def infer(net: WarmStartNet, images, max_pixels: int = 1 << 23):
 
 
 def estimate(net: WarmStartNet, sv):
-    """Network estimate of the deblended data of every patch of a survey."""
+    """Network estimate of the deblended data of every patch of a survey,
+    made on the host as agd_gpu_solve_learned makes it on the device: with
+    one input channel the mean of the estimates from the lines along every
+    source axis; with 2 k + 1 channels the estimate from the lines along
+    the slowest source axis, each with its neighbours along the next faster
+    one (neighbour_lines; the line itself where there is no other)."""
     est = []
     for d, st in zip(sv.data, sv.shottimes):
-        ax = trace_axis(d.shape, st)
-        imgs, restore = to_images(d, ax)
-        est.append(restore(infer(net, imgs)).astype(np.float32))
+        axes = source_axes(d.shape, st)
+        if net.in_channels == 1:
+            outs = []
+            for ax in axes:
+                imgs, restore = to_images(d, ax)
+                outs.append(restore(infer(net, imgs)))
+            est.append(np.mean(outs, axis=0).astype(np.float32))
+            continue
+        k = (net.in_channels - 1) // 2
+        line = axes[-1]
+        imgs, restore = to_images(d, line)
+        if len(axes) > 1:
+            x = neighbour_lines(d, line, axes[-2], k)
+        else:
+            x = np.repeat(imgs[..., None], net.in_channels, axis=-1)
+        est.append(restore(infer(net, x)).astype(np.float32))
     return est
 
 

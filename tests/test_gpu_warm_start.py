@@ -84,32 +84,20 @@ def test_learned_start_reaches_plain_snr_faster():
     assert t_learned < t_plain
 
 
-def _host_estimate(net, v, k):
-    """The estimate agd_gpu_solve_learned computes on the device for a
-    multi-channel network, made on the host: the lines along the slow
-    source axis of the vibroseis volume v (sY) with their neighbours along
-    sX (neighbour_lines), normalised by each line's RMS, run through net,
-    scaled back."""
-    x = WS.neighbour_lines(v, 0, 1, k)
-    rms = np.sqrt(np.mean(x[..., 0].astype(np.float64) ** 2, axis=(1, 2)))
-    rms[rms == 0] = 1.0
-    est = net.forward((x / rms[:, None, None, None]).astype(np.float32))
-    est = est * rms[:, None, None]
-    a = np.moveaxis(v, 0, -2)
-    return [np.moveaxis(est.reshape(a.shape), -2, 0).astype(np.float32)]
-
-
-def test_learned_estimate_with_neighbour_channels_matches_host():
-    """A network with three input channels: agd_gpu_solve_learned's device
-    estimate (the lines along the slow source axis sY, each with its two
-    neighbours along sX, clamped at the edges) gives the same warm start as
-    the estimate built on the host and passed to agd_gpu_solve_warm."""
+@pytest.mark.parametrize("in_ch", [1, 3])
+def test_learned_estimate_with_neighbour_channels_matches_host(in_ch):
+    """agd_gpu_solve_learned's device estimate gives the same warm start as
+    the host's estimate of the same rule (warmstart.estimate) passed to
+    agd_gpu_solve_warm: with one input channel the mean over the lines along
+    both source axes of a vibroseis survey, with three the lines along the
+    slow source axis sY, each with its two neighbours along sX (clamped at
+    the edges)."""
     sv = S.vibroseis_4d(seed=4200, n_sy=32, n_sx=16, n_ch=16, nt=2048,
                         window=(16, 16, 16, 256), n_its=20)
-    net = WarmStartNet(8, seed=5, in_channels=3)
+    net = WarmStartNet(8, seed=5, in_channels=in_ch)
     p = A.Problem.from_survey(sv)
     dev = WS.solve_learned(p, net, sv.data, 1.0, 20, 20)
-    host = WS.solve_warm(p, sv.data, _host_estimate(net, sv.data[0], 1), 1.0, 20, 20)
+    host = WS.solve_warm(p, sv.data, WS.estimate(net, sv), 1.0, 20, 20)
     p.close()
     net.close()
     d, h = np.asarray(dev[0], np.float64), np.asarray(host[0], np.float64)
