@@ -5,7 +5,7 @@ run on the tensor cores) maps 2-D gathers of pseudo-deblended data (traces x
 time samples, each normalised by its RMS) to an estimate of the deblended
 data.  The solver then starts from the model that reproduces that estimate
 (agd_gpu_solve_warm) and runs only the tail of the plain method's threshold
-schedule.  The plain method is unchanged and stays the judge: the warm
+schedule.  The plain method is unchanged and decides the result: the warm
 start only changes where its iterations begin.
 
 Training pairs are made by the plain method itself: seeded synthetic 2-D

@@ -4,7 +4,7 @@ C++ examples compiled against include/agdeblend.h and linked with
 agdeblend_b200/libagdeblend.so, and its Python examples through its own
 cffi wrapper built with AGD_LIB_DIR=agdeblend_b200.  make_data (the
 reference's seeded data generator, examples/make_data.c, calling agd_blend)
-writes the data; each example is then judged by the reference's own
+writes the data; each example is then checked by the reference's own
 checker with the thresholds of examples/Makefile:29-55: exact blending
 (check_example.c), RMS error fraction <= 1/50 for examples 4, 5 and 7 and
 <= 0.05 for examples 8 and 9 (check_example_rmse.c)."""
